@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""Benchmark of the BSSN RK4 evolution step on B200.
+
+Default workload (N=1): the batched form -- a seeded single-level octree of
+~20,000 blocks with padded sides drawn from {13,19,31,55} with block-count
+fractions {0.7,0.2,0.08,0.02}, Brill-Lindquist two-puncture data (m=0.5 at
+(+-1,0,0)) plus a seeded 1e-8 perturbation, FP64, KO sigma 0.4, eta 2,
+dt = 0.25*dx.  One timed step = one full RK4 step (4 x {ghost fill, fused
+RHS over all blocks, zip + stage update + constraint enforcement}), replayed
+as a CUDA graph.  Prints one JSON line (see the keys below).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload mix20k|mix4k|uniform512|small]
+
+Under torchrun each rank evolves its own replica of the workload (weak
+scaling); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "dendro-gr_b200")
+sys.path.insert(0, PKG)
+
+WORKLOADS = {
+    # name: (mesh mode, dims, description)
+    "mix20k": (1, (10, 10, 7), "batched form: ~20,000 blocks, seeded size mix"),
+    "mix4k": (1, (7, 5, 4), "mixed-level plain-path size: ~4,000 blocks"),
+    "uniform512": (0, (8, 8, 8), "uniform octree of 512 blocks of 13^3"),
+    "small": (1, (2, 2, 1), "small mix for profiler captures"),
+}
+SEED_MESH = 20261203
+MIX = (0.7, 0.2, 0.08, 0.02)
+FLOP_PER_ZONE_STAGE = 6535.0  # 6,439 RHS + 96 RK axpy (per zone, per stage)
+
+
+def fused_rhs_bytes(sides):
+    """Compulsory HBM bytes of one fused-RHS pass: read the 24 padded
+    variables, write the 24 interior right-hand sides."""
+    return sum(8 * 24 * (s ** 3 + (s - 6) ** 3) for s in sides)
+
+
+def step_bytes(sides, n_nodes):
+    """Compulsory bytes of one RK stage of this implementation: ghost fill
+    (read zipped, write padded), fused RHS (read padded, write interior),
+    zip + update (read RHS, u, acc; write stage state and acc)."""
+    pad = sum(s ** 3 for s in sides)
+    inner = sum((s - 6) ** 3 for s in sides)
+    return 8 * 24 * (n_nodes + pad + pad + inner + inner + 4 * n_nodes)
+
+
+class Clocks:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's own CPU bssnrhs on the host cores
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(sides_all, seconds=15.0, threads=0):
+    """Time the reference CPU right-hand side (oracle/_ref, compiled from the
+    reference sources; else the repository's CPU restatement) on a bounded,
+    size-stratified sample of the workload's blocks with all host threads.
+    Returns (zone-updates/s, info).  One RK4 zone-update = 4 RHS passes;
+    ghost fill, zip and the stage algebra are excluded (favours the CPU)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+
+    ref = ol.reference()
+    kind = "reference"
+    if ref is None:
+        ref = ol.oracle()
+        kind = "port"
+    rng = np.random.default_rng(1)
+    # stratified sample: keep the workload's size fractions, ~2.5M zones
+    sides_all = np.asarray(sides_all)
+    uniq, counts = np.unique(sides_all, return_counts=True)
+    zones_all = float(((sides_all - 6.0) ** 3).sum())
+    target = 2.5e6
+    frac = min(1.0, target / zones_all)
+    sample = []
+    for s, c in zip(uniq, counts):
+        k = max(1, int(round(c * frac)))
+        sample += [int(s)] * k
+    # lay the sample out as independent blocks with BL-like data
+    offs, off = [], 0
+    for s in sample:
+        offs.append(off)
+        off += s ** 3
+    U = np.zeros((24, off))
+    U[[0, 1, 12, 15, 17]] = 1.0
+    U += 1e-8 * rng.uniform(-1, 1, U.shape)
+    blocks = []
+    for s, o in zip(sample, offs):
+        h = 0.05
+        pmin = rng.uniform(-6, 6, 3)
+        blocks.append((o, s, pmin, pmin + (s - 1) * h))
+    nthreads = threads or os.cpu_count()
+
+    class RB(C.Structure):
+        _fields_ = [("offset", C.c_int64), ("sz", C.c_int32), ("bflag", C.c_uint32),
+                    ("g0", C.c_int32 * 3), ("level", C.c_int32),
+                    ("ptmin", C.c_double * 3), ("ptmax", C.c_double * 3)]
+    arr = (RB * len(blocks))()
+    for i, (o, s, pm, px) in enumerate(blocks):
+        arr[i].offset, arr[i].sz, arr[i].bflag = o, s, 0
+        arr[i].ptmin[:] = list(pm)
+        arr[i].ptmax[:] = list(px)
+    R = np.zeros_like(U)
+    prm = ol.params()
+    fn = ref.lib.ref_bssnRHS_blocks if kind == "reference" else ref.lib.orc_bssnRHS
+    zones = float(sum((s - 6) ** 3 for s in sample))
+    t0 = time.perf_counter()
+    passes = 0
+    while True:
+        fn(ol.rows(R), ol.rows(U), arr, len(blocks), C.byref(prm), nthreads)
+        passes += 1
+        if time.perf_counter() - t0 > seconds and passes >= 4:
+            break
+    dt = time.perf_counter() - t0
+    rate = zones * passes / 4.0 / dt
+    return rate, {"kind": kind, "cores": nthreads,
+                  "sample": f"{len(sample)} blocks ({zones:.3g} zones) drawn with the "
+                            f"workload's size fractions; {passes} RHS passes in {dt:.1f} s; "
+                            "RHS only (ghost fill / zip / RK algebra excluded)"}
+
+
+def run_reference(args, wl):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import bssn_b200 as B
+    mode, dims, desc = WORKLOADS[wl]
+    spec = B.generate_mesh(mode, dims, MIX, seed=SEED_MESH)
+    rates = []
+    for _ in range(args.warmup):
+        cpu_reference_rate(spec.sides, seconds=2.0)
+    for _ in range(args.steps):
+        r, info = cpu_reference_rate(spec.sides, seconds=6.0)
+        rates.append(r)
+    rate = statistics.median(rates)
+    ms = spec.zones() / rate * 1e3
+    out = {"metric": "BSSN RK4 zone-updates/s FP64 on 1 B200, batched vs plain; % HBM roofline",
+           "impl": "reference", "value": rate, "unit": "zone-updates/s",
+           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": wl, "description": desc, "blocks": spec.nblocks},
+           "cpu_baseline": dict(info, value=rate, unit="zone-updates/s"),
+           "e2e": {"value": rate, "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mix20k", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    wl = args.workload
+    if args.impl == "reference":
+        run_reference(args, wl)
+        return
+
+    import torch
+    import bssn_b200 as B
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    mode, dims, desc = WORKLOADS[wl]
+    spec = B.generate_mesh(mode, dims, MIX, seed=SEED_MESH)
+    zones = spec.zones()
+    prm = B.default_params()
+    dt = 0.25 * spec.h
+    mesh = B.Mesh(spec)
+    U = torch.zeros((24, spec.n_nodes), dtype=torch.float64, device="cuda")
+    B.initial_data(U, spec)
+    U0 = None
+    stream = torch.cuda.current_stream()
+
+    # ---- batched, graph-captured plan
+    plan = B.RK4Plan(mesh, prm, B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
+    chosen, table = plan.autotune(U, reps=2)
+    for _ in range(args.warmup):
+        plan.step(U, dt)
+    torch.cuda.synchronize()
+    # kernel roofline: the fused RHS pass timed alone (CUDA events)
+    rhs_ms = C.c_float(0)
+    B.check(B.lib.bssn_rk4_plan_time_rhs(plan.h, 3, B.stream_ptr(), C.byref(rhs_ms)), "time_rhs")
+    scratch = torch.zeros(1, dtype=torch.float64, device="cuda")
+    fp64 = C.c_double(0)
+    B.lib.bssn_fp64_probe.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_double)]
+    B.check(B.lib.bssn_fp64_probe(C.c_void_p(scratch.data_ptr()), 20000, B.stream_ptr(), C.byref(fp64)), "fp64_probe")
+
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.step(U, dt)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+    ms_total = max_over_ranks(e0.elapsed_time(e1))
+    ms_step = ms_total / args.steps
+    value = zones * args.steps * world / (ms_total * 1e-3)
+    violations = plan.violations()
+    finite = bool(torch.isfinite(U).all().item())
+    plan.close()
+
+    # ---- plain path: one RHS launch per block, no graph
+    plain = None
+    if not args.no_plain:
+        pplan = B.RK4Plan(mesh, prm, B.PLAN_ENFORCE_STAGES | B.PLAN_PER_BLOCK)
+        pplan.step(U, dt)
+        torch.cuda.synchronize()
+        k = max(1, min(3, args.steps))
+        barrier()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(k):
+            pplan.step(U, dt)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        pms = max_over_ranks(a0.elapsed_time(a1)) / k
+        plain = {"value": zones * world / (pms * 1e-3), "ms_per_step": pms, "steps": k,
+                 "launches_per_step": 4 * (spec.nblocks + 2)}
+        pplan.close()
+
+    # ---- end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty_like(U, device="cpu").pin_memory()
+        host.copy_(U)
+        plan = B.RK4Plan(mesh, prm, B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
+        Ud = torch.empty_like(U)
+        nbytes = U.numel() * 8
+        Ud.copy_(host, non_blocking=True)
+        plan.step(Ud, dt)
+        host.copy_(Ud, non_blocking=True)
+        torch.cuda.synchronize()
+        k = max(1, min(3, args.steps))
+        barrier()
+        b0 = torch.cuda.Event(enable_timing=True)
+        b1 = torch.cuda.Event(enable_timing=True)
+        b0.record(stream)
+        for _ in range(k):
+            Ud.copy_(host, non_blocking=True)
+            plan.step(Ud, dt)
+            host.copy_(Ud, non_blocking=True)
+        b1.record(stream)
+        torch.cuda.synchronize()
+        ems = max_over_ranks(b0.elapsed_time(b1)) / k
+        e2e = {"value": zones * world / (ems * 1e-3), "unit": "zone-updates/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+               "ms_per_step": ems,
+               "path": "pinned host state -> device, one RK4 step through bssn_rk4_plan_step, device -> host"}
+        plan.close()
+        del host
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    peaks, peak_src = measured_peaks()
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    rb = fused_rhs_bytes(spec.sides)
+    achieved = rb / (rhs_ms.value * 1e-3) / 1e9
+    flops_rhs = zones * FLOP_PER_ZONE_STAGE
+    roofline = {"bound": "hbm", "kernel": "fused RHS pass (bssn::rhs_kernel, all buckets)",
+                "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "peak_source": peak_src,
+                "traffic": None, "launch_ms": rhs_ms.value,
+                "bytes_per_launch": rb,
+                "fp64": {"achieved_tflops": flops_rhs / (rhs_ms.value * 1e-3) / 1e12,
+                         "peak_tflops": fp64.value, "peak_source": "measured FMA probe",
+                         "frac": flops_rhs / (rhs_ms.value * 1e-3) / 1e12 / fp64.value}}
+    sb = step_bytes(spec.sides, spec.n_nodes) * 4
+    out = {"metric": "BSSN RK4 zone-updates/s FP64 on 1 B200, batched vs plain; % HBM roofline",
+           "value": value, "unit": "zone-updates/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (Brill-Lindquist + seeded 1e-8 noise)",
+           "config": {"workload": wl, "description": desc, "blocks": spec.nblocks,
+                      "zones": zones, "sides": {str(s): int((spec.sides == s).sum()) for s in sorted(set(spec.sides.tolist()))},
+                      "nodes": spec.n_nodes, "dt_over_dx": 0.25,
+                      "l2": "inputs larger than L2 (24 x %.3g nodes x 8 B)" % spec.n_nodes,
+                      "parallelism": f"replicas x{world}", "tiles": {str(k): v for k, v in chosen.items()}},
+           "roofline": roofline,
+           "step_hbm": {"bytes_per_step": sb, "achieved_gbs": sb / (ms_step * 1e-3) / 1e9,
+                        "frac": sb / (ms_step * 1e-3) / 1e9 / hbm_peak},
+           "plain": plain, "batched_vs_plain": (value / plain["value"]) if plain else None,
+           "e2e": e2e, "clocks": clk,
+           "gpu_launches": args.steps * 4 * (2 + len(chosen)),
+           "enforce_violations": violations, "state_finite": finite,
+           "autotune_ms": {str(k): v for k, v in table.items()}}
+    if not args.no_cpu:
+        rate, info = cpu_reference_rate(spec.sides, seconds=15.0)
+        out["cpu_baseline"] = dict(info, value=rate, unit="zone-updates/s")
+    print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

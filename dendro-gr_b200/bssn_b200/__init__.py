@@ -1,0 +1,309 @@
+"""Python plumbing over the C ABI of libbssn_b200.so (include/bssn_b200.h).
+
+PyTorch is used only to own device memory and streams; every computation is
+a kernel of libbssn_b200.so.  Importing this module loads the library and
+raises if it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libbssn_b200.so")
+NVARS = 24
+
+VAR_NAMES = ["alpha", "chi", "K", "Gt0", "Gt1", "Gt2", "beta0", "beta1",
+             "beta2", "B0", "B1", "B2", "gt0", "gt1", "gt2", "gt3", "gt4",
+             "gt5", "At0", "At1", "At2", "At3", "At4", "At5"]
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `make -C dendro-gr_b200` "
+        "(there is no CPU fallback)")
+lib = C.CDLL(LIB_PATH)
+
+_dp = C.POINTER(C.c_double)
+_PtrArr = C.c_void_p * NVARS
+
+
+class BssnParams(C.Structure):
+    _fields_ = [("ko_sigma", C.c_double), ("lambda_", C.c_uint * 4),
+                ("lambda_f", C.c_double * 2), ("eta_central", C.c_double),
+                ("eta_outer", C.c_double), ("eta_width", C.c_double),
+                ("cako_enabled", C.c_int), ("eps_cako_gauge", C.c_double),
+                ("eps_cako_other", C.c_double), ("chi_floor", C.c_double)]
+
+
+class BssnBlockDesc(C.Structure):
+    _fields_ = [("offset", C.c_int64), ("sz", C.c_int32), ("bflag", C.c_uint32),
+                ("g0", C.c_int32 * 3), ("level", C.c_int32),
+                ("ptmin", C.c_double * 3), ("ptmax", C.c_double * 3)]
+
+
+def default_params(ko_sigma=0.4, eta=2.0, chi_floor=1e-4, cako=False):
+    """sigma=0.4, lambda={1,1,1,1}, lambda_f={1,0}, constant eta (RIT
+    central = outer), CHI_FLOOR=1e-4: the workloads' parameters."""
+    return BssnParams(ko_sigma, (1, 1, 1, 1), (1.0, 0.0), eta, eta, 40.0,
+                      int(cako), 0.99, 0.3, chi_floor)
+
+
+def _sig():
+    vp, i, i64, d, u32 = C.c_void_p, C.c_int, C.c_int64, C.c_double, C.c_uint
+    P = C.POINTER
+    lib.bssn_version.restype = C.c_char_p
+    lib.bssn_deriv644_f64.argtypes = [i, vp, vp, d, P(u32), u32, vp]
+    lib.bssn_deriv644adv_f64.argtypes = [i, vp, vp, d, P(u32), vp, u32, vp]
+    lib.bssn_bssnrhs_f64.argtypes = [vp, vp, i64, P(d), P(d), P(u32), u32, P(BssnParams), vp]
+    lib.bssn_mesh_create.argtypes = [P(BssnBlockDesc), i, P(C.c_int32), P(vp)]
+    lib.bssn_mesh_destroy.argtypes = [vp]
+    lib.bssn_mesh_unzip_size.argtypes = [vp]
+    lib.bssn_mesh_unzip_size.restype = i64
+    lib.bssn_rhs_blocks_f64.argtypes = [vp, vp, vp, P(BssnParams), i, vp]
+    lib.bssn_unzip_f64.argtypes = [vp, vp, vp, i, vp]
+    lib.bssn_zip_f64.argtypes = [vp, vp, vp, i, vp]
+    lib.bssn_rk4_stage_f64.argtypes = [i, vp, vp, vp, i64, d, i, d, vp, vp]
+    lib.bssn_enforce_f64.argtypes = [vp, i64, d, vp, vp]
+    lib.bssn_initial_data_f64.argtypes = [vp, P(C.c_int32), P(d), d, P(d), d, d, d, d, C.c_uint64, vp]
+    lib.bssn_mesh_generate.argtypes = [i, P(C.c_int32), P(d), C.c_uint64, d, d,
+                                       P(BssnBlockDesc), P(i), P(C.c_int32), P(d)]
+    lib.bssn_rk4_plan_create.argtypes = [vp, P(BssnParams), i, P(vp)]
+    lib.bssn_rk4_plan_step.argtypes = [vp, vp, d, vp]
+    lib.bssn_rk4_plan_autotune.argtypes = [vp, vp, i, vp, P(C.c_float)]
+    lib.bssn_rk4_plan_tile.argtypes = [vp, i]
+    lib.bssn_rk4_plan_violations.argtypes = [vp, P(i)]
+    lib.bssn_rk4_plan_destroy.argtypes = [vp]
+    lib.bssn_tile_count.argtypes = []
+    lib.bssn_tile_info.argtypes = [i, P(i)]
+
+
+_sig()
+
+
+class BssnError(RuntimeError):
+    pass
+
+
+def check(rc, what=""):
+    if rc != 0:
+        raise BssnError(f"{what} failed with status {rc}")
+
+
+def ptrs(t, n_per_var=None):
+    """Array of 24 device pointers for a (24, n) float64 CUDA tensor (or a
+    list of 24 tensors)."""
+    if isinstance(t, (list, tuple)):
+        return _PtrArr(*[x.data_ptr() for x in t])
+    assert t.dtype.is_floating_point and t.is_cuda and t.is_contiguous()
+    n = t.shape[-1] if n_per_var is None else n_per_var
+    base = t.data_ptr()
+    return _PtrArr(*[base + v * n * 8 for v in range(NVARS)])
+
+
+def stream_ptr(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+# ---------------------------------------------------------------------------
+# meshes
+# ---------------------------------------------------------------------------
+@dataclass
+class MeshSpec:
+    blocks: object          # ctypes array of BssnBlockDesc
+    nblocks: int
+    G: tuple
+    h: float
+    xmin: float
+    sides: np.ndarray = field(default=None)
+
+    @property
+    def n_nodes(self):
+        return int(self.G[0]) * int(self.G[1]) * int(self.G[2])
+
+    @property
+    def n_unzip(self):
+        b = self.blocks[self.nblocks - 1]
+        return int(b.offset) + int(b.sz) ** 3
+
+    def zones(self):
+        return int(sum((int(s) - 6) ** 3 for s in self.sides))
+
+    def as_numpy(self):
+        """Structured copy for the CPU oracle (same memory layout)."""
+        return np.ctypeslib.as_array(self.blocks, shape=(self.nblocks,)).copy()
+
+
+def generate_mesh(mode, dims, p=(0.7, 0.2, 0.08, 0.02), seed=0, xmin=-8.0, L=16.0):
+    """mode 0: uniform 13^3 blocks on a dims[0]^3 octant box; mode 1: seeded
+    mix of 13/19/31/55 blocks on a dims super-cell box (8^3 octants each)."""
+    d = (C.c_int32 * 3)(*dims)
+    pp = (C.c_double * 4)(*p)
+    n = C.c_int(0)
+    G = (C.c_int32 * 3)()
+    h = C.c_double(0)
+    check(lib.bssn_mesh_generate(mode, d, pp, seed, xmin, L, None, C.byref(n), G, C.byref(h)), "mesh_generate")
+    blocks = (BssnBlockDesc * n.value)()
+    check(lib.bssn_mesh_generate(mode, d, pp, seed, xmin, L, blocks, C.byref(n), G, C.byref(h)), "mesh_generate")
+    sides = np.array([blocks[b].sz for b in range(n.value)], dtype=np.int32)
+    return MeshSpec(blocks, n.value, tuple(G), h.value, xmin, sides)
+
+
+class Mesh:
+    """Device mesh handle (bssn_mesh)."""
+
+    def __init__(self, spec: MeshSpec):
+        self.spec = spec
+        self.h = C.c_void_p()
+        G = (C.c_int32 * 3)(*spec.G)
+        check(lib.bssn_mesh_create(spec.blocks, spec.nblocks, G, C.byref(self.h)), "mesh_create")
+        self.n_unzip = lib.bssn_mesh_unzip_size(self.h)
+
+    def close(self):
+        if self.h:
+            lib.bssn_mesh_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def unzip(self, unz, zip_, nvars=NVARS, stream=None):
+        check(lib.bssn_unzip_f64(self.h, ptrs(unz), ptrs(zip_), nvars, stream_ptr(stream)), "unzip")
+
+    def zip(self, zip_, unz, nvars=NVARS, stream=None):
+        check(lib.bssn_zip_f64(self.h, ptrs(zip_), ptrs(unz), nvars, stream_ptr(stream)), "zip")
+
+    def rhs(self, out, u, params, tile=-1, stream=None):
+        check(lib.bssn_rhs_blocks_f64(self.h, ptrs(out), ptrs(u), C.byref(params), tile, stream_ptr(stream)), "rhs_blocks")
+
+
+def bssnrhs_block(out, u, offset, pmin, pmax, side, bflag, params, stream=None):
+    pm = (C.c_double * 3)(*pmin)
+    px = (C.c_double * 3)(*pmax)
+    sz = (C.c_uint * 3)(side, side, side)
+    check(lib.bssn_bssnrhs_f64(ptrs(out), ptrs(u), offset, pm, px, sz, bflag, C.byref(params), stream_ptr(stream)), "bssnrhs")
+
+
+def deriv(kind, D, u, h, sz, bflag, stream=None):
+    s = (C.c_uint * 3)(*sz)
+    check(lib.bssn_deriv644_f64(kind, C.c_void_p(D.data_ptr()), C.c_void_p(u.data_ptr()), h, s, bflag, stream_ptr(stream)), "deriv644")
+
+
+def initial_data(U, spec: MeshSpec, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0), m1=0.5, m2=0.5,
+                 chi_floor=1e-4, eps=1e-8, seed=20261203, stream=None):
+    G = (C.c_int32 * 3)(*spec.G)
+    xm = (C.c_double * 3)(spec.xmin, spec.xmin, spec.xmin)
+    b = (C.c_double * 6)(*bh)
+    check(lib.bssn_initial_data_f64(ptrs(U), G, xm, spec.h, b, m1, m2, chi_floor, eps, seed, stream_ptr(stream)), "initial_data")
+
+
+def rk4_stage(stage, out, prev, k, n, dt, enforce=True, chi_floor=1e-4, status=None, stream=None):
+    if stage < 3:
+        kp = ptrs(k)
+    else:
+        kp = (C.c_void_p * (4 * NVARS))(*[p for kk in k for p in ptrs(kk)])
+    st = C.c_void_p(status.data_ptr()) if status is not None else None
+    check(lib.bssn_rk4_stage_f64(stage, ptrs(out), ptrs(prev), kp, n, dt, int(enforce), chi_floor, st, stream_ptr(stream)), "rk4_stage")
+
+
+def enforce(U, n, chi_floor=1e-4, status=None, stream=None):
+    st = C.c_void_p(status.data_ptr()) if status is not None else None
+    check(lib.bssn_enforce_f64(ptrs(U), n, chi_floor, st, stream_ptr(stream)), "enforce")
+
+
+class PlainRK4:
+    """The plain GPU path of one classical RK4 step, mirroring
+    BSSN_GR/src/rkBSSN.cpp:764-860 call for call: per stage unzip -> bssnRHS
+    over all blocks -> zip -> stage axpy (+ enforce)."""
+
+    def __init__(self, mesh: Mesh, params, enforce_stages=True, tile=-1):
+        import torch
+        self.mesh = mesh
+        self.params = params
+        self.enforce_stages = enforce_stages
+        self.tile = tile
+        n = mesh.spec.n_nodes
+        nu = mesh.n_unzip
+        dev = "cuda"
+        self.prev = torch.empty((NVARS, n), dtype=torch.float64, device=dev)
+        self.im = torch.empty((NVARS, n), dtype=torch.float64, device=dev)
+        self.k = [torch.empty((NVARS, n), dtype=torch.float64, device=dev) for _ in range(4)]
+        self.uz = torch.zeros((NVARS, nu), dtype=torch.float64, device=dev)
+        self.rz = torch.zeros((NVARS, nu), dtype=torch.float64, device=dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def step(self, U, dt, stream=None):
+        n = self.mesh.spec.n_nodes
+        cf = self.params.chi_floor
+        self.prev.copy_(U)
+        for stage in range(4):
+            src = U if stage == 0 else self.im
+            self.mesh.unzip(self.uz, src, stream=stream)
+            self.mesh.rhs(self.rz, self.uz, self.params, tile=self.tile, stream=stream)
+            self.mesh.zip(self.k[stage], self.rz, stream=stream)
+            if stage < 3:
+                rk4_stage(stage, self.im, self.prev, self.k[stage], n, dt,
+                          self.enforce_stages, cf, self.status, stream)
+            else:
+                rk4_stage(3, U, self.prev, self.k, n, dt, True, cf, self.status, stream)
+
+
+def tiles():
+    out = []
+    info = (C.c_int * 4)()
+    for t in range(lib.bssn_tile_count()):
+        check(lib.bssn_tile_info(t, info), "tile_info")
+        out.append(tuple(info))
+    return out
+
+
+PLAN_ENFORCE_STAGES = 1
+PLAN_GRAPH = 2
+PLAN_PER_BLOCK = 4
+
+
+class RK4Plan:
+    """bssn_rk4_plan: one whole RK4 step (unzip -> fused RHS -> zip+stage
+    update, x4), batched per block-size bucket and optionally captured as a
+    CUDA graph; or the plain path with one RHS launch per block."""
+
+    def __init__(self, mesh: Mesh, params, flags=PLAN_ENFORCE_STAGES | PLAN_GRAPH):
+        self.mesh = mesh
+        self.params = params
+        self.h = C.c_void_p()
+        check(lib.bssn_rk4_plan_create(mesh.h, C.byref(params), flags, C.byref(self.h)), "rk4_plan_create")
+
+    def step(self, U, dt, stream=None):
+        check(lib.bssn_rk4_plan_step(self.h, ptrs(U), dt, stream_ptr(stream)), "rk4_plan_step")
+
+    def autotune(self, U, reps=3, stream=None):
+        sides = sorted(set(self.mesh.spec.sides.tolist()))
+        nt = lib.bssn_tile_count()
+        times = (C.c_float * (len(sides) * nt))()
+        check(lib.bssn_rk4_plan_autotune(self.h, ptrs(U), reps, stream_ptr(stream), times), "autotune")
+        table = {side: [times[i * nt + t] for t in range(nt)] for i, side in enumerate(sides)}
+        chosen = {side: lib.bssn_rk4_plan_tile(self.h, side) for side in sides}
+        return chosen, table
+
+    def violations(self):
+        c = C.c_int(0)
+        check(lib.bssn_rk4_plan_violations(self.h, C.byref(c)), "violations")
+        return c.value
+
+    def close(self):
+        if self.h:
+            lib.bssn_rk4_plan_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

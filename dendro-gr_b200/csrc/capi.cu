@@ -1,0 +1,224 @@
+// The extern "C" entry points of include/bssn_b200.h: argument checks and
+// kernel launches.  No entry point allocates device memory except the mesh
+// handle's creation and its first use of a tile shape (task list upload).
+#include <cuda_runtime.h>
+
+#include <cstring>
+
+#include "bssn_b200.h"
+#include "bssn_common.cuh"
+#include "kernels.cuh"
+#include "mesh.h"
+#include "plan.h"
+#include "rhs_fused.cuh"
+
+struct bssn_mesh_s {
+    bssn::MeshState* st;
+};
+
+struct bssn_rk4_plan_s {
+    bssn::Plan* p;
+};
+
+namespace {
+
+bool valid_side(int s) { return s == 13 || s == 19 || s == 31 || s == 55; }
+
+cudaStream_t S(bssn_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int default_tile() { return 0; }
+
+int tile_for_side(const bssn::MeshState* m, int side) {
+    auto it = m->tuned.find(side);
+    return it == m->tuned.end() ? default_tile() : it->second;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bssn_version(void) { return "bssn-b200 0.1 (sm_100a, FP64)"; }
+
+int bssn_deriv644_f64(int kind, double* D_dev, const double* u_dev, double h,
+                      const unsigned sz[3], unsigned bflag, bssn_stream_t stream) {
+    if (!D_dev || !u_dev || !sz) return BSSN_EINVAL;
+    if (kind < 0 || kind > 8) return BSSN_EKIND;
+    for (int d = 0; d < 3; d++)
+        if (sz[d] < 12) return BSSN_EBLOCKSIZE;
+    return bssn::launch_stencil(kind, D_dev, u_dev, h, sz, bflag, S(stream));
+}
+
+int bssn_deriv644adv_f64(int dir, double* D_dev, const double* u_dev, double h,
+                         const unsigned sz[3], const double* beta_dev, unsigned bflag,
+                         bssn_stream_t stream) {
+    (void)beta_dev;
+    if (dir < 0 || dir > 2) return BSSN_EKIND;
+    return bssn_deriv644_f64(dir, D_dev, u_dev, h, sz, bflag, stream);
+}
+
+int bssn_bssnrhs_f64(double* const* rhs_dev, const double* const* u_dev, int64_t offset,
+                     const double pmin[3], const double pmax[3], const unsigned sz[3],
+                     unsigned bflag, const BssnParams* params, bssn_stream_t stream) {
+    if (!rhs_dev || !u_dev || !pmin || !pmax || !sz || !params) return BSSN_EINVAL;
+    if (sz[0] != sz[1] || sz[1] != sz[2] || !valid_side((int)sz[0])) return BSSN_EBLOCKSIZE;
+    bssn::RhsArgs A;
+    for (int v = 0; v < bssn::NVARS; v++) {
+        if (!u_dev[v] || !rhs_dev[v]) return BSSN_EINVAL;
+        A.u.p[v] = u_dev[v];
+        A.rhs.p[v] = rhs_dev[v];
+    }
+    A.prm = *params;
+    BssnBlockDesc b;
+    std::memset(&b, 0, sizeof(b));
+    b.offset = offset;
+    b.sz = (int32_t)sz[0];
+    b.bflag = bflag;
+    for (int d = 0; d < 3; d++) {
+        b.ptmin[d] = pmin[d];
+        b.ptmax[d] = pmax[d];
+    }
+    return bssn::launch_rhs_single(default_tile(), A, b, S(stream));
+}
+
+int bssn_mesh_create(const BssnBlockDesc* blocks, int nblocks, const int32_t G[3],
+                     bssn_mesh* out) {
+    if (!blocks || nblocks <= 0 || !G || !out) return BSSN_EINVAL;
+    for (int b = 0; b < nblocks; b++)
+        if (!valid_side(blocks[b].sz) || blocks[b].offset < 0) return BSSN_EBLOCKSIZE;
+    bssn::MeshState* st = nullptr;
+    int r = bssn::mesh_create(blocks, nblocks, G, &st);
+    if (r) return r;
+    *out = new bssn_mesh_s{st};
+    return 0;
+}
+
+int bssn_mesh_destroy(bssn_mesh mesh) {
+    if (!mesh) return BSSN_EINVAL;
+    bssn::mesh_destroy(mesh->st);
+    delete mesh;
+    return 0;
+}
+
+int64_t bssn_mesh_unzip_size(bssn_mesh mesh) { return mesh ? mesh->st->unzip_size : -1; }
+
+int bssn_rhs_blocks_f64(bssn_mesh mesh, double* const* rhs_dev, const double* const* u_dev,
+                        const BssnParams* params, int tile, bssn_stream_t stream) {
+    if (!mesh || !rhs_dev || !u_dev || !params) return BSSN_EINVAL;
+    if (tile < -1 || tile >= bssn::tile_count()) return BSSN_EINVAL;
+    bssn::RhsArgs A;
+    for (int v = 0; v < bssn::NVARS; v++) {
+        if (!u_dev[v] || !rhs_dev[v]) return BSSN_EINVAL;
+        A.u.p[v] = u_dev[v];
+        A.rhs.p[v] = rhs_dev[v];
+    }
+    A.prm = *params;
+    const int t = tile >= 0 ? tile : tile_for_side(mesh->st, 0);
+    const bssn::BrickTask* tasks;
+    int ntasks;
+    int r = bssn::mesh_tasks(mesh->st, t, &tasks, &ntasks);
+    if (r) return r;
+    return bssn::launch_rhs_tasks(t, A, mesh->st->d_blocks, tasks, ntasks, S(stream));
+}
+
+int bssn_unzip_f64(bssn_mesh mesh, double* const* unzip_dev, const double* const* zip_dev,
+                   int nvars, bssn_stream_t stream) {
+    if (!mesh || !unzip_dev || !zip_dev || nvars < 1 || nvars > bssn::NVARS) return BSSN_EINVAL;
+    return bssn::launch_unzip(mesh->st, unzip_dev, zip_dev, nvars, S(stream));
+}
+
+int bssn_zip_f64(bssn_mesh mesh, double* const* zip_dev, const double* const* unzip_dev,
+                 int nvars, bssn_stream_t stream) {
+    if (!mesh || !unzip_dev || !zip_dev || nvars < 1 || nvars > bssn::NVARS) return BSSN_EINVAL;
+    return bssn::launch_zip(mesh->st, zip_dev, unzip_dev, nvars, S(stream));
+}
+
+int bssn_rk4_stage_f64(int stage, double* const* out_dev, const double* const* u_prev_dev,
+                       const double* const* k_dev, int64_t n, double dt, int enforce,
+                       double chi_floor, int* status_dev, bssn_stream_t stream) {
+    if (stage < 0 || stage > 3 || !out_dev || !u_prev_dev || !k_dev || n < 0) return BSSN_EINVAL;
+    if (n == 0) return 0;
+    return bssn::launch_rk4_stage(stage, out_dev, u_prev_dev, k_dev, n, dt, enforce,
+                                  chi_floor, status_dev, S(stream));
+}
+
+int bssn_enforce_f64(double* const* u_dev, int64_t n, double chi_floor, int* status_dev,
+                     bssn_stream_t stream) {
+    if (!u_dev || n < 0) return BSSN_EINVAL;
+    if (n == 0) return 0;
+    return bssn::launch_enforce(u_dev, n, chi_floor, status_dev, S(stream));
+}
+
+int bssn_initial_data_f64(double* const* u_dev, const int32_t G[3], const double xmin[3],
+                          double h, const double bh[6], double m1, double m2,
+                          double chi_floor, double eps, uint64_t seed, bssn_stream_t stream) {
+    if (!u_dev || !G || !xmin || !bh) return BSSN_EINVAL;
+    return bssn::launch_initial_data(u_dev, G, xmin, h, bh, m1, m2, chi_floor, eps, seed,
+                                     S(stream));
+}
+
+int bssn_mesh_generate(int mode, const int32_t dims[3], const double p[4], uint64_t seed,
+                       double xmin, double L, BssnBlockDesc* blocks, int* nblocks,
+                       int32_t G[3], double* h) {
+    if (!dims || !nblocks || !G || !h || (mode == 1 && !p)) return BSSN_EINVAL;
+    return bssn::mesh_generate(mode, dims, p, seed, xmin, L, blocks, nblocks, G, h);
+}
+
+int bssn_rk4_plan_create(bssn_mesh mesh, const BssnParams* params, int flags,
+                         bssn_rk4_plan* out) {
+    if (!mesh || !params || !out) return BSSN_EINVAL;
+    bssn::Plan* p = nullptr;
+    int st = bssn::plan_create(mesh->st, *params, flags, &p);
+    if (st) return st;
+    *out = new bssn_rk4_plan_s{p};
+    return 0;
+}
+
+int bssn_rk4_plan_step(bssn_rk4_plan plan, double* const* u_dev, double dt,
+                       bssn_stream_t stream) {
+    if (!plan || !u_dev) return BSSN_EINVAL;
+    for (int v = 0; v < bssn::NVARS; v++)
+        if (!u_dev[v]) return BSSN_EINVAL;
+    return bssn::plan_step(plan->p, u_dev, dt, S(stream));
+}
+
+int bssn_rk4_plan_autotune(bssn_rk4_plan plan, double* const* u_dev, int reps,
+                           bssn_stream_t stream, float* times) {
+    if (!plan || !u_dev || reps < 1) return BSSN_EINVAL;
+    return bssn::plan_autotune(plan->p, u_dev, reps, S(stream), times);
+}
+
+int bssn_rk4_plan_tile(bssn_rk4_plan plan, int side) {
+    if (!plan) return -BSSN_EINVAL;
+    return bssn::plan_tile(plan->p, side);
+}
+
+int bssn_rk4_plan_violations(bssn_rk4_plan plan, int* count) {
+    if (!plan || !count) return BSSN_EINVAL;
+    return bssn::cuda_status(cudaMemcpy(count, plan->p->status, sizeof(int), cudaMemcpyDeviceToHost));
+}
+
+int bssn_rk4_plan_time_rhs(bssn_rk4_plan plan, int reps, bssn_stream_t stream, float* ms) {
+    if (!plan || reps < 1 || !ms) return BSSN_EINVAL;
+    return bssn::plan_time_rhs(plan->p, reps, S(stream), ms);
+}
+
+int bssn_fp64_probe(double* scratch_dev, int iters, bssn_stream_t stream, double* tflops) {
+    if (!scratch_dev || iters < 1 || !tflops) return BSSN_EINVAL;
+    return bssn::fp64_probe(scratch_dev, iters, S(stream), tflops);
+}
+
+int bssn_rk4_plan_destroy(bssn_rk4_plan plan) {
+    if (!plan) return BSSN_EINVAL;
+    bssn::plan_destroy(plan->p);
+    delete plan;
+    return 0;
+}
+
+int bssn_tile_count(void) { return bssn::tile_count(); }
+
+int bssn_tile_info(int tile, int info[4]) {
+    if (!info) return BSSN_EINVAL;
+    return bssn::tile_info(tile, info);
+}
+
+}  // extern "C"

@@ -1,0 +1,47 @@
+// Host-side mesh state behind the bssn_mesh handle.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <utility>
+#include <vector>
+
+#include "bssn_b200.h"
+#include "rhs_fused.cuh"
+
+namespace bssn {
+
+// A run of consecutive points of one block handled by one CTA.
+struct Chunk {
+    int32_t blk;
+    int32_t count;
+    int64_t start;
+};
+
+struct MeshState {
+    std::vector<BssnBlockDesc> blocks;
+    int32_t G[3];
+    int64_t unzip_size;
+    BssnBlockDesc* d_blocks = nullptr;
+    Chunk* d_pad_chunks = nullptr;
+    Chunk* d_int_chunks = nullptr;
+    int n_pad_chunks = 0;
+    int n_int_chunks = 0;
+    // brick task lists per (tile shape, block side; side 0 = all blocks):
+    // (device pointer, count)
+    std::map<std::pair<int, int>, std::pair<BrickTask*, int>> tasks;
+    // autotuned tile per padded side (0 = not tuned)
+    std::map<int, int> tuned;
+};
+
+int mesh_create(const BssnBlockDesc* blocks, int nblocks, const int32_t G[3],
+                MeshState** out);
+void mesh_destroy(MeshState* m);
+int mesh_tasks(MeshState* m, int tile, const BrickTask** tasks, int* ntasks);
+int mesh_tasks_side(MeshState* m, int tile, int side, const BrickTask** tasks, int* ntasks);
+int mesh_generate(int mode, const int32_t dims[3], const double p[4], uint64_t seed,
+                  double xmin, double L, BssnBlockDesc* blocks, int* nblocks,
+                  int32_t G[3], double* h);
+
+}  // namespace bssn

@@ -1,0 +1,304 @@
+// The whole RK4 step as one plan: per stage a ghost fill (unzip), the fused
+// right-hand side over every brick of every block (one launch per block-size
+// bucket with that bucket's autotuned tile), and the zip fused with the stage
+// algebra.  Optionally captured once as a CUDA graph and replayed, or run as
+// the plain path with one right-hand-side launch per block (the structure of
+// the reference's bssnRHS block loop, rhs.cpp:10-73) for comparison.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <set>
+#include <vector>
+
+#include "bssn_b200.h"
+#include "bssn_common.cuh"
+#include "kernels.cuh"
+#include "mesh.h"
+#include "plan.h"
+#include "rhs_fused.cuh"
+
+namespace bssn {
+
+namespace {
+
+int alloc(double** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) return 0;
+    return cudaMalloc((void**)p, n * sizeof(double)) == cudaSuccess ? 0 : BSSN_ENOMEM;
+}
+
+void set_ptrs(double* base, int64_t n, double* out[NVARS]) {
+    for (int v = 0; v < NVARS; v++) out[v] = base + v * n;
+}
+
+}  // namespace
+
+int plan_create(MeshState* m, const BssnParams& prm, int flags, Plan** out) {
+    Plan* p = new Plan();
+    p->mesh = m;
+    p->prm = prm;
+    p->flags = flags;
+    const int64_t nu = m->unzip_size;
+    const int64_t nn = (int64_t)m->G[0] * m->G[1] * m->G[2];
+    p->n_nodes = nn;
+    int st = alloc(&p->P, (size_t)NVARS * nu);
+    if (!st) st = alloc(&p->R, (size_t)NVARS * nu);
+    if (!st) st = alloc(&p->im, (size_t)NVARS * nn);
+    if (!st) st = alloc(&p->acc, (size_t)NVARS * nn);
+    if (!st && cudaMalloc((void**)&p->status, sizeof(int)) != cudaSuccess) st = BSSN_ENOMEM;
+    if (!st) st = cuda_status(cudaMemset(p->status, 0, sizeof(int)));
+    // padded buffers start at zero so never-written points stay finite
+    if (!st) st = cuda_status(cudaMemset(p->P, 0, sizeof(double) * NVARS * nu));
+    if (!st) st = cuda_status(cudaMemset(p->R, 0, sizeof(double) * NVARS * nu));
+    if (st) {
+        plan_destroy(p);
+        return st;
+    }
+    std::set<int> sides;
+    for (auto& b : m->blocks) sides.insert(b.sz);
+    p->sides.assign(sides.begin(), sides.end());
+    // task lists and kernel attributes must exist before any graph capture
+    for (int side : p->sides) {
+        for (int t = 0; t < tile_count(); t++) {
+            const BrickTask* tk;
+            int nt;
+            st = mesh_tasks_side(m, t, side, &tk, &nt);
+            if (st) {
+                plan_destroy(p);
+                return st;
+            }
+        }
+    }
+    st = prepare_all_tiles();
+    if (st) {
+        plan_destroy(p);
+        return st;
+    }
+    *out = p;
+    return 0;
+}
+
+void plan_destroy(Plan* p) {
+    if (!p) return;
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    cudaFree(p->P);
+    cudaFree(p->R);
+    cudaFree(p->im);
+    cudaFree(p->acc);
+    cudaFree(p->status);
+    delete p;
+}
+
+int plan_tile(const Plan* p, int side) {
+    auto it = p->mesh->tuned.find(side);
+    return it == p->mesh->tuned.end() ? 0 : it->second;
+}
+
+int plan_rhs(Plan* p, cudaStream_t s) {
+    MeshState* m = p->mesh;
+    RhsArgs A;
+    A.prm = p->prm;
+    double* Pp[NVARS];
+    double* Rp[NVARS];
+    set_ptrs(p->P, m->unzip_size, Pp);
+    set_ptrs(p->R, m->unzip_size, Rp);
+    for (int v = 0; v < NVARS; v++) {
+        A.u.p[v] = Pp[v];
+        A.rhs.p[v] = Rp[v];
+    }
+    if (p->flags & BSSN_PLAN_PER_BLOCK) {
+        for (auto& b : m->blocks) {
+            int st = launch_rhs_single(plan_tile(p, b.sz), A, b, s);
+            if (st) return st;
+        }
+        return 0;
+    }
+    for (int side : p->sides) {
+        const int t = plan_tile(p, side);
+        const BrickTask* tk;
+        int nt;
+        int st = mesh_tasks_side(m, t, side, &tk, &nt);
+        if (!st) st = launch_rhs_tasks(t, A, m->d_blocks, tk, nt, s);
+        if (st) return st;
+    }
+    return 0;
+}
+
+int plan_enqueue(Plan* p, double* const* u, double dt, cudaStream_t s) {
+    MeshState* m = p->mesh;
+    double* Pp[NVARS];
+    double* Rp[NVARS];
+    double* Ip[NVARS];
+    double* Ap[NVARS];
+    set_ptrs(p->P, m->unzip_size, Pp);
+    set_ptrs(p->R, m->unzip_size, Rp);
+    set_ptrs(p->im, p->n_nodes, Ip);
+    set_ptrs(p->acc, p->n_nodes, Ap);
+    const int enf = (p->flags & BSSN_PLAN_ENFORCE_STAGES) ? 1 : 0;
+    for (int stage = 0; stage < 4; stage++) {
+        const double* const* src = stage == 0 ? (const double* const*)u : (const double* const*)Ip;
+        int st = launch_unzip(m, Pp, src, NVARS, s);
+        if (!st) st = plan_rhs(p, s);
+        if (!st) st = launch_zip_stage(m, stage, Ip, Ap, u, Rp, dt, enf, p->prm.chi_floor,
+                                       p->status, s);
+        if (st) return st;
+    }
+    return 0;
+}
+
+int plan_step(Plan* p, double* const* u, double dt, cudaStream_t s) {
+    if (!(p->flags & BSSN_PLAN_GRAPH)) return plan_enqueue(p, u, dt, s);
+    bool same = p->exec && p->graph_dt == dt;
+    for (int v = 0; v < NVARS && same; v++) same = p->graph_u[v] == u[v];
+    if (!same) {
+        if (p->exec) cudaGraphExecDestroy(p->exec);
+        if (p->graph) cudaGraphDestroy(p->graph);
+        p->exec = nullptr;
+        p->graph = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return cuda_status(e);
+        int st = plan_enqueue(p, u, dt, s);
+        cudaGraph_t g = nullptr;
+        e = cudaStreamEndCapture(s, &g);
+        if (st) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        if (e != cudaSuccess) return cuda_status(e);
+        p->graph = g;
+        e = cudaGraphInstantiate(&p->exec, g, 0);
+        if (e != cudaSuccess) return cuda_status(e);
+        for (int v = 0; v < NVARS; v++) p->graph_u[v] = u[v];
+        p->graph_dt = dt;
+    }
+    return cuda_status(cudaGraphLaunch(p->exec, s));
+}
+
+// Project-written autotuner: for every block-size bucket of the mesh, time
+// the fused right-hand side of that bucket with every compiled tile shape on
+// the current padded state (CUDA events, best of `reps` after one warm-up)
+// and keep the fastest.  Blocking.
+int plan_autotune(Plan* p, double* const* u, int reps, cudaStream_t s, float* times_out) {
+    MeshState* m = p->mesh;
+    double* Pp[NVARS];
+    set_ptrs(p->P, m->unzip_size, Pp);
+    int st = launch_unzip(m, Pp, (const double* const*)u, NVARS, s);
+    if (st) return st;
+    RhsArgs A;
+    A.prm = p->prm;
+    double* Rp[NVARS];
+    set_ptrs(p->R, m->unzip_size, Rp);
+    for (int v = 0; v < NVARS; v++) {
+        A.u.p[v] = Pp[v];
+        A.rhs.p[v] = Rp[v];
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int nt = tile_count();
+    int idx = 0;
+    for (int side : p->sides) {
+        float best = 1e30f;
+        int best_t = 0;
+        for (int t = 0; t < nt; t++) {
+            const BrickTask* tk;
+            int ntask;
+            st = mesh_tasks_side(m, t, side, &tk, &ntask);
+            if (st) break;
+            float tbest = 1e30f;
+            for (int r = 0; r <= reps; r++) {
+                cudaEventRecord(e0, s);
+                st = launch_rhs_tasks(t, A, m->d_blocks, tk, ntask, s);
+                cudaEventRecord(e1, s);
+                if (st) break;
+                cudaEventSynchronize(e1);
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (r > 0) tbest = std::min(tbest, ms);
+            }
+            if (st) break;
+            if (times_out) times_out[idx * nt + t] = tbest;
+            if (tbest < best) {
+                best = tbest;
+                best_t = t;
+            }
+        }
+        if (st) break;
+        m->tuned[side] = best_t;
+        idx++;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (p->exec) {  // tile choice changed: recapture on the next step
+        cudaGraphExecDestroy(p->exec);
+        cudaGraphDestroy(p->graph);
+        p->exec = nullptr;
+        p->graph = nullptr;
+    }
+    return st;
+}
+
+// Average duration of one full fused-RHS pass (all buckets) on the plan's
+// current padded state, CUDA events on `s` around `reps` back-to-back passes
+// after one warm-up pass.  Blocking.
+int plan_time_rhs(Plan* p, int reps, cudaStream_t s, float* ms) {
+    int st = plan_rhs(p, s);
+    if (st) return st;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < reps && !st; r++) st = plan_rhs(p, s);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    *ms = t / reps;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return st ? st : cuda_status(cudaGetLastError());
+}
+
+namespace {
+// FP64 multiply-add throughput probe: 8 independent chains per thread.
+__global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
+    double x[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) x[q] = threadIdx.x * 1e-3 + q;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int q = 0; q < 8; q++) x[q] = fma(x[q], a, b);
+    }
+    double s = 0;
+#pragma unroll
+    for (int q = 0; q < 8; q++) s += x[q];
+    if (s == 12345.678) out[0] = s;  // keeps the chains alive
+}
+}  // namespace
+
+int fp64_probe(double* scratch, int iters, cudaStream_t s, double* tflops) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int blocks = sms * 8, threads = 256;
+    fp64_probe_kernel<<<blocks, threads, 0, s>>>(scratch, 16, 0.999999, 1e-7);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    fp64_probe_kernel<<<blocks, threads, 0, s>>>(scratch, iters, 0.999999, 1e-7);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return cuda_status(cudaGetLastError());
+}
+
+}  // namespace bssn

@@ -1,0 +1,38 @@
+// RK4 plan state behind the bssn_rk4_plan handle.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "bssn_b200.h"
+#include "bssn_common.cuh"
+#include "mesh.h"
+
+namespace bssn {
+
+struct Plan {
+    MeshState* mesh = nullptr;
+    BssnParams prm;
+    int flags = 0;
+    int64_t n_nodes = 0;
+    double* P = nullptr;    // padded stage state (24 x unzip size)
+    double* R = nullptr;    // padded right-hand side
+    double* im = nullptr;   // zipped intermediate stage state
+    double* acc = nullptr;  // zipped RK4 accumulator
+    int* status = nullptr;  // enforcement violations (device)
+    std::vector<int> sides; // block-size buckets present
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double* graph_u[NVARS] = {nullptr};
+    double graph_dt = 0.0;
+};
+
+int plan_create(MeshState* m, const BssnParams& prm, int flags, Plan** out);
+void plan_destroy(Plan* p);
+int plan_step(Plan* p, double* const* u, double dt, cudaStream_t s);
+int plan_autotune(Plan* p, double* const* u, int reps, cudaStream_t s, float* times_out);
+int plan_tile(const Plan* p, int side);
+int plan_time_rhs(Plan* p, int reps, cudaStream_t s, float* ms);
+int fp64_probe(double* scratch, int iters, cudaStream_t s, double* tflops);
+
+}  // namespace bssn

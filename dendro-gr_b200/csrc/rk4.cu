@@ -1,0 +1,282 @@
+// RK4 stage updates, constraint enforcement and puncture initial data on
+// zipped node vectors.  Memory-bound elementwise kernels; every product and
+// sum is explicitly rounded in the reference's order so the stage algebra is
+// bit-identical to the CPU restatement (BSSN_GR/src/rkBSSN.cpp:764-860).
+#include <cuda_runtime.h>
+
+#include "bssn_common.cuh"
+#include "kernels.cuh"
+#include "mesh.h"
+
+namespace bssn {
+namespace {
+
+__constant__ double kRK4_C[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+__constant__ double kRK4_U[4] = {0.0, 1.0 / 2.0, 1.0 / 2.0, 1.0};
+
+#define M_(a, b) __dmul_rn(a, b)
+#define A_(a, b) __dadd_rn(a, b)
+#define S_(a, b) __dsub_rn(a, b)
+
+// enforce_bssn_constraints on one node held in registers
+// (BSSN_GR/include/bssn_constraints.h:15-172).  Returns 1 on a violation;
+// the reference exits there, this code counts it and continues with the
+// reference's fallback (flat metric when det < 0).
+__device__ int enforce_regs(double v[NVARS], double chi_floor) {
+    const double one_third = 1.0 / 3.0;
+    int bad = 0;
+    double g00 = v[U_SYMGT0], g01 = v[U_SYMGT1], g02 = v[U_SYMGT2],
+           g11 = v[U_SYMGT3], g12 = v[U_SYMGT4], g22 = v[U_SYMGT5];
+    double a00 = v[U_SYMAT0], a01 = v[U_SYMAT1], a02 = v[U_SYMAT2],
+           a11 = v[U_SYMAT3], a12 = v[U_SYMAT4], a22 = v[U_SYMAT5];
+    auto det3 = [&]() {
+        // g00*(g11*g22 - g12*g12) - g01*g01*g22 + 2.0*g01*g02*g12 - g02*g02*g11
+        double t = M_(g00, S_(M_(g11, g22), M_(g12, g12)));
+        t = S_(t, M_(M_(g01, g01), g22));
+        t = A_(t, M_(M_(M_(2.0, g01), g02), g12));
+        t = S_(t, M_(M_(g02, g02), g11));
+        return t;
+    };
+    double det = det3();
+    if (det < 0.0) {
+        bad = 1;
+        g00 = g11 = g22 = 1.0;
+        g01 = g02 = g12 = 0.0;
+        det = 1.0;
+    }
+    const double f = __ddiv_rn(1.0, pow(det, one_third));
+    g00 = M_(g00, f); g01 = M_(g01, f); g02 = M_(g02, f);
+    g11 = M_(g11, f); g12 = M_(g12, f); g22 = M_(g22, f);
+    det = det3();
+    if (fabs(S_(det, 1.0)) > 1.0e-6) bad = 1;
+    const double idet = __ddiv_rn(1.0, det);
+    const double u00 = M_(idet, S_(M_(g11, g22), M_(g12, g12)));
+    const double u01 = M_(idet, A_(M_(-g01, g22), M_(g02, g12)));
+    const double u02 = M_(idet, S_(M_(g01, g12), M_(g02, g11)));
+    const double u11 = M_(idet, S_(M_(g00, g22), M_(g02, g02)));
+    const double u12 = M_(idet, A_(M_(-g00, g12), M_(g01, g02)));
+    const double u22 = M_(idet, S_(M_(g00, g11), M_(g01, g01)));
+    auto trace = [&]() {
+        double t = A_(A_(M_(a00, u00), M_(a11, u11)), M_(a22, u22));
+        const double o = A_(A_(M_(a01, u01), M_(a02, u02)), M_(a12, u12));
+        return A_(t, M_(2.0, o));
+    };
+    const double tt = M_(one_third, trace());
+    a00 = S_(a00, M_(tt, g00)); a01 = S_(a01, M_(tt, g01));
+    a02 = S_(a02, M_(tt, g02)); a11 = S_(a11, M_(tt, g11));
+    a12 = S_(a12, M_(tt, g12)); a22 = S_(a22, M_(tt, g22));
+    if (fabs(trace()) > 1.0e-6) bad = 1;
+    v[U_SYMAT0] = a00; v[U_SYMAT1] = a01; v[U_SYMAT2] = a02;
+    v[U_SYMAT3] = a11; v[U_SYMAT4] = a12; v[U_SYMAT5] = a22;
+    v[U_SYMGT0] = g00; v[U_SYMGT1] = g01; v[U_SYMGT2] = g02;
+    v[U_SYMGT3] = g11; v[U_SYMGT4] = g12; v[U_SYMGT5] = g22;
+    if (v[U_CHI] < chi_floor) v[U_CHI] = chi_floor;
+    v[U_ALPHA] = fmax(v[U_ALPHA], chi_floor);
+    return bad;
+}
+
+struct KPtrs { const double* p[4 * NVARS]; };
+
+__global__ void rk4_stage_kernel(int stage, MutVars out, ConstVars prev, KPtrs k,
+                                 int64_t n, double dt, int enforce,
+                                 double chi_floor, int* status) {
+    int bad = 0;
+    for (int64_t node = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; node < n;
+         node += (int64_t)gridDim.x * blockDim.x) {
+        double v[NVARS];
+        if (stage < 3) {
+            const double c = M_(kRK4_U[stage + 1], dt);
+#pragma unroll
+            for (int q = 0; q < NVARS; q++) v[q] = A_(prev.p[q][node], M_(c, k.p[q][node]));
+        } else {
+#pragma unroll
+            for (int q = 0; q < NVARS; q++) {
+                double t = prev.p[q][node];
+#pragma unroll
+                for (int s = 0; s < 4; s++) t = A_(t, M_(M_(kRK4_C[s], dt), k.p[s * NVARS + q][node]));
+                v[q] = t;
+            }
+        }
+        if (enforce) bad += enforce_regs(v, chi_floor);
+#pragma unroll
+        for (int q = 0; q < NVARS; q++) out.p[q][node] = v[q];
+    }
+    if (status && bad) atomicAdd(status, bad);
+}
+
+__global__ void enforce_kernel(MutVars u, int64_t n, double chi_floor, int* status) {
+    int bad = 0;
+    for (int64_t node = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; node < n;
+         node += (int64_t)gridDim.x * blockDim.x) {
+        double v[NVARS];
+#pragma unroll
+        for (int q = 0; q < NVARS; q++) v[q] = u.p[q][node];
+        bad += enforce_regs(v, chi_floor);
+#pragma unroll
+        for (int q = 0; q < NVARS; q++) u.p[q][node] = v[q];
+    }
+    if (status && bad) atomicAdd(status, bad);
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// Brill-Lindquist data with zero momenta and spins
+// (BSSN_GR/src/grUtils.cpp:1033-1035, 1082-1100), then a seeded uniform
+// perturbation and enforcement.
+__global__ void initial_data_kernel(MutVars u, int gx, int gy, int gz, double x0,
+                                    double y0, double z0, double h, double b0,
+                                    double b1, double b2, double b3, double b4,
+                                    double b5, double m1, double m2,
+                                    double chi_floor, double eps, uint64_t seed) {
+    const int64_t N = (int64_t)gx * gy * gz;
+    for (int64_t node = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; node < N;
+         node += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t ix = node % gx, iy = (node / gx) % gy, iz = node / ((int64_t)gx * gy);
+        const double x = A_(x0, M_((double)ix, h)), y = A_(y0, M_((double)iy, h)),
+                     z = A_(z0, M_((double)iz, h));
+        const double x1 = S_(x, b0), y1 = S_(y, b1), z1 = S_(z, b2);
+        const double x2 = S_(x, b3), y2 = S_(y, b4), z2 = S_(z, b5);
+        const double rv1 = __dsqrt_rn(A_(A_(M_(x1, x1), M_(y1, y1)), M_(z1, z1)));
+        const double rv2 = __dsqrt_rn(A_(A_(M_(x2, x2), M_(y2, y2)), M_(z2, z2)));
+        double psi = A_(1.0, __ddiv_rn(m1, M_(2.0, rv1)));
+        psi = A_(psi, __ddiv_rn(m2, M_(2.0, rv2)));
+        double v[NVARS];
+#pragma unroll
+        for (int q = 0; q < NVARS; q++) v[q] = 0.0;
+        v[U_ALPHA] = fmax(__ddiv_rn(1.0, M_(psi, psi)), chi_floor);
+        v[U_CHI] = __ddiv_rn(1.0, pow(psi, 4.0));
+        if (v[U_CHI] < chi_floor) v[U_CHI] = chi_floor;
+        v[U_SYMGT0] = v[U_SYMGT3] = v[U_SYMGT5] = 1.0;
+#pragma unroll
+        for (int q = 0; q < NVARS; q++) {
+            const uint64_t r = mix64(seed + 0x9E3779B97F4A7C15ULL * (uint64_t)(q * N + node + 1));
+            const double unit = M_((double)(r >> 11), 1.0 / 9007199254740992.0);
+            v[q] = A_(v[q], M_(eps, S_(M_(2.0, unit), 1.0)));
+        }
+        enforce_regs(v, chi_floor);
+#pragma unroll
+        for (int q = 0; q < NVARS; q++) u.p[q][node] = v[q];
+    }
+}
+
+// Zip fused with the RK4 stage algebra: every node owned by a block takes
+// its right-hand side k from the block's padded output R and updates the
+// stage state (stage 0..2) or the final state (stage 3):
+//   stage s < 3:  im  = u + RK4_U[s+1]*dt*k   (then enforce, optional)
+//                 acc = (s == 0 ? u : acc) + RK4_C[s]*dt*k
+//   stage 3:      u   = acc + RK4_C[3]*dt*k   (then enforce)
+// The accumulation order equals rkBSSN.cpp:851-858 term by term.
+__global__ void zip_stage_kernel(int stage, MutVars im, MutVars acc, MutVars u,
+                                 ConstVars R, const BssnBlockDesc* __restrict__ blocks,
+                                 const Chunk* __restrict__ chunks, int gx, int gy, int gz,
+                                 double dt, int enforce, double chi_floor, int* status) {
+    const Chunk c = chunks[blockIdx.x];
+    const BssnBlockDesc b = blocks[c.blk];
+    const int s = b.sz, N = s - 6;
+    const int64_t n = (int64_t)N * N * N;
+    const int64_t q = c.start + threadIdx.x;
+    int bad = 0;
+    if (q < n && threadIdx.x < c.count) {
+        const int i = (int)(q % N), j = (int)((q / N) % N), k = (int)(q / ((int64_t)N * N));
+        const int64_t x = b.g0[0] + i, y = b.g0[1] + j, z = b.g0[2] + k;
+        const bool own = (i < N - 1 || x == gx - 1) && (j < N - 1 || y == gy - 1) &&
+                         (k < N - 1 || z == gz - 1);
+        if (own) {
+            const int64_t node = x + (int64_t)gx * (y + (int64_t)gy * z);
+            const int64_t p = b.offset + (i + 3) + (int64_t)s * ((j + 3) + (int64_t)s * (k + 3));
+            double v[NVARS];
+            if (stage < 3) {
+                const double cu = M_(kRK4_U[stage + 1], dt);
+                const double cc = M_(kRK4_C[stage], dt);
+#pragma unroll
+                for (int q2 = 0; q2 < NVARS; q2++) {
+                    const double kk = __ldg(R.p[q2] + p);
+                    const double u0 = u.p[q2][node];
+                    const double a0 = stage == 0 ? u0 : acc.p[q2][node];
+                    acc.p[q2][node] = A_(a0, M_(cc, kk));
+                    v[q2] = A_(u0, M_(cu, kk));
+                }
+                if (enforce) bad = enforce_regs(v, chi_floor);
+#pragma unroll
+                for (int q2 = 0; q2 < NVARS; q2++) im.p[q2][node] = v[q2];
+            } else {
+                const double cc = M_(kRK4_C[3], dt);
+#pragma unroll
+                for (int q2 = 0; q2 < NVARS; q2++)
+                    v[q2] = A_(acc.p[q2][node], M_(cc, __ldg(R.p[q2] + p)));
+                bad = enforce_regs(v, chi_floor);
+#pragma unroll
+                for (int q2 = 0; q2 < NVARS; q2++) u.p[q2][node] = v[q2];
+            }
+        }
+    }
+    if (status && bad) atomicAdd(status, bad);
+}
+
+int grid_for(int64_t n, int threads) {
+    int64_t b = (n + threads - 1) / threads;
+    if (b > 148 * 64) b = 148 * 64;
+    return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+int launch_rk4_stage(int stage, double* const* out, const double* const* prev,
+                     const double* const* k, int64_t n, double dt, int enforce,
+                     double chi_floor, int* status, cudaStream_t s) {
+    MutVars o;
+    ConstVars p;
+    KPtrs kk = {};
+    for (int q = 0; q < NVARS; q++) {
+        o.p[q] = out[q];
+        p.p[q] = prev[q];
+    }
+    const int nk = stage < 3 ? NVARS : 4 * NVARS;
+    for (int q = 0; q < nk; q++) kk.p[q] = k[q];
+    rk4_stage_kernel<<<grid_for(n, 256), 256, 0, s>>>(stage, o, p, kk, n, dt, enforce, chi_floor, status);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_enforce(double* const* u, int64_t n, double chi_floor, int* status,
+                   cudaStream_t s) {
+    MutVars o;
+    for (int q = 0; q < NVARS; q++) o.p[q] = u[q];
+    enforce_kernel<<<grid_for(n, 256), 256, 0, s>>>(o, n, chi_floor, status);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_initial_data(double* const* u, const int32_t G[3], const double xmin[3],
+                        double h, const double bh[6], double m1, double m2,
+                        double chi_floor, double eps, uint64_t seed, cudaStream_t s) {
+    MutVars o;
+    for (int q = 0; q < NVARS; q++) o.p[q] = u[q];
+    const int64_t n = (int64_t)G[0] * G[1] * G[2];
+    initial_data_kernel<<<grid_for(n, 256), 256, 0, s>>>(
+        o, G[0], G[1], G[2], xmin[0], xmin[1], xmin[2], h, bh[0], bh[1], bh[2],
+        bh[3], bh[4], bh[5], m1, m2, chi_floor, eps, seed);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_zip_stage(const MeshState* m, int stage, double* const* im, double* const* acc,
+                     double* const* u, const double* const* R, double dt, int enforce,
+                     double chi_floor, int* status, cudaStream_t s) {
+    MutVars I, Ac, U;
+    ConstVars Rr;
+    for (int q = 0; q < NVARS; q++) {
+        I.p[q] = im[q];
+        Ac.p[q] = acc[q];
+        U.p[q] = u[q];
+        Rr.p[q] = R[q];
+    }
+    if (m->n_int_chunks == 0) return 0;
+    zip_stage_kernel<<<m->n_int_chunks, 1024, 0, s>>>(stage, I, Ac, U, Rr, m->d_blocks,
+                                                      m->d_int_chunks, m->G[0], m->G[1],
+                                                      m->G[2], dt, enforce, chi_floor, status);
+    return cuda_status(cudaGetLastError());
+}
+
+}  // namespace bssn

@@ -1,0 +1,236 @@
+/* bssn_b200.h -- C ABI of the B200-native BSSN evolution hot path.
+ *
+ * Plain pointers and sizes only.  Every array argument named *_dev is device
+ * memory; the caller owns all of it.  Variable arrays follow the reference's
+ * structure-of-arrays layout: an array of 24 per-variable base pointers
+ * indexed u[v][offset + i + nx*(j + ny*k)], variable order
+ *   alpha, chi, K, Gt0..2, beta0..2, B0..2, gt0..5, At0..5
+ * (BSSN_GR/include/grDef.h:35-60).  Blocks are padded cubes of side
+ * s in {13, 19, 31, 55} with a 3-point halo; only interior points
+ * [3, s-3)^3 of a right-hand side are written.
+ *
+ * Boundary flag bits: x-min, x-max, y-min, y-max, z-min, z-max = bits 0..5
+ * (the reference's 1u << OCT_DIR_{LEFT,RIGHT,DOWN,UP,BACK,FRONT}).
+ *
+ * Return codes: 0 success; > 0 invalid argument (BSSN_E*); < 0 a CUDA error
+ * (the negated cudaError_t).  No entry point traps, asserts or exits.  All
+ * calls are asynchronous on the given stream unless stated otherwise, and a
+ * handle may be used from one stream at a time.
+ */
+#ifndef BSSN_B200_H
+#define BSSN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* bssn_stream_t; /* == cudaStream_t */
+
+#define BSSN_OK 0
+#define BSSN_EINVAL 1       /* null pointer or bad size */
+#define BSSN_EBLOCKSIZE 2   /* block side not in {13,19,31,55} or not cubic */
+#define BSSN_EKIND 3        /* unknown stencil kind */
+#define BSSN_ENOMEM 4       /* device allocation failed */
+#define BSSN_ESTATE 5       /* handle used out of order */
+#define BSSN_ELIMIT 6       /* size exceeds a documented fixed maximum */
+
+#define BSSN_NUM_VARS 24
+
+/* Hot-path parameters the reference reads from bssn:: globals
+ * (BSSN_GR/src/parameters.cpp:14-16,40-43,123-136). */
+typedef struct BssnParams {
+    double ko_sigma;        /* KO_DISS_SIGMA */
+    unsigned lambda[4];     /* BSSN_LAMBDA */
+    double lambda_f[2];     /* BSSN_LAMBDA_F */
+    double eta_central;     /* RIT_ETA_CENTRAL */
+    double eta_outer;       /* RIT_ETA_OUTER */
+    double eta_width;       /* RIT_ETA_WIDTH */
+    int cako_enabled;       /* BSSN_CAKO_ENABLED */
+    double eps_cako_gauge;  /* BSSN_EPSILON_CAKO_GAUGE */
+    double eps_cako_other;  /* BSSN_EPSILON_CAKO_OTHER */
+    double chi_floor;       /* CHI_FLOOR */
+} BssnParams;
+
+/* One block (the reference's ot::Block as read by bssnRHS, rhs.cpp:50-67 and
+ * BlockGPU3D, bssn_kernels.cuh:1352-1357).  ptmin/ptmax are the coordinates
+ * of padded points (0,0,0) and (s-1,s-1,s-1); the grid spacing is
+ * (ptmax-ptmin)/(s-1) per axis exactly as the reference computes it.
+ * g0 is the global node index of the block's first interior node in the
+ * zipped node grid (used by unzip/zip only). */
+typedef struct BssnBlockDesc {
+    int64_t offset;
+    int32_t sz;
+    uint32_t bflag;
+    int32_t g0[3];
+    int32_t level;
+    double ptmin[3];
+    double ptmax[3];
+} BssnBlockDesc;
+
+/* ---------------------------------------------------------------------- */
+/* Stand-alone stencils on one padded block, bit-identical to the reference
+ * (same expression order, no contraction).
+ * kind: 0 deriv644_x, 1 _y, 2 _z, 3 _xx, 4 _yy, 5 _zz,
+ *       6 ko_deriv42_x, 7 _y, 8 _z.
+ * Replaces deriv644_{x,y,z,xx,yy,zz} (BSSN_GR/src/derivs.cpp:2619-3312,
+ * include/derivs.h:76-130) and ko_deriv42_{x,y,z} (derivs.cpp:964-1305).
+ * Writes exactly the points the reference writes. */
+int bssn_deriv644_f64(int kind, double* D_dev, const double* u_dev, double h,
+                      const unsigned sz[3], unsigned bflag,
+                      bssn_stream_t stream);
+/* deriv644adv_{x,y,z}(..., beta, ...) (derivs.cpp:3313-3347): the reference
+ * hard-wires them to the centred stencil; beta_dev is accepted and unused. */
+int bssn_deriv644adv_f64(int dir, double* D_dev, const double* u_dev, double h,
+                         const unsigned sz[3], const double* beta_dev,
+                         unsigned bflag, bssn_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
+/* Fused right-hand side of one block: derivatives, pointwise BSSN
+ * equations, Sommerfeld boundary conditions and Kreiss-Oliger dissipation in
+ * one kernel; derivatives never leave the chip.
+ * Replaces bssnrhs(unzipVarsRHS, uZipVars, offset, pmin, pmax, sz, bflag,
+ * t, uZipConstVars) (BSSN_GR/src/rhs.cpp:80-504, include/rhs.h:32-36); t and
+ * the constraint arrays are unused by the standard-gauge equations. */
+int bssn_bssnrhs_f64(double* const* rhs_dev, const double* const* u_dev,
+                     int64_t offset, const double pmin[3],
+                     const double pmax[3], const unsigned sz[3],
+                     unsigned bflag, const BssnParams* params,
+                     bssn_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
+/* Mesh handle: a device copy of a block list plus the zipped node grid
+ * dims G (the zipped vector of each variable holds G[0]*G[1]*G[2] nodes,
+ * node index gx + G[0]*(gy + G[1]*gz)).  Created once per mesh; blocking. */
+typedef struct bssn_mesh_s* bssn_mesh;
+int bssn_mesh_create(const BssnBlockDesc* blocks, int nblocks,
+                     const int32_t G[3], bssn_mesh* out);
+int bssn_mesh_destroy(bssn_mesh mesh);
+/* total padded points (sum of s^3 rounded per block to the layout's
+ * offsets) = one past the largest offset + s^3 */
+int64_t bssn_mesh_unzip_size(bssn_mesh mesh);
+
+/* All blocks of a mesh in one launch.  Replaces bssnRHS(unzipVarsRHS,
+ * uZipVars, blkList, numBlocks, t, uZipConstVars) (rhs.cpp:10-73) and the
+ * GPU comparator device::bssnrhs3 (cuda/include/bssn_kernels.cuh:1526-1538).
+ * tile: -1 = the autotuned choice per block size (the default tile before
+ * tuning); otherwise a tile id in [0, bssn_tile_count()). */
+int bssn_rhs_blocks_f64(bssn_mesh mesh, double* const* rhs_dev,
+                        const double* const* u_dev, const BssnParams* params,
+                        int tile, bssn_stream_t stream);
+
+/* Ghost fill: zipped node vectors -> padded block arrays (interior and
+ * halo).  Padded points whose node lies outside the node grid get 0.
+ * Replaces ot::Mesh::unzip (dendrolib, absent; call sites
+ * BSSN_GR/src/rkBSSN.cpp:611-650, bssnCtx.cpp:73). */
+int bssn_unzip_f64(bssn_mesh mesh, double* const* unzip_dev,
+                   const double* const* zip_dev, int nvars,
+                   bssn_stream_t stream);
+/* Padded block interiors -> zipped nodes; each node is written by exactly
+ * one block (the one containing octant floor(g/6), clamped to the grid).
+ * Replaces ot::Mesh::zip (dendrolib; rkBSSN.cpp:633,647, bssnCtx.cpp:103). */
+int bssn_zip_f64(bssn_mesh mesh, double* const* zip_dev,
+                 const double* const* unzip_dev, int nvars,
+                 bssn_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
+/* RK4 stage updates on zipped vectors of n nodes (rkBSSN.cpp:764-860,
+ * coefficients rkBSSN.h:50-53).
+ *   stage in 0..2:  u_im = u_prev + RK4_U[stage+1]*dt*k   (then optionally
+ *                   enforce constraints on u_im)
+ *   stage 3:        u = u_prev + sum_s RK4_C[s]*dt*k_s, k_s given as 4
+ *                   arrays of 24 pointers (k_dev[s*24 + v]); then enforce.
+ * enforce: 1 = apply enforce_bssn_constraints to every written node.
+ * status_dev (optional, may be NULL): an int the kernel atomically adds the
+ * number of nodes that violated det(gt)>0 / |det-1|<=1e-6 / |trA|<=1e-6
+ * (the reference exits at the first one; this library counts and goes on). */
+int bssn_rk4_stage_f64(int stage, double* const* out_dev,
+                       const double* const* u_prev_dev,
+                       const double* const* k_dev, int64_t n, double dt,
+                       int enforce, double chi_floor, int* status_dev,
+                       bssn_stream_t stream);
+
+/* enforce_bssn_constraints on n zipped nodes in place
+ * (BSSN_GR/include/bssn_constraints.h:15-172); violations counted as above. */
+int bssn_enforce_f64(double* const* u_dev, int64_t n, double chi_floor,
+                     int* status_dev, bssn_stream_t stream);
+
+/* Brill-Lindquist puncture data (BSSN_GR/src/grUtils.cpp:864-1178 with zero
+ * momenta and spins) on the G[0]xG[1]xG[2] node grid with coordinates
+ * xmin + g*h, plus a seeded uniform perturbation of amplitude eps on every
+ * variable (counter-based: node and variable index hashed with the seed),
+ * then enforcement.  bh = {x1,y1,z1,x2,y2,z2}. */
+int bssn_initial_data_f64(double* const* u_dev, const int32_t G[3],
+                          const double xmin[3], double h, const double bh[6],
+                          double m1, double m2, double chi_floor, double eps,
+                          uint64_t seed, bssn_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
+/* One whole RK4 step as a plan over a mesh (the reference's per-step
+ * sequence rkBSSN.cpp:764-860: per stage unzip -> bssnRHS -> zip -> stage
+ * update).  The plan owns its scratch buffers (two padded 24-variable
+ * arrays of bssn_mesh_unzip_size doubles and two zipped 24-variable arrays),
+ * allocated at creation.  Per stage it runs the ghost fill, the fused
+ * right-hand side (one launch per block-size bucket with that bucket's tile,
+ * or one launch per block with BSSN_PLAN_PER_BLOCK), and the zip fused with
+ * the stage algebra; with BSSN_PLAN_GRAPH the 4-stage sequence is captured
+ * once as a CUDA graph and replayed (recaptured when u_dev or dt change).
+ * u_dev (24 zipped arrays of G[0]*G[1]*G[2] doubles) is advanced in place. */
+#define BSSN_PLAN_ENFORCE_STAGES 1 /* enforce constraints on stage states */
+#define BSSN_PLAN_GRAPH 2          /* capture / replay as a CUDA graph */
+#define BSSN_PLAN_PER_BLOCK 4      /* one RHS launch per block (plain path) */
+typedef struct bssn_rk4_plan_s* bssn_rk4_plan;
+int bssn_rk4_plan_create(bssn_mesh mesh, const BssnParams* params, int flags,
+                         bssn_rk4_plan* out);
+int bssn_rk4_plan_step(bssn_rk4_plan plan, double* const* u_dev, double dt,
+                       bssn_stream_t stream);
+/* Autotuner: times every tile shape on every block-size bucket of the mesh
+ * with the state u_dev (best of reps) and keeps the fastest per bucket in the
+ * mesh handle.  Blocking.  times (optional): nbuckets x bssn_tile_count()
+ * milliseconds, buckets in increasing side order. */
+int bssn_rk4_plan_autotune(bssn_rk4_plan plan, double* const* u_dev, int reps,
+                           bssn_stream_t stream, float* times);
+/* The tile chosen for block side `side` (after autotuning; 0 before). */
+int bssn_rk4_plan_tile(bssn_rk4_plan plan, int side);
+/* Enforcement violations accumulated since creation (blocking read). */
+int bssn_rk4_plan_violations(bssn_rk4_plan plan, int* count);
+int bssn_rk4_plan_destroy(bssn_rk4_plan plan);
+/* Average milliseconds of one fused right-hand-side pass over all blocks on
+ * the plan's current stage state (CUDA events, after one warm-up).
+ * Blocking.  Used for the kernel's roofline. */
+int bssn_rk4_plan_time_rhs(bssn_rk4_plan plan, int reps, bssn_stream_t stream,
+                           float* ms);
+/* Measured FP64 fused-multiply-add throughput of this device in TFLOP/s
+ * (2 flops per FMA, all SMs, independent chains); scratch_dev: 1 double. */
+int bssn_fp64_probe(double* scratch_dev, int iters, bssn_stream_t stream,
+                    double* tflops);
+
+/* ---------------------------------------------------------------------- */
+/* Synthetic single-level octree meshes (host only, no device work).
+ * The domain is a box of super-cells of 8^3 octants; each super-cell is
+ * split top-down with seeded choices into blocks of 1, 2, 4 or 8 octants
+ * per side (padded sides 13, 19, 31, 55) so that the expected block-count
+ * fractions are p[0..3].  mode 0: uniform 13^3 blocks on an M^3 octant box
+ * (M = dims[0]); mode 1: seeded mix on a dims[0]xdims[1]xdims[2] super-cell
+ * box.  Coordinates: the box spans [xmin, xmin + L] along its longest axis,
+ * octant width L / octants, h = octant width / 6.  Block offsets are packed
+ * in block order, each rounded up to an even number of doubles.
+ * Call once with blocks == NULL to get the count in *nblocks. */
+int bssn_mesh_generate(int mode, const int32_t dims[3], const double p[4],
+                       uint64_t seed, double xmin, double L,
+                       BssnBlockDesc* blocks, int* nblocks, int32_t G[3],
+                       double* h);
+
+/* Number of compiled tile shapes and their description (bx, by, bz,
+ * threads) for the fused RHS kernel. */
+int bssn_tile_count(void);
+int bssn_tile_info(int tile, int info[4]);
+
+const char* bssn_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BSSN_B200_H */

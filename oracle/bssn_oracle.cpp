@@ -1,0 +1,914 @@
+// Test infrastructure only: the CPU oracle (see bssn_oracle.h).  Loaded by
+// tests/, the smoke check and bench.py's CPU-baseline leg, never by the
+// product library.  Build: make -C oracle (g++ -O2 -ffp-contract=off).
+//
+// The stencils keep the reference's expression order so that, compiled
+// without floating-point contraction, they are bit-identical to
+// BSSN_GR/src/derivs.cpp.  The pointwise BSSN equations are written from the
+// symbolic definitions in CodeGen/bssn.py and CodeGen/dendro.py as plain
+// tensor loops (not from the generated C), so they agree with the reference
+// to rounding only.
+#include "bssn_oracle.h"
+
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+enum {
+    U_ALPHA = 0, U_CHI, U_K, U_GT0, U_GT1, U_GT2, U_BETA0, U_BETA1, U_BETA2,
+    U_B0, U_B1, U_B2, U_SYMGT0, U_SYMGT1, U_SYMGT2, U_SYMGT3, U_SYMGT4,
+    U_SYMGT5, U_SYMAT0, U_SYMAT1, U_SYMAT2, U_SYMAT3, U_SYMAT4, U_SYMAT5,
+    NVARS
+};
+
+inline int sym(int i, int j) {
+    static const int m[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    return m[i][j];
+}
+
+// ---------------------------------------------------------------------------
+// Stencils: BSSN_GR/src/derivs.cpp:2619-3312 (deriv644_*), :964-1305
+// (ko_deriv42_*).  dir = 0,1,2 for x,y,z.
+// ---------------------------------------------------------------------------
+
+// Loop ranges of the first-derivative stencils: x over all j,k
+// (derivs.cpp:2627-2633), y over all k (:2728-2734), z interior only.
+void first_range(int dir, const unsigned* sz, int lo[3], int hi[3]) {
+    for (int d = 0; d < 3; d++) {
+        lo[d] = 3;
+        hi[d] = (int)sz[d] - 3;
+    }
+    if (dir == 0) { lo[1] = 0; hi[1] = sz[1]; lo[2] = 0; hi[2] = sz[2]; }
+    if (dir == 1) { lo[2] = 0; hi[2] = sz[2]; }
+}
+
+void deriv644(double* D, const double* u, double dx, const unsigned* sz,
+              unsigned bflag, int dir) {
+    const double idx = 1.0 / dx;
+    const double idx_by_12 = idx / 12.0;
+    const double idx_by_60 = idx / 60.0;
+    const int nx = sz[0], ny = sz[1];
+    const int n = dir == 0 ? 1 : (dir == 1 ? nx : nx * ny);
+    int lo[3], hi[3];
+    first_range(dir, sz, lo, hi);
+    const int N = sz[dir];
+    const int ie = N - 3;
+    for (int k = lo[2]; k < hi[2]; k++)
+        for (int j = lo[1]; j < hi[1]; j++)
+            for (int i = lo[0]; i < hi[0]; i++) {
+                const int pp = i + nx * (j + ny * k);
+                D[pp] = (-u[pp - 3 * n] + 9.0 * u[pp - 2 * n] -
+                         45.0 * u[pp - n] + 45.0 * u[pp + n] -
+                         9.0 * u[pp + 2 * n] + u[pp + 3 * n]) *
+                        idx_by_60;
+            }
+    const bool lo_face = bflag & (1u << (2 * dir));
+    const bool hi_face = bflag & (1u << (2 * dir + 1));
+    if (!lo_face && !hi_face) return;
+    for (int k = lo[2]; k < hi[2]; k++)
+        for (int j = lo[1]; j < hi[1]; j++)
+            for (int i = lo[0]; i < hi[0]; i++) {
+                const int c[3] = {i, j, k};
+                const int a = c[dir];
+                // base = index of the point with along-coordinate 0
+                const int base = i + nx * (j + ny * k) - a * n;
+                auto U = [&](int m) { return u[base + m * n]; };
+                double* out = &D[base + a * n];
+                if (lo_face) {
+                    if (a == 3)
+                        *out = (-25.0 * U(3) + 48.0 * U(4) - 36.0 * U(5) +
+                                16.0 * U(6) - 3.0 * U(7)) * idx_by_12;
+                    else if (a == 4)
+                        *out = (-3.0 * U(3) - 10.0 * U(4) + 18.0 * U(5) -
+                                6.0 * U(6) + U(7)) * idx_by_12;
+                    else if (a == 5)
+                        *out = (+U(3) - 8.0 * U(4) + 8.0 * U(6) - U(7)) *
+                               idx_by_12;
+                }
+                if (hi_face) {
+                    if (a == ie - 3)
+                        *out = (+U(ie - 5) - 8.0 * U(ie - 4) + 8.0 * U(ie - 2) -
+                                U(ie - 1)) * idx_by_12;
+                    else if (a == ie - 2)
+                        *out = (-U(ie - 5) + 6.0 * U(ie - 4) - 18.0 * U(ie - 3) +
+                                10.0 * U(ie - 2) + 3.0 * U(ie - 1)) * idx_by_12;
+                    else if (a == ie - 1)
+                        *out = (3.0 * U(ie - 5) - 16.0 * U(ie - 4) +
+                                36.0 * U(ie - 3) - 48.0 * U(ie - 2) +
+                                25.0 * U(ie - 1)) * idx_by_12;
+                }
+            }
+}
+
+void deriv644_2(double* D, const double* u, double dx, const unsigned* sz,
+                unsigned bflag, int dir) {
+    const double idx_sqrd = 1.0 / (dx * dx);
+    const double idx_sqrd_by_180 = idx_sqrd / 180.0;
+    const double idx_sqrd_by_12 = idx_sqrd / 12.0;
+    const int nx = sz[0], ny = sz[1], nz = sz[2];
+    const int n = dir == 0 ? 1 : (dir == 1 ? nx : nx * ny);
+    const int ie = sz[dir] - 3;
+    const bool lo_face = bflag & (1u << (2 * dir));
+    const bool hi_face = bflag & (1u << (2 * dir + 1));
+    for (int k = 3; k < nz - 3; k++)
+        for (int j = 3; j < ny - 3; j++)
+            for (int i = 3; i < nx - 3; i++) {
+                const int pp = i + nx * (j + ny * k);
+                D[pp] = (2.0 * u[pp - 3 * n] - 27.0 * u[pp - 2 * n] +
+                         270.0 * u[pp - n] - 490.0 * u[pp] + 270.0 * u[pp + n] -
+                         27.0 * u[pp + 2 * n] + 2.0 * u[pp + 3 * n]) *
+                        idx_sqrd_by_180;
+            }
+    if (!lo_face && !hi_face) return;
+    for (int k = 3; k < nz - 3; k++)
+        for (int j = 3; j < ny - 3; j++)
+            for (int i = 3; i < nx - 3; i++) {
+                const int c[3] = {i, j, k};
+                const int a = c[dir];
+                const int base = i + nx * (j + ny * k) - a * n;
+                auto U = [&](int m) { return u[base + m * n]; };
+                double* out = &D[base + a * n];
+                if (lo_face) {
+                    if (a == 3)
+                        *out = (45.0 * U(3) - 154.0 * U(4) + 214.0 * U(5) -
+                                156.0 * U(6) + 61.0 * U(7) - 10.0 * U(8)) *
+                               idx_sqrd_by_12;
+                    else if (a == 4)
+                        *out = (10.0 * U(3) - 15.0 * U(4) - 4.0 * U(5) +
+                                14.0 * U(6) - 6.0 * U(7) + U(8)) * idx_sqrd_by_12;
+                    else if (a == 5)
+                        *out = (-U(3) + 16.0 * U(4) - 30.0 * U(5) + 16.0 * U(6) -
+                                U(7)) * idx_sqrd_by_12;
+                }
+                if (hi_face) {
+                    if (a == ie - 3)
+                        *out = (-U(ie - 5) + 16.0 * U(ie - 4) - 30.0 * U(ie - 3) +
+                                16.0 * U(ie - 2) - U(ie - 1)) * idx_sqrd_by_12;
+                    else if (a == ie - 2)
+                        *out = (U(ie - 6) - 6.0 * U(ie - 5) + 14.0 * U(ie - 4) -
+                                4.0 * U(ie - 3) - 15.0 * U(ie - 2) +
+                                10.0 * U(ie - 1)) * idx_sqrd_by_12;
+                    else if (a == ie - 1)
+                        *out = (-10.0 * U(ie - 6) + 61.0 * U(ie - 5) -
+                                156.0 * U(ie - 4) + 214.0 * U(ie - 3) -
+                                154.0 * U(ie - 2) + 45.0 * U(ie - 1)) *
+                               idx_sqrd_by_12;
+                }
+            }
+}
+
+void ko_deriv42(double* D, const double* u, double dx, const unsigned* sz,
+                unsigned bflag, int dir) {
+    const double pre_factor_6_dx = -1.0 / 64.0 / dx;
+    const double smr3 = 59.0 / 48.0 * 64 * dx;
+    const double smr2 = 43.0 / 48.0 * 64 * dx;
+    const double smr1 = 49.0 / 48.0 * 64 * dx;
+    const double spr3 = smr3, spr2 = smr2, spr1 = smr1;
+    const int nx = sz[0], ny = sz[1], nz = sz[2];
+    const int n = dir == 0 ? 1 : (dir == 1 ? nx : nx * ny);
+    const int ie = sz[dir] - 3;
+    const bool lo_face = bflag & (1u << (2 * dir));
+    const bool hi_face = bflag & (1u << (2 * dir + 1));
+    for (int k = 3; k < nz - 3; k++)
+        for (int j = 3; j < ny - 3; j++)
+            for (int i = 3; i < nx - 3; i++) {
+                const int pp = i + nx * (j + ny * k);
+                D[pp] = pre_factor_6_dx *
+                        (-u[pp - 3 * n] + 6.0 * u[pp - 2 * n] -
+                         15.0 * u[pp - n] + 20.0 * u[pp] - 15.0 * u[pp + n] +
+                         6.0 * u[pp + 2 * n] - u[pp + 3 * n]);
+            }
+    if (!lo_face && !hi_face) return;
+    for (int k = 3; k < nz - 3; k++)
+        for (int j = 3; j < ny - 3; j++)
+            for (int i = 3; i < nx - 3; i++) {
+                const int c[3] = {i, j, k};
+                const int a = c[dir];
+                const int base = i + nx * (j + ny * k) - a * n;
+                auto U = [&](int m) { return u[base + m * n]; };
+                double* out = &D[base + a * n];
+                if (lo_face) {
+                    if (a == 3)
+                        *out = (U(6) - 3.0 * U(5) + 3.0 * U(4) - U(3)) / smr3;
+                    else if (a == 4)
+                        *out = (U(7) - 6.0 * U(6) + 12.0 * U(5) - 10.0 * U(4) +
+                                3.0 * U(3)) / smr2;
+                    else if (a == 5)
+                        *out = (U(8) - 6.0 * U(7) + 15.0 * U(6) - 19.0 * U(5) +
+                                12.0 * U(4) - 3.0 * U(3)) / smr1;
+                }
+                if (hi_face) {
+                    if (a == ie - 3)
+                        *out = (U(ie - 6) - 6.0 * U(ie - 5) + 15.0 * U(ie - 4) -
+                                19.0 * U(ie - 3) + 12.0 * U(ie - 2) -
+                                3.0 * U(ie - 1)) / spr1;
+                    else if (a == ie - 2)
+                        *out = (U(ie - 5) - 6.0 * U(ie - 4) + 12.0 * U(ie - 3) -
+                                10.0 * U(ie - 2) + 3.0 * U(ie - 1)) / spr2;
+                    else if (a == ie - 1)
+                        *out = (U(ie - 4) - 3.0 * U(ie - 3) + 3.0 * U(ie - 2) -
+                                U(ie - 1)) / spr3;
+                }
+            }
+}
+
+// ---------------------------------------------------------------------------
+// Pointwise BSSN equations, standard puncture gauge with constant eta:
+// CodeGen/bssn.py:70-230 (bssn_puncture_gauge, unstaged) using the tensor
+// helpers of CodeGen/dendro.py (lie :222, DiDj :173, laplacian :266,
+// sqr :309, trace_free :323, Christoffels :395-483, compute_ricci :485-550).
+// ---------------------------------------------------------------------------
+
+// Vars whose second derivatives enter the equations (bssnrhs_derivs.h).
+const bool kNeedsD2[NVARS] = {
+    true,  true,  false, false, false, false, true,  true,  true,  false,
+    false, false, true,  true,  true,  true,  true,  true,  false, false,
+    false, false, false, false};
+
+struct Pt {
+    double u[NVARS];
+    double d1[NVARS][3];
+    double d2[NVARS][6];
+};
+
+void conformal_geometry(const Pt& P, double g[3][3], double ig[3][3],
+                        double C1[3][3][3], double C2[3][3][3],
+                        double CalGt[3]) {
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) g[i][j] = P.u[U_SYMGT0 + sym(i, j)];
+    // inverse metric through the adjugate (dendro.py:375-392, 'ADJ')
+    const double det = g[0][0] * (g[1][1] * g[2][2] - g[1][2] * g[2][1]) -
+                       g[0][1] * (g[1][0] * g[2][2] - g[1][2] * g[2][0]) +
+                       g[0][2] * (g[1][0] * g[2][1] - g[1][1] * g[2][0]);
+    ig[0][0] = (g[1][1] * g[2][2] - g[1][2] * g[2][1]) / det;
+    ig[0][1] = (g[0][2] * g[2][1] - g[0][1] * g[2][2]) / det;
+    ig[0][2] = (g[0][1] * g[1][2] - g[0][2] * g[1][1]) / det;
+    ig[1][1] = (g[0][0] * g[2][2] - g[0][2] * g[2][0]) / det;
+    ig[1][2] = (g[0][2] * g[1][0] - g[0][0] * g[1][2]) / det;
+    ig[2][2] = (g[0][0] * g[1][1] - g[0][1] * g[1][0]) / det;
+    ig[1][0] = ig[0][1];
+    ig[2][0] = ig[0][2];
+    ig[2][1] = ig[1][2];
+    // dg[i][j][k] = d_k g_ij
+    double dg[3][3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+            for (int k = 0; k < 3; k++) dg[i][j][k] = P.d1[U_SYMGT0 + sym(i, j)][k];
+    // C1[k][i][j] = 1/2 (d_j g_ki + d_i g_kj - d_k g_ij)   (dendro.py:413-417)
+    for (int k = 0; k < 3; k++)
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+                C1[k][i][j] = 0.5 * (dg[k][i][j] + dg[k][j][i] - dg[i][j][k]);
+    // C2[i][j][k] = ig[i][m] C1[m][j][k]                   (dendro.py:446-447)
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+            for (int k = 0; k < 3; k++) {
+                double s = 0.0;
+                for (int m = 0; m < 3; m++) s += ig[i][m] * C1[m][j][k];
+                C2[i][j][k] = s;
+            }
+    // CalGt[i] = ig[k][l] C2[i][k][l]                      (dendro.py:516)
+    for (int i = 0; i < 3; i++) {
+        double s = 0.0;
+        for (int k = 0; k < 3; k++)
+            for (int l = 0; l < 3; l++) s += ig[k][l] * C2[i][k][l];
+        CalGt[i] = s;
+    }
+}
+
+// Conformal Ricci tensor R = Rt + Rphi (dendro.py:485-550).
+void ricci(const Pt& P, const double g[3][3], const double ig[3][3],
+           const double C1[3][3][3], const double C2[3][3][3],
+           const double CalGt[3], double R[3][3]) {
+    const double chi = P.u[U_CHI];
+    const double* dchi = P.d1[U_CHI];
+    double ddchi[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) ddchi[i][j] = P.d2[U_CHI][sym(i, j)];
+    // dGt[k][j] = d_j Gt^k
+    double dGt[3][3];
+    for (int k = 0; k < 3; k++)
+        for (int j = 0; j < 3; j++) dGt[k][j] = P.d1[U_GT0 + k][j];
+    // sum_{kl} ig^{kl}(d_k d_l chi - 3/(2 chi) d_k chi d_l chi) - CalGt^m d_m chi
+    double trace_term = 0.0;
+    for (int k = 0; k < 3; k++)
+        for (int l = 0; l < 3; l++)
+            trace_term += ig[k][l] * (ddchi[k][l] -
+                                      3.0 / (2.0 * chi) * dchi[k] * dchi[l]);
+    for (int m = 0; m < 3; m++) trace_term -= CalGt[m] * dchi[m];
+
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            double rt = 0.0;
+            for (int l = 0; l < 3; l++)
+                for (int m = 0; m < 3; m++)
+                    rt += -0.5 * ig[l][m] * P.d2[U_SYMGT0 + sym(i, j)][sym(l, m)];
+            for (int k = 0; k < 3; k++)
+                rt += 0.5 * (g[k][i] * dGt[k][j] + g[k][j] * dGt[k][i]);
+            for (int k = 0; k < 3; k++)
+                rt += 0.5 * CalGt[k] * (C1[i][j][k] + C1[j][i][k]);
+            for (int k = 0; k < 3; k++)
+                for (int l = 0; l < 3; l++)
+                    for (int m = 0; m < 3; m++)
+                        rt += ig[l][m] * (C2[k][l][i] * C1[j][k][m] +
+                                          C2[k][l][j] * C1[i][k][m] +
+                                          C2[k][i][m] * C1[k][l][j]);
+            double s = ddchi[i][j];
+            for (int k = 0; k < 3; k++) s -= C2[k][j][i] * dchi[k];
+            double rphi = 1.0 / (2.0 * chi) * s -
+                          1.0 / (4.0 * chi * chi) * dchi[i] * dchi[j] +
+                          1.0 / (2.0 * chi) * g[i][j] * trace_term;
+            R[i][j] = rt + rphi;
+        }
+}
+
+void rhs_point(const Pt& P, const OrcParams* prm, double eta,
+               double out[NVARS]) {
+    const double alpha = P.u[U_ALPHA], chi = P.u[U_CHI], K = P.u[U_K];
+    const double l1 = prm->lambda[0], l2 = prm->lambda[1], l3 = prm->lambda[2],
+                 l4 = prm->lambda[3];
+    const double lf0 = prm->lambda_f[0], lf1 = prm->lambda_f[1];
+    double beta[3], B[3], A[3][3];
+    for (int i = 0; i < 3; i++) {
+        beta[i] = P.u[U_BETA0 + i];
+        B[i] = P.u[U_B0 + i];
+    }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) A[i][j] = P.u[U_SYMAT0 + sym(i, j)];
+    double g[3][3], ig[3][3], C1[3][3][3], C2[3][3][3], CalGt[3];
+    conformal_geometry(P, g, ig, C1, C2, CalGt);
+    double R[3][3];
+    ricci(P, g, ig, C1, C2, CalGt, R);
+
+    const double* dalpha = P.d1[U_ALPHA];
+    const double* dchi = P.d1[U_CHI];
+    const double* dK = P.d1[U_K];
+    double dbeta[3][3];  // dbeta[i][j] = d_j beta^i
+    double divb = 0.0;
+    for (int i = 0; i < 3; i++) {
+        for (int j = 0; j < 3; j++) dbeta[i][j] = P.d1[U_BETA0 + i][j];
+        divb += dbeta[i][i];
+    }
+    auto adv = [&](int v) {
+        return beta[0] * P.d1[v][0] + beta[1] * P.d1[v][1] + beta[2] * P.d1[v][2];
+    };
+
+    // C3 = C2 - 1/(2chi)(delta_ij d_k chi + delta_ik d_j chi - g_jk ig^im d_m chi)
+    // (dendro.py:452-483)
+    double igdchi[3];
+    for (int i = 0; i < 3; i++)
+        igdchi[i] = ig[i][0] * dchi[0] + ig[i][1] * dchi[1] + ig[i][2] * dchi[2];
+    double C3[3][3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+            for (int k = 0; k < 3; k++)
+                C3[i][j][k] = C2[i][j][k] -
+                              0.5 / chi * ((i == j ? dchi[k] : 0.0) +
+                                           (i == k ? dchi[j] : 0.0) -
+                                           g[j][k] * igdchi[i]);
+    // DiDj alpha (dendro.py:173-184)
+    double DDa[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            double s = P.d2[U_ALPHA][sym(i, j)];
+            for (int l = 0; l < 3; l++) s -= C3[l][i][j] * dalpha[l];
+            DDa[i][j] = s;
+        }
+    // A^{ij} (dendro.py:202-209) and A_ik ig^kl A_lj
+    double AUU[3][3], AikAkj[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            double s = 0.0, t = 0.0;
+            for (int k = 0; k < 3; k++)
+                for (int l = 0; l < 3; l++) {
+                    s += ig[i][k] * ig[j][l] * A[k][l];
+                    t += A[i][k] * ig[k][l] * A[l][j];
+                }
+            AUU[i][j] = s;
+            AikAkj[i][j] = t;
+        }
+    double sqrA = 0.0;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) sqrA += A[i][j] * AUU[i][j];
+
+    // a_rhs = l1 L_beta alpha - 2 alpha K                  (bssn.py:99)
+    out[U_ALPHA] = l1 * adv(U_ALPHA) - 2.0 * alpha * K;
+    // b_rhs = 3/4 (lf0 + lf1 alpha) B + l2 beta.grad beta   (bssn.py:101-104)
+    for (int i = 0; i < 3; i++)
+        out[U_BETA0 + i] = 0.75 * (lf0 + lf1 * alpha) * B[i] + l2 * adv(U_BETA0 + i);
+    // gt_rhs = L_beta gt (weight -2/3) - 2 alpha At           (bssn.py:106)
+    for (int i = 0; i < 3; i++)
+        for (int j = i; j < 3; j++) {
+            double s = 0.0;
+            for (int k = 0; k < 3; k++)
+                s += beta[k] * P.d1[U_SYMGT0 + sym(i, j)][k] + g[i][k] * dbeta[k][j] +
+                     g[k][j] * dbeta[k][i] - 2.0 / 3.0 * g[i][j] * dbeta[k][k];
+            out[U_SYMGT0 + sym(i, j)] = s - 2.0 * alpha * A[i][j];
+        }
+    // chi_rhs = L_beta chi (weight -2/3) + 2/3 chi alpha K    (bssn.py:108)
+    out[U_CHI] = adv(U_CHI) - 2.0 / 3.0 * chi * divb + 2.0 / 3.0 * chi * alpha * K;
+    // At_rhs = L_beta At + chi TF(alpha R - DiDj alpha) + alpha(K At - 2 A.A)
+    // (bssn.py:129-133)
+    double X[3][3], trX = 0.0;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) X[i][j] = alpha * R[i][j] - DDa[i][j];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) trX += ig[i][j] * X[i][j];
+    for (int i = 0; i < 3; i++)
+        for (int j = i; j < 3; j++) {
+            double s = 0.0;
+            for (int k = 0; k < 3; k++)
+                s += beta[k] * P.d1[U_SYMAT0 + sym(i, j)][k] + A[i][k] * dbeta[k][j] +
+                     A[k][j] * dbeta[k][i] - 2.0 / 3.0 * A[i][j] * dbeta[k][k];
+            out[U_SYMAT0 + sym(i, j)] = s + chi * (X[i][j] - g[i][j] * trX / 3.0) +
+                                        alpha * (K * A[i][j] - 2.0 * AikAkj[i][j]);
+        }
+    // K_rhs = L_beta K - laplacian(alpha) + alpha (K^2/3 + A_ij A^ij)
+    // (bssn.py:135-139); the full inverse metric is chi * ig.
+    double lap = 0.0;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) lap += chi * ig[i][j] * DDa[i][j];
+    out[U_K] = adv(U_K) - lap + alpha * (K * K / 3.0 + sqrA);
+    // Gt_rhs (bssn.py:143-205)
+    double Gt_rhs[3];
+    for (int i = 0; i < 3; i++) {
+        double s = adv(U_GT0 + i);
+        for (int j = 0; j < 3; j++) s -= CalGt[j] * dbeta[i][j];
+        s += 2.0 / 3.0 * CalGt[i] * divb;
+        for (int j = 0; j < 3; j++)
+            for (int k = 0; k < 3; k++)
+                s += ig[j][k] * P.d2[U_BETA0 + i][sym(j, k)] +
+                     ig[i][j] * P.d2[U_BETA0 + k][sym(j, k)] / 3.0;
+        for (int j = 0; j < 3; j++) s -= 2.0 * AUU[i][j] * dalpha[j];
+        for (int j = 0; j < 3; j++)
+            for (int k = 0; k < 3; k++) s += 2.0 * alpha * C2[i][j][k] * AUU[j][k];
+        for (int j = 0; j < 3; j++)
+            s -= alpha * (3.0 / chi * AUU[i][j] * dchi[j] +
+                          4.0 / 3.0 * ig[i][j] * dK[j]);
+        Gt_rhs[i] = s;
+        out[U_GT0 + i] = s;
+    }
+    // B_rhs = Gt_rhs - eta B + l3 beta.grad B - l4 beta.grad Gt (bssn.py:209-217)
+    for (int i = 0; i < 3; i++)
+        out[U_B0 + i] = Gt_rhs[i] - eta * B[i] + l3 * adv(U_B0 + i) -
+                        l4 * adv(U_GT0 + i);
+}
+
+// Sommerfeld falloff and asymptotic value per variable (rhs.cpp:275-327).
+const double kFalloff[NVARS] = {1, 1, 1, 2, 2, 2, 1, 1, 1, 1, 1, 1,
+                                1, 1, 1, 1, 1, 1, 2, 2, 2, 2, 2, 2};
+const double kAsymp[NVARS] = {1, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,
+                              1, 0, 0, 1, 0, 1, 0, 0, 0, 0, 0, 0};
+// CAKO gauge split (rhs.cpp:356-433): alpha, beta and B.
+const bool kGaugeVar[NVARS] = {true,  false, false, false, false, false,
+                               true,  true,  true,  true,  true,  true,
+                               false, false, false, false, false, false,
+                               false, false, false, false, false, false};
+
+constexpr int WS_D1 = 0;                 // 24*3 slabs
+constexpr int WS_D2 = NVARS * 3;         // 24*6 slabs (only 11 vars used)
+constexpr int WS_KO = NVARS * 3 + NVARS * 6;  // 24*3 slabs
+constexpr int WS_SLABS = WS_KO + NVARS * 3;
+
+// All derivatives of one variable in the reference's order: x, xx, y, yy,
+// z, zz, then the mixed ones y(x), z(x), z(y) (bssnrhs_derivs.h).
+void var_derivs(double* ws, int v, const double* u, const double h[3],
+                const unsigned* sz, unsigned bflag, bool second) {
+    const size_t n = (size_t)sz[0] * sz[1] * sz[2];
+    double* d1 = ws + (size_t)(WS_D1 + 3 * v) * n;
+    double* d2 = ws + (size_t)(WS_D2 + 6 * v) * n;
+    deriv644(d1 + 0 * n, u, h[0], sz, bflag, 0);
+    if (second) deriv644_2(d2 + 0 * n, u, h[0], sz, bflag, 0);
+    deriv644(d1 + 1 * n, u, h[1], sz, bflag, 1);
+    if (second) deriv644_2(d2 + 3 * n, u, h[1], sz, bflag, 1);
+    deriv644(d1 + 2 * n, u, h[2], sz, bflag, 2);
+    if (second) deriv644_2(d2 + 5 * n, u, h[2], sz, bflag, 2);
+    if (second) {
+        deriv644(d2 + 1 * n, d1 + 0 * n, h[1], sz, bflag, 1);  // xy
+        deriv644(d2 + 2 * n, d1 + 0 * n, h[2], sz, bflag, 2);  // xz
+        deriv644(d2 + 4 * n, d1 + 1 * n, h[2], sz, bflag, 2);  // yz
+    }
+}
+
+void gather_point(Pt& P, const double** u, unsigned offset, const double* ws,
+                  size_t n, size_t pp) {
+    for (int v = 0; v < NVARS; v++) {
+        P.u[v] = u[v][offset + pp];
+        for (int d = 0; d < 3; d++) P.d1[v][d] = ws[(WS_D1 + 3 * v + d) * n + pp];
+        if (kNeedsD2[v])
+            for (int d = 0; d < 6; d++) P.d2[v][d] = ws[(WS_D2 + 6 * v + d) * n + pp];
+        else
+            for (int d = 0; d < 6; d++) P.d2[v][d] = 0.0;
+    }
+}
+
+void bssnrhs_ws(double** rhs, const double** u, unsigned offset,
+                const double* pmin, const double* pmax, const unsigned* sz,
+                unsigned bflag, const OrcParams* prm, double* ws) {
+    const int nx = sz[0], ny = sz[1], nz = sz[2];
+    const size_t n = (size_t)nx * ny * nz;
+    const double h[3] = {(pmax[0] - pmin[0]) / (nx - 1),
+                         (pmax[1] - pmin[1]) / (ny - 1),
+                         (pmax[2] - pmin[2]) / (nz - 1)};
+    for (int v = 0; v < NVARS; v++)
+        var_derivs(ws, v, u[v] + offset, h, sz, bflag, kNeedsD2[v]);
+    Pt P;
+    double out[NVARS];
+    for (int k = 3; k < nz - 3; k++)
+        for (int j = 3; j < ny - 3; j++)
+            for (int i = 3; i < nx - 3; i++) {
+                const size_t pp = i + nx * (j + ny * (size_t)k);
+                const double x = pmin[0] + i * h[0];
+                const double y = pmin[1] + j * h[1];
+                const double z = pmin[2] + k * h[2];
+                const double r_coord = sqrt(x * x + y * y + z * z);
+                const double w = r_coord / prm->eta_width;
+                const double arg = -w * w * w * w;
+                const double eta =
+                    (prm->eta_central - prm->eta_outer) * exp(arg) + prm->eta_outer;
+                gather_point(P, u, offset, ws, n, pp);
+                rhs_point(P, prm, eta, out);
+                for (int v = 0; v < NVARS; v++) rhs[v][offset + pp] = out[v];
+            }
+    // Sommerfeld BC on boundary faces (rhs.cpp:272-330, 511-631): the value on
+    // a face point does not depend on which face is processed last.
+    if (bflag) {
+        for (int k = 3; k < nz - 3; k++)
+            for (int j = 3; j < ny - 3; j++)
+                for (int i = 3; i < nx - 3; i++) {
+                    const bool on_face =
+                        ((bflag & 1u) && i == 3) || ((bflag & 2u) && i == nx - 4) ||
+                        ((bflag & 4u) && j == 3) || ((bflag & 8u) && j == ny - 4) ||
+                        ((bflag & 16u) && k == 3) || ((bflag & 32u) && k == nz - 4);
+                    if (!on_face) continue;
+                    const size_t pp = i + nx * (j + ny * (size_t)k);
+                    const double x = pmin[0] + i * h[0];
+                    const double y = pmin[1] + j * h[1];
+                    const double z = pmin[2] + k * h[2];
+                    const double inv_r = 1.0 / sqrt(x * x + y * y + z * z);
+                    for (int v = 0; v < NVARS; v++) {
+                        const double* d1 = ws + (size_t)(WS_D1 + 3 * v) * n;
+                        rhs[v][offset + pp] =
+                            -inv_r * (x * d1[pp] + y * d1[n + pp] + z * d1[2 * n + pp] +
+                                      kFalloff[v] * (u[v][offset + pp] - kAsymp[v]));
+                    }
+                }
+    }
+    // KO dissipation (bssnrhs_ko_derivs.h, rhs.cpp:338-492)
+    for (int v = 0; v < NVARS; v++) {
+        double* ko = ws + (size_t)(WS_KO + 3 * v) * n;
+        for (int d = 0; d < 3; d++) ko_deriv42(ko + d * n, u[v] + offset, h[d], sz, bflag, d);
+    }
+    for (int k = 3; k < nz - 3; k++)
+        for (int j = 3; j < ny - 3; j++)
+            for (int i = 3; i < nx - 3; i++) {
+                const size_t pp = i + nx * (j + ny * (size_t)k);
+                for (int v = 0; v < NVARS; v++) {
+                    const double* ko = ws + (size_t)(WS_KO + 3 * v) * n;
+                    double s = prm->ko_sigma;
+                    if (prm->cako_enabled) {
+                        const double sc = sqrt(u[U_CHI][offset + pp]);
+                        s = kGaugeVar[v] ? sc * prm->eps_cako_gauge
+                                         : sc * prm->eps_cako_other;
+                    }
+                    rhs[v][offset + pp] += s * (ko[pp] + ko[n + pp] + ko[2 * n + pp]);
+                }
+            }
+}
+
+// Constraint enforcement on one node, restated from
+// BSSN_GR/include/bssn_constraints.h:15-172 with the same arithmetic order;
+// returns 1 if the node violated a check (the reference exits there).
+int enforce_node(double** u, int64_t node, double chi_floor) {
+    const double one_third = 1.0 / 3.0;
+    double gtd[3][3], Atd[3][3];
+    int bad = 0;
+    gtd[0][0] = u[U_SYMGT0][node]; gtd[0][1] = u[U_SYMGT1][node];
+    gtd[0][2] = u[U_SYMGT2][node]; gtd[1][1] = u[U_SYMGT3][node];
+    gtd[1][2] = u[U_SYMGT4][node]; gtd[2][2] = u[U_SYMGT5][node];
+    gtd[1][0] = gtd[0][1]; gtd[2][0] = gtd[0][2]; gtd[2][1] = gtd[1][2];
+    Atd[0][0] = u[U_SYMAT0][node]; Atd[0][1] = u[U_SYMAT1][node];
+    Atd[0][2] = u[U_SYMAT2][node]; Atd[1][1] = u[U_SYMAT3][node];
+    Atd[1][2] = u[U_SYMAT4][node]; Atd[2][2] = u[U_SYMAT5][node];
+    Atd[1][0] = Atd[0][1]; Atd[2][0] = Atd[0][2]; Atd[2][1] = Atd[1][2];
+    double det_gtd = gtd[0][0] * (gtd[1][1] * gtd[2][2] - gtd[1][2] * gtd[1][2]) -
+                     gtd[0][1] * gtd[0][1] * gtd[2][2] +
+                     2.0 * gtd[0][1] * gtd[0][2] * gtd[1][2] -
+                     gtd[0][2] * gtd[0][2] * gtd[1][1];
+    if (det_gtd < 0.0) {
+        bad = 1;
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) gtd[a][b] = a == b ? 1.0 : 0.0;
+        det_gtd = 1.0;
+    }
+    const double det_gtd_to_neg_third = 1.0 / pow(det_gtd, one_third);
+    for (int j = 0; j < 3; j++)
+        for (int i = 0; i < 3; i++) gtd[i][j] *= det_gtd_to_neg_third;
+    det_gtd = gtd[0][0] * (gtd[1][1] * gtd[2][2] - gtd[1][2] * gtd[1][2]) -
+              gtd[0][1] * gtd[0][1] * gtd[2][2] +
+              2.0 * gtd[0][1] * gtd[0][2] * gtd[1][2] -
+              gtd[0][2] * gtd[0][2] * gtd[1][1];
+    if (fabs(det_gtd - 1.0) > 1.0e-6) bad = 1;
+    double gtu[3][3];
+    const double idet_gtd = 1.0 / det_gtd;
+    gtu[0][0] = idet_gtd * (gtd[1][1] * gtd[2][2] - gtd[1][2] * gtd[1][2]);
+    gtu[0][1] = idet_gtd * (-gtd[0][1] * gtd[2][2] + gtd[0][2] * gtd[1][2]);
+    gtu[0][2] = idet_gtd * (gtd[0][1] * gtd[1][2] - gtd[0][2] * gtd[1][1]);
+    gtu[1][1] = idet_gtd * (gtd[0][0] * gtd[2][2] - gtd[0][2] * gtd[0][2]);
+    gtu[1][2] = idet_gtd * (-gtd[0][0] * gtd[1][2] + gtd[0][1] * gtd[0][2]);
+    gtu[2][2] = idet_gtd * (gtd[0][0] * gtd[1][1] - gtd[0][1] * gtd[0][1]);
+    const double one_third_trace_Atd =
+        one_third *
+        (Atd[0][0] * gtu[0][0] + Atd[1][1] * gtu[1][1] + Atd[2][2] * gtu[2][2] +
+         2.0 * (Atd[0][1] * gtu[0][1] + Atd[0][2] * gtu[0][2] + Atd[1][2] * gtu[1][2]));
+    Atd[0][0] -= one_third_trace_Atd * gtd[0][0];
+    Atd[0][1] -= one_third_trace_Atd * gtd[0][1];
+    Atd[0][2] -= one_third_trace_Atd * gtd[0][2];
+    Atd[1][1] -= one_third_trace_Atd * gtd[1][1];
+    Atd[1][2] -= one_third_trace_Atd * gtd[1][2];
+    Atd[2][2] -= one_third_trace_Atd * gtd[2][2];
+    const double tr_A =
+        Atd[0][0] * gtu[0][0] + Atd[1][1] * gtu[1][1] + Atd[2][2] * gtu[2][2] +
+        2.0 * (Atd[0][1] * gtu[0][1] + Atd[0][2] * gtu[0][2] + Atd[1][2] * gtu[1][2]);
+    if (fabs(tr_A) > 1.0e-6) bad = 1;
+    u[U_SYMAT0][node] = Atd[0][0]; u[U_SYMAT1][node] = Atd[0][1];
+    u[U_SYMAT2][node] = Atd[0][2]; u[U_SYMAT3][node] = Atd[1][1];
+    u[U_SYMAT4][node] = Atd[1][2]; u[U_SYMAT5][node] = Atd[2][2];
+    u[U_SYMGT0][node] = gtd[0][0]; u[U_SYMGT1][node] = gtd[0][1];
+    u[U_SYMGT2][node] = gtd[0][2]; u[U_SYMGT3][node] = gtd[1][1];
+    u[U_SYMGT4][node] = gtd[1][2]; u[U_SYMGT5][node] = gtd[2][2];
+    if (u[U_CHI][node] < chi_floor) u[U_CHI][node] = chi_floor;
+    u[U_ALPHA][node] = std::max(u[U_ALPHA][node], chi_floor);
+    return bad;
+}
+
+uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_deriv644_x(double* D, const double* u, double h, const unsigned* sz, unsigned b) { deriv644(D, u, h, sz, b, 0); }
+void orc_deriv644_y(double* D, const double* u, double h, const unsigned* sz, unsigned b) { deriv644(D, u, h, sz, b, 1); }
+void orc_deriv644_z(double* D, const double* u, double h, const unsigned* sz, unsigned b) { deriv644(D, u, h, sz, b, 2); }
+void orc_deriv644_xx(double* D, const double* u, double h, const unsigned* sz, unsigned b) { deriv644_2(D, u, h, sz, b, 0); }
+void orc_deriv644_yy(double* D, const double* u, double h, const unsigned* sz, unsigned b) { deriv644_2(D, u, h, sz, b, 1); }
+void orc_deriv644_zz(double* D, const double* u, double h, const unsigned* sz, unsigned b) { deriv644_2(D, u, h, sz, b, 2); }
+void orc_ko_deriv42_x(double* D, const double* u, double h, const unsigned* sz, unsigned b) { ko_deriv42(D, u, h, sz, b, 0); }
+void orc_ko_deriv42_y(double* D, const double* u, double h, const unsigned* sz, unsigned b) { ko_deriv42(D, u, h, sz, b, 1); }
+void orc_ko_deriv42_z(double* D, const double* u, double h, const unsigned* sz, unsigned b) { ko_deriv42(D, u, h, sz, b, 2); }
+
+void orc_bssnrhs(double** rhs, const double** u, unsigned offset,
+                 const double* pmin, const double* pmax, const unsigned* sz,
+                 unsigned bflag, const OrcParams* prm, double* ws) {
+    std::vector<double> own;
+    if (!ws) {
+        own.resize((size_t)WS_SLABS * sz[0] * sz[1] * sz[2]);
+        ws = own.data();
+    }
+    bssnrhs_ws(rhs, u, offset, pmin, pmax, sz, bflag, prm, ws);
+}
+
+void orc_bssnRHS(double** rhs, const double** u, const OrcBlock* blks,
+                 int nblk, const OrcParams* prm, int nthreads) {
+    int maxs = 0;
+    for (int b = 0; b < nblk; b++) maxs = std::max(maxs, (int)blks[b].sz);
+    const size_t wsz = (size_t)WS_SLABS * maxs * maxs * maxs;
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel num_threads(nthreads)
+    {
+        std::vector<double> ws(wsz);
+#pragma omp for schedule(dynamic, 1)
+        for (int b = 0; b < nblk; b++) {
+            const unsigned sz[3] = {(unsigned)blks[b].sz, (unsigned)blks[b].sz,
+                                    (unsigned)blks[b].sz};
+            bssnrhs_ws(rhs, u, (unsigned)blks[b].offset, blks[b].ptmin,
+                       blks[b].ptmax, sz, blks[b].bflag, prm, ws.data());
+        }
+    }
+}
+
+int64_t orc_enforce(double** u, int64_t n, double chi_floor) {
+    int64_t bad = 0;
+#pragma omp parallel for reduction(+ : bad)
+    for (int64_t node = 0; node < n; node++) bad += enforce_node(u, node, chi_floor);
+    return bad;
+}
+
+void orc_initial_data(double** u, const int32_t* G, const double* xmin,
+                      double h, const double* bh, double m1, double m2,
+                      double chi_floor, double eps, uint64_t seed) {
+    const int64_t N = (int64_t)G[0] * G[1] * G[2];
+#pragma omp parallel for
+    for (int64_t node = 0; node < N; node++) {
+        const int64_t gx = node % G[0];
+        const int64_t gy = (node / G[0]) % G[1];
+        const int64_t gz = node / ((int64_t)G[0] * G[1]);
+        const double x = xmin[0] + gx * h, y = xmin[1] + gy * h, z = xmin[2] + gz * h;
+        // Brill-Lindquist conformal factor (grUtils.cpp:1033-1035,1082-1100)
+        const double x1 = x - bh[0], y1 = y - bh[1], z1 = z - bh[2];
+        const double x2 = x - bh[3], y2 = y - bh[4], z2 = z - bh[5];
+        const double rv1 = sqrt(x1 * x1 + y1 * y1 + z1 * z1);
+        const double rv2 = sqrt(x2 * x2 + y2 * y2 + z2 * z2);
+        double psi = 1.0 + m1 / (2.0 * rv1);
+        psi = psi + m2 / (2.0 * rv2);
+        double v[NVARS] = {0};
+        v[U_ALPHA] = std::max(1.0 / (psi * psi), chi_floor);
+        v[U_CHI] = 1.0 / pow(psi, 4);
+        if (v[U_CHI] < chi_floor) v[U_CHI] = chi_floor;
+        v[U_SYMGT0] = v[U_SYMGT3] = v[U_SYMGT5] = 1.0;
+        for (int k = 0; k < NVARS; k++) {
+            const uint64_t r = mix64(seed + 0x9E3779B97F4A7C15ULL *
+                                                (uint64_t)(k * N + node + 1));
+            const double unit = (double)(r >> 11) * (1.0 / 9007199254740992.0);
+            u[k][node] = v[k] + eps * (2.0 * unit - 1.0);
+        }
+    }
+    orc_enforce(u, N, chi_floor);
+}
+
+static inline bool in_grid(const int64_t g[3], const int32_t* G) {
+    return g[0] >= 0 && g[1] >= 0 && g[2] >= 0 && g[0] < G[0] && g[1] < G[1] &&
+           g[2] < G[2];
+}
+
+void orc_unzip_map(int64_t* map, const OrcBlock* blks, int nblk,
+                   const int32_t* G) {
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int b = 0; b < nblk; b++) {
+        const int s = blks[b].sz;
+        for (int k = 0; k < s; k++)
+            for (int j = 0; j < s; j++)
+                for (int i = 0; i < s; i++) {
+                    const int64_t g[3] = {blks[b].g0[0] + i - 3, blks[b].g0[1] + j - 3,
+                                          blks[b].g0[2] + k - 3};
+                    const int64_t p = blks[b].offset + i + (int64_t)s * (j + (int64_t)s * k);
+                    map[p] = in_grid(g, G) ? g[0] + (int64_t)G[0] * (g[1] + (int64_t)G[1] * g[2]) : -1;
+                }
+    }
+}
+
+void orc_unzip(double** unzip, const double** zip, const OrcBlock* blks,
+               int nblk, const int32_t* G, int nvars) {
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int b = 0; b < nblk; b++) {
+        const int s = blks[b].sz;
+        for (int k = 0; k < s; k++)
+            for (int j = 0; j < s; j++)
+                for (int i = 0; i < s; i++) {
+                    const int64_t g[3] = {blks[b].g0[0] + i - 3, blks[b].g0[1] + j - 3,
+                                          blks[b].g0[2] + k - 3};
+                    const int64_t p = blks[b].offset + i + (int64_t)s * (j + (int64_t)s * k);
+                    const bool in = in_grid(g, G);
+                    const int64_t node = in ? g[0] + (int64_t)G[0] * (g[1] + (int64_t)G[1] * g[2]) : 0;
+                    for (int v = 0; v < nvars; v++) unzip[v][p] = in ? zip[v][node] : 0.0;
+                }
+    }
+}
+
+void orc_zip(double** zip, const double** unzip, const OrcBlock* blks,
+             int nblk, const int32_t* G, int nvars) {
+    const int M[3] = {(G[0] - 1) / 6, (G[1] - 1) / 6, (G[2] - 1) / 6};
+    std::vector<int> owner((size_t)M[0] * M[1] * M[2], -1);
+    for (int b = 0; b < nblk; b++) {
+        const int w = (blks[b].sz - 7) / 6;  // octants per side
+        const int o0[3] = {blks[b].g0[0] / 6, blks[b].g0[1] / 6, blks[b].g0[2] / 6};
+        for (int c = 0; c < w; c++)
+            for (int bb = 0; bb < w; bb++)
+                for (int a = 0; a < w; a++)
+                    owner[(o0[0] + a) + (size_t)M[0] * ((o0[1] + bb) + (size_t)M[1] * (o0[2] + c))] = b;
+    }
+    const int64_t N = (int64_t)G[0] * G[1] * G[2];
+#pragma omp parallel for
+    for (int64_t node = 0; node < N; node++) {
+        const int64_t g[3] = {node % G[0], (node / G[0]) % G[1], node / ((int64_t)G[0] * G[1])};
+        int64_t o[3];
+        for (int d = 0; d < 3; d++) o[d] = std::min<int64_t>(g[d] / 6, M[d] - 1);
+        const int b = owner[o[0] + (size_t)M[0] * (o[1] + (size_t)M[1] * o[2])];
+        const int s = blks[b].sz;
+        const int64_t i = g[0] - blks[b].g0[0] + 3, j = g[1] - blks[b].g0[1] + 3,
+                      k = g[2] - blks[b].g0[2] + 3;
+        const int64_t p = blks[b].offset + i + s * (j + s * k);
+        for (int v = 0; v < nvars; v++) zip[v][node] = unzip[v][p];
+    }
+}
+
+int64_t orc_rk4_step(double** u, const OrcBlock* blks, int nblk,
+                     const int32_t* G, int64_t n_unzip, double dt,
+                     const OrcParams* prm, double chi_floor,
+                     int enforce_stages, int nthreads) {
+    static const double RK4_C[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+    static const double RK4_U[4] = {0.0, 1.0 / 2.0, 1.0 / 2.0, 1.0};
+    const int64_t N = (int64_t)G[0] * G[1] * G[2];
+    std::vector<double> prev(NVARS * N), im(NVARS * N), kst(4 * NVARS * N);
+    std::vector<double> uz(NVARS * n_unzip, 0.0), rz(NVARS * n_unzip, 0.0);
+    double *pu[NVARS], *pim[NVARS], *puz[NVARS], *prz[NVARS];
+    for (int v = 0; v < NVARS; v++) {
+        std::memcpy(&prev[v * N], u[v], N * sizeof(double));
+        pu[v] = u[v];
+        pim[v] = &im[v * N];
+        puz[v] = &uz[v * n_unzip];
+        prz[v] = &rz[v * n_unzip];
+    }
+    int64_t bad = 0;
+    for (int stage = 0; stage < 4; stage++) {
+        double** cur = stage == 0 ? pu : pim;
+        orc_unzip(puz, (const double**)cur, blks, nblk, G, NVARS);
+        orc_bssnRHS(prz, (const double**)puz, blks, nblk, prm, nthreads);
+        double* ks[NVARS];
+        for (int v = 0; v < NVARS; v++) ks[v] = &kst[(stage * NVARS + v) * N];
+        orc_zip(ks, (const double**)prz, blks, nblk, G, NVARS);
+        if (stage < 3) {
+#pragma omp parallel for reduction(+ : bad)
+            for (int64_t node = 0; node < N; node++) {
+                for (int v = 0; v < NVARS; v++) {
+                    pim[v][node] = prev[v * N + node];
+                    pim[v][node] += (RK4_U[stage + 1] * dt * ks[v][node]);
+                }
+                if (enforce_stages) bad += enforce_node(pim, node, chi_floor);
+            }
+        }
+    }
+#pragma omp parallel for reduction(+ : bad)
+    for (int64_t node = 0; node < N; node++) {
+        for (int v = 0; v < NVARS; v++) {
+            pu[v][node] = prev[v * N + node];
+            for (int s = 0; s < 4; s++)
+                pu[v][node] += (RK4_C[s] * dt * kst[(s * NVARS + v) * N + node]);
+        }
+        bad += enforce_node(pu, node, chi_floor);
+    }
+    return bad;
+}
+
+// Hamiltonian and momentum constraints (CodeGen/constraints.py:250-283):
+//   ham   = chi ig^jk R_jk - A_ij A^ij + 2/3 K^2
+//   mom_i = ig^jk (d_k A_ij - C2^m_ki A_jm) - Gt^j A_ij
+//           - 3/2 ig^jk A_ki d_j chi / chi - 2/3 d_i K
+void orc_physical_constraints(double** cons, const double** u, unsigned offset,
+                              const double* pmin, const double* pmax,
+                              const unsigned* sz, unsigned bflag, double* ws) {
+    std::vector<double> own;
+    const int nx = sz[0], ny = sz[1], nz = sz[2];
+    const size_t n = (size_t)nx * ny * nz;
+    if (!ws) {
+        own.resize((size_t)WS_SLABS * n);
+        ws = own.data();
+    }
+    const double h[3] = {(pmax[0] - pmin[0]) / (nx - 1),
+                         (pmax[1] - pmin[1]) / (ny - 1),
+                         (pmax[2] - pmin[2]) / (nz - 1)};
+    for (int v = 0; v < NVARS; v++)
+        var_derivs(ws, v, u[v] + offset, h, sz, bflag, kNeedsD2[v]);
+    Pt P;
+    for (int k = 3; k < nz - 3; k++)
+        for (int j = 3; j < ny - 3; j++)
+            for (int i = 3; i < nx - 3; i++) {
+                const size_t pp = i + nx * (j + ny * (size_t)k);
+                gather_point(P, u, offset, ws, n, pp);
+                double g[3][3], ig[3][3], C1[3][3][3], C2[3][3][3], CalGt[3], R[3][3];
+                conformal_geometry(P, g, ig, C1, C2, CalGt);
+                ricci(P, g, ig, C1, C2, CalGt, R);
+                const double chi = P.u[U_CHI], K = P.u[U_K];
+                double A[3][3];
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) A[a][b] = P.u[U_SYMAT0 + sym(a, b)];
+                double ham = 0.0, sqrA = 0.0;
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) {
+                        ham += chi * ig[a][b] * R[a][b];
+                        double s = 0.0;
+                        for (int c = 0; c < 3; c++)
+                            for (int d = 0; d < 3; d++) s += ig[a][c] * ig[b][d] * A[c][d];
+                        sqrA += A[a][b] * s;
+                    }
+                cons[0][offset + pp] = ham - sqrA + 2.0 / 3.0 * K * K;
+                for (int a = 0; a < 3; a++) {
+                    double m = 0.0;
+                    for (int b = 0; b < 3; b++)
+                        for (int c = 0; c < 3; c++) {
+                            double t = P.d1[U_SYMAT0 + sym(a, b)][c];
+                            for (int q = 0; q < 3; q++) t -= C2[q][c][a] * A[b][q];
+                            m += ig[b][c] * t;
+                        }
+                    for (int b = 0; b < 3; b++) m -= P.u[U_GT0 + b] * A[a][b];
+                    for (int b = 0; b < 3; b++)
+                        for (int c = 0; c < 3; c++)
+                            m -= 1.5 * ig[b][c] * A[c][a] * P.d1[U_CHI][b] / chi;
+                    m -= 2.0 / 3.0 * P.d1[U_K][a];
+                    cons[1 + a][offset + pp] = m;
+                }
+            }
+}
+
+}  // extern "C"

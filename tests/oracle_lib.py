@@ -1,0 +1,159 @@
+"""ctypes access to the CPU oracles (test infrastructure only).
+
+liboracle.so  -- this repository's CPU restatement (oracle/bssn_oracle.cpp)
+libbssn_ref.so -- the reference's own stencils and generated equations,
+                  compiled from the reference sources in place (oracle/_ref)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle.so")
+REF_SO = os.path.join(ORACLE_DIR, "_ref", "libbssn_ref.so")
+NVARS = 24
+_dp = C.POINTER(C.c_double)
+_PA = C.c_void_p * NVARS
+
+
+def build_oracle():
+    if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < os.path.getmtime(
+            os.path.join(ORACLE_DIR, "bssn_oracle.cpp")):
+        subprocess.run(["make", "-C", ORACLE_DIR, "liboracle.so"], check=True,
+                       stdout=subprocess.DEVNULL)
+
+
+class OrcParams(C.Structure):
+    _fields_ = [("ko_sigma", C.c_double), ("lambda_", C.c_uint * 4),
+                ("lambda_f", C.c_double * 2), ("eta_central", C.c_double),
+                ("eta_outer", C.c_double), ("eta_width", C.c_double),
+                ("cako_enabled", C.c_int), ("eps_cako_gauge", C.c_double),
+                ("eps_cako_other", C.c_double)]
+
+
+def params(ko_sigma=0.4, eta=2.0, cako=False):
+    return OrcParams(ko_sigma, (1, 1, 1, 1), (1.0, 0.0), eta, eta, 40.0, int(cako), 0.99, 0.3)
+
+
+def P(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def rows(a):
+    """24 row pointers of a (24, n) float64 array."""
+    assert a.flags.c_contiguous and a.shape[0] == NVARS
+    return _PA(*[a.ctypes.data + v * a.shape[1] * 8 for v in range(NVARS)])
+
+
+class Oracle:
+    STENCILS = ["deriv644_x", "deriv644_y", "deriv644_z", "deriv644_xx", "deriv644_yy",
+                "deriv644_zz", "ko_deriv42_x", "ko_deriv42_y", "ko_deriv42_z"]
+
+    def __init__(self, path=ORACLE_SO, prefix="orc_"):
+        self.lib = C.CDLL(path)
+        self.prefix = prefix
+
+    def stencil(self, kind, u, h, sz, bflag):
+        out = np.zeros(int(np.prod(sz)))
+        s = (C.c_uint * 3)(*sz)
+        getattr(self.lib, self.prefix + self.STENCILS[kind])(P(out), P(u), C.c_double(h), s, C.c_uint(bflag))
+        return out
+
+    def bssnrhs(self, U, offset, pmin, pmax, side, bflag, prm):
+        """RHS of one block; U is (24, n) with the block at `offset`."""
+        R = np.zeros_like(U)
+        n = side ** 3
+        ws = np.zeros(288 * n) if self.prefix == "orc_" else np.zeros(138 * n)
+        pm = np.ascontiguousarray(pmin, dtype=np.float64)
+        px = np.ascontiguousarray(pmax, dtype=np.float64)
+        sz = (C.c_uint * 3)(side, side, side)
+        getattr(self.lib, self.prefix + "bssnrhs")(rows(R), rows(U), C.c_uint(offset), P(pm), P(px), sz,
+                                                   C.c_uint(bflag), C.byref(prm), P(ws))
+        return R
+
+
+def oracle():
+    build_oracle()
+    return Oracle()
+
+
+def reference():
+    if not os.path.exists(REF_SO):
+        return None
+    return Oracle(REF_SO, prefix="ref_")
+
+
+def blocks_array(spec):
+    """Mesh blocks as a ctypes array usable by the oracle (same layout as
+    OrcBlock)."""
+    return spec.blocks
+
+
+class MeshOracle:
+    """Oracle-side unzip / zip / RHS over a block list."""
+
+    def __init__(self, spec, lib=None):
+        self.spec = spec
+        self.lib = (lib or oracle()).lib
+        self.G = (C.c_int32 * 3)(*spec.G)
+
+    def unzip(self, Z, nvars=NVARS):
+        U = np.zeros((NVARS, self.spec.n_unzip))
+        self.lib.orc_unzip(rows(U), rows(Z), self.spec.blocks, self.spec.nblocks, self.G, nvars)
+        return U
+
+    def zip(self, U, nvars=NVARS):
+        Z = np.zeros((NVARS, self.spec.n_nodes))
+        self.lib.orc_zip(rows(Z), rows(U), self.spec.blocks, self.spec.nblocks, self.G, nvars)
+        return Z
+
+    def unzip_map(self):
+        m = np.zeros(self.spec.n_unzip, dtype=np.int64)
+        self.lib.orc_unzip_map(m.ctypes.data_as(C.c_void_p), self.spec.blocks, self.spec.nblocks, self.G)
+        return m
+
+    def rhs(self, U, prm, nthreads=0):
+        R = np.zeros_like(U)
+        self.lib.orc_bssnRHS(rows(R), rows(U), self.spec.blocks, self.spec.nblocks, C.byref(prm), nthreads)
+        return R
+
+    def initial_data(self, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0), m1=0.5, m2=0.5, chi_floor=1e-4,
+                     eps=1e-8, seed=20261203):
+        Z = np.zeros((NVARS, self.spec.n_nodes))
+        xm = (C.c_double * 3)(self.spec.xmin, self.spec.xmin, self.spec.xmin)
+        b = (C.c_double * 6)(*bh)
+        self.lib.orc_initial_data(rows(Z), self.G, xm, C.c_double(self.spec.h), b, C.c_double(m1),
+                                  C.c_double(m2), C.c_double(chi_floor), C.c_double(eps),
+                                  C.c_uint64(seed))
+        return Z
+
+    def rk4_step(self, Z, dt, prm, chi_floor=1e-4, enforce_stages=True, nthreads=0):
+        self.lib.orc_rk4_step.restype = C.c_int64
+        return self.lib.orc_rk4_step(rows(Z), self.spec.blocks, self.spec.nblocks, self.G,
+                                     C.c_int64(self.spec.n_unzip), C.c_double(dt), C.byref(prm),
+                                     C.c_double(chi_floor), int(enforce_stages), nthreads)
+
+
+def interior_mask(spec):
+    """Boolean mask over the unzipped vector selecting block interiors."""
+    m = np.zeros(spec.n_unzip, dtype=bool)
+    for b in range(spec.nblocks):
+        blk = spec.blocks[b]
+        s = int(blk.sz)
+        cube = np.zeros((s, s, s), dtype=bool)
+        cube[3:-3, 3:-3, 3:-3] = True
+        m[int(blk.offset):int(blk.offset) + s ** 3] = cube.ravel()
+    return m
+
+
+def rel_err(ref, got):
+    """Per-variable ||got - ref||_inf / ||ref||_inf (0 where ref is 0)."""
+    num = np.abs(got - ref).max(axis=1)
+    den = np.abs(ref).max(axis=1)
+    return np.where(den > 0, num / np.where(den > 0, den, 1), num)

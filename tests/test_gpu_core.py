@@ -1,0 +1,209 @@
+"""GPU parity of the stencils, the fused right-hand side, the ghost fill and
+the RK4 stage algebra against the CPU oracle (test infrastructure) on the
+same seeded inputs."""
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def B():
+    import bssn_b200
+    return bssn_b200
+
+
+@pytest.fixture(scope="module")
+def O():
+    return ol.oracle()
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("side", [13, 19, 31])
+def test_stencils_bit_exact(B, O, side):
+    rng = np.random.default_rng(side)
+    u = rng.standard_normal(side ** 3)
+    du = dev(u)
+    for kind in range(9):
+        for bflag in (0, 1, 2, 4, 8, 16, 32, 63, 21, 42):
+            ref = O.stencil(kind, u, 0.37, (side, side, side), bflag)
+            D = torch.zeros(side ** 3, dtype=torch.float64, device="cuda")
+            B.deriv(kind, D, du, 0.37, (side, side, side), bflag)
+            torch.cuda.synchronize()
+            got = D.cpu().numpy()
+            assert np.array_equal(ref.view(np.uint64), got.view(np.uint64)), (kind, bflag)
+
+
+def bl_block(side, bflag_seed, h=1.0 / 3.0, shift=(0.0, -1.0, -1.0), noise=1e-6, seed=0):
+    rng = np.random.default_rng(seed)
+    n = side ** 3
+    pmin = np.array(shift) - 3 * h
+    pmax = pmin + (side - 1) * h
+    x = pmin[0] + np.arange(side) * h
+    y = pmin[1] + np.arange(side) * h
+    z = pmin[2] + np.arange(side) * h
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    r1 = np.sqrt((X - 1.0) ** 2 + Y ** 2 + Z ** 2)
+    r2 = np.sqrt((X + 1.0) ** 2 + Y ** 2 + Z ** 2)
+    with np.errstate(divide="ignore"):
+        psi = 1 + 0.5 / (2 * r1) + 0.5 / (2 * r2)
+    U = np.zeros((24, n))
+    U[0] = np.maximum(1 / psi ** 2, 1e-4).ravel()
+    U[1] = np.maximum(1 / psi ** 4, 1e-4).ravel()
+    U[12] = U[15] = U[17] = 1.0
+    U += noise * rng.uniform(-1, 1, U.shape)
+    return U, pmin, pmax
+
+
+@pytest.mark.parametrize("side", [13, 19, 31, 55])
+@pytest.mark.parametrize("bflag", [0, 1 | 4 | 16, 2 | 8 | 32, 63])
+def test_bssnrhs_single_block(B, O, side, bflag):
+    U, pmin, pmax = bl_block(side, bflag, h=2.0 / (side - 7), seed=side + bflag)
+    prm = ol.params()
+    ref = O.bssnrhs(U, 0, pmin, pmax, side, bflag, prm)
+    dU = dev(U)
+    dR = torch.zeros_like(dU)
+    B.bssnrhs_block(dR, dU, 0, pmin, pmax, side, bflag, B.default_params())
+    torch.cuda.synchronize()
+    got = dR.cpu().numpy()
+    sl = np.s_[:, 3:-3, 3:-3, 3:-3]
+    r = ref.reshape(24, side, side, side)[sl].reshape(24, -1)
+    g = got.reshape(24, side, side, side)[sl].reshape(24, -1)
+    err = ol.rel_err(r, g)
+    assert np.all(np.isfinite(g))
+    assert err.max() <= 1e-12, (err.max(), int(err.argmax()))
+
+
+def test_mesh_unzip_zip_bit_exact(B, O):
+    spec = B.generate_mesh(1, (2, 1, 1), seed=7)
+    mo = ol.MeshOracle(spec, O)
+    rng = np.random.default_rng(3)
+    Z = rng.standard_normal((24, spec.n_nodes))
+    m = B.Mesh(spec)
+    dZ = dev(Z)
+    dU = torch.full((24, spec.n_unzip), np.nan, dtype=torch.float64, device="cuda")
+    m.unzip(dU, dZ)
+    torch.cuda.synchronize()
+    ref_u = mo.unzip(Z)
+    mask = np.ones(spec.n_unzip, dtype=bool)
+    # points between blocks (offset rounding) are not part of any block
+    valid = np.zeros(spec.n_unzip, dtype=bool)
+    for b in range(spec.nblocks):
+        blk = spec.blocks[b]
+        valid[int(blk.offset):int(blk.offset) + int(blk.sz) ** 3] = True
+    got_u = dU.cpu().numpy()
+    assert np.array_equal(ref_u[:, valid].view(np.uint64), got_u[:, valid].view(np.uint64))
+    # zip back the unzipped data: identity on every node
+    dZ2 = torch.zeros_like(dZ)
+    m.zip(dZ2, dU)
+    torch.cuda.synchronize()
+    assert np.array_equal(dZ2.cpu().numpy().view(np.uint64), Z.view(np.uint64))
+    assert np.array_equal(mo.zip(ref_u).view(np.uint64), Z.view(np.uint64))
+    del mask
+
+
+def test_mesh_rhs_mixed_sizes(B, O):
+    spec = B.generate_mesh(1, (1, 1, 1), seed=11)
+    assert len(set(spec.sides.tolist())) >= 2
+    mo = ol.MeshOracle(spec, O)
+    Z = mo.initial_data()
+    Uz = mo.unzip(Z)
+    prm = ol.params()
+    ref = mo.rhs(Uz, prm)
+    m = B.Mesh(spec)
+    dU = dev(Uz)
+    for t in range(len(B.tiles())):
+        dR = torch.zeros_like(dU)
+        m.rhs(dR, dU, B.default_params(), tile=t)
+        torch.cuda.synchronize()
+        mask = ol.interior_mask(spec)
+        got = dR.cpu().numpy()[:, mask]
+        r = ref[:, mask]
+        err = ol.rel_err(r, got)
+        assert err.max() <= 1e-12, (t, err.max(), int(err.argmax()))
+
+
+def test_initial_data_config1(B, O):
+    spec = B.generate_mesh(0, (8, 8, 8))
+    mo = ol.MeshOracle(spec, O)
+    Zref = mo.initial_data()
+    dZ = torch.zeros((24, spec.n_nodes), dtype=torch.float64, device="cuda")
+    B.initial_data(dZ, spec)
+    torch.cuda.synchronize()
+    err0 = ol.rel_err(Zref, dZ.cpu().numpy())
+    assert err0.max() <= 1e-14, err0.max()
+
+
+@pytest.mark.parametrize("path", ["python", "batched", "graph", "per_block"])
+@pytest.mark.parametrize("mesh", ["uniform", "mix"])
+def test_rk4_step_vs_oracle(B, O, path, mesh):
+    """One RK4 step from the same state on the GPU paths and on the CPU
+    oracle (rkBSSN.cpp:764-860 restated); states compared per variable
+    relative to the variable's largest magnitude."""
+    spec = B.generate_mesh(0, (4, 4, 4)) if mesh == "uniform" else B.generate_mesh(1, (1, 1, 1), seed=5)
+    mo = ol.MeshOracle(spec, O)
+    Z0 = mo.initial_data(eps=1e-8)
+    dt = 0.25 * spec.h
+    Z1 = Z0.copy()
+    bad = mo.rk4_step(Z1, dt, ol.params())
+    assert bad == 0
+    m = B.Mesh(spec)
+    dZ = dev(Z0)
+    prm = B.default_params()
+    if path == "python":
+        B.PlainRK4(m, prm).step(dZ, dt)
+    else:
+        flags = B.PLAN_ENFORCE_STAGES | {"batched": 0, "graph": B.PLAN_GRAPH,
+                                         "per_block": B.PLAN_PER_BLOCK}[path]
+        plan = B.RK4Plan(m, prm, flags)
+        plan.step(dZ, dt)
+        torch.cuda.synchronize()
+        assert plan.violations() == 0
+        plan.close()
+    torch.cuda.synchronize()
+    got = dZ.cpu().numpy()
+    err = ol.rel_err(Z1, got)
+    assert err.max() <= 1e-13, (err.max(), int(err.argmax()))
+    # the increment itself, for the variables whose RHS is not noise-level
+    for v in (0, 1, 2):
+        d_ref = Z1[v] - Z0[v]
+        d_got = got[v] - Z0[v]
+        assert np.abs(d_got - d_ref).max() <= 1e-10 * np.abs(d_ref).max(), v
+
+
+def test_graph_replay_matches_eager(B):
+    spec = B.generate_mesh(1, (1, 1, 1), seed=9)
+    m = B.Mesh(spec)
+    U = torch.zeros((24, spec.n_nodes), dtype=torch.float64, device="cuda")
+    B.initial_data(U, spec)
+    V = U.clone()
+    dt = 0.25 * spec.h
+    prm = B.default_params()
+    pg = B.RK4Plan(m, prm, B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
+    pe = B.RK4Plan(m, prm, B.PLAN_ENFORCE_STAGES)
+    for _ in range(3):
+        pg.step(U, dt)
+        pe.step(V, dt)
+    torch.cuda.synchronize()
+    assert torch.equal(U, V)
+
+
+def test_autotune_picks_a_tile_per_bucket(B):
+    spec = B.generate_mesh(1, (1, 1, 1), seed=13)
+    m = B.Mesh(spec)
+    U = torch.zeros((24, spec.n_nodes), dtype=torch.float64, device="cuda")
+    B.initial_data(U, spec)
+    plan = B.RK4Plan(m, B.default_params())
+    chosen, table = plan.autotune(U, reps=1)
+    nt = len(B.tiles())
+    assert set(chosen) == set(spec.sides.tolist())
+    for side, t in chosen.items():
+        assert 0 <= t < nt
+        assert table[side][t] == min(table[side])
