@@ -216,6 +216,8 @@ int bssn_rk4_plan_destroy(bssn_rk4_plan plan) {
 
 int bssn_tile_count(void) { return bssn::tile_count(); }
 
+long bssn_tile_selfcheck(int tile) { return bssn::tile_selfcheck(tile); }
+
 int bssn_tile_info(int tile, int info[4]) {
     if (!info) return BSSN_EINVAL;
     return bssn::tile_info(tile, info);

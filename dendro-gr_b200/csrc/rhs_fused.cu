@@ -194,8 +194,13 @@ __device__ __forceinline__ void rhs_brick(const RhsArgs& A, const BssnBlockDesc&
     };
 
     // zone of this thread
-    const int tx = tid % BX, ty = (tid / BX) % BY, tz = tid / (BX * BY);
-    const bool active = tid < Bk::NZ && tx < e[0] && ty < e[1] && tz < e[2];
+    // threads past the brick's zone count take zone (0,0,0) so that every
+    // shared-memory read they make stays inside the tile; they store nothing
+    const bool in_brick = tid < Bk::NZ;
+    const int tx = in_brick ? tid % BX : 0;
+    const int ty = in_brick ? (tid / BX) % BY : 0;
+    const int tz = in_brick ? tid / (BX * BY) : 0;
+    const bool active = in_brick && tx < e[0] && ty < e[1] && tz < e[2];
     ZoneCtx zc;
     zc.s = s;
     zc.bflag = bflag;
@@ -228,10 +233,14 @@ __device__ __forceinline__ void rhs_brick(const RhsArgs& A, const BssnBlockDesc&
         if (active) A.rhs.p[v][pidx] = val;
     };
 
-    const double x = blk.ptmin[0] + za0 * hh[0];
-    const double y = blk.ptmin[1] + za1 * hh[1];
-    const double z = blk.ptmin[2] + za2 * hh[2];
-    const double r_coord = sqrt(x * x + y * y + z * z);
+    // coordinates and radius rounded exactly as the reference computes them
+    // (pmin + i*h, no contraction), so a face point at the origin gives the
+    // reference's infinite 1/r
+    const double x = __dadd_rn(blk.ptmin[0], __dmul_rn((double)za0, hh[0]));
+    const double y = __dadd_rn(blk.ptmin[1], __dmul_rn((double)za1, hh[1]));
+    const double z = __dadd_rn(blk.ptmin[2], __dmul_rn((double)za2, hh[2]));
+    const double r_coord =
+        __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
     const double eta = [&] {
         const double w = r_coord / A.prm.eta_width;
         const double arg = -w * w * w * w;
@@ -254,8 +263,14 @@ __device__ __forceinline__ void rhs_brick(const RhsArgs& A, const BssnBlockDesc&
     };
     // final value of variable v: (boundary face ? Sommerfeld : equations) + sigma KO
     auto finish = [&](int v, double eq, const double d1[3], double f, double ko) {
-        const double bc = -inv_r * (x * d1[0] + y * d1[1] + z * d1[2] + falloff(v) * (f - asymptotic(v)));
-        return (onface ? bc : eq) + sigma(v) * ko;
+        double val = eq;
+        if (onface) {
+            // -inv_r (x dxf + y dyf + z dzf + falloff (f - f_inf)), rhs.cpp:542-547
+            double t = __dadd_rn(__dadd_rn(__dmul_rn(x, d1[0]), __dmul_rn(y, d1[1])), __dmul_rn(z, d1[2]));
+            t = __dadd_rn(t, __dmul_rn(falloff(v), __dsub_rn(f, asymptotic(v))));
+            val = __dmul_rn(-inv_r, t);
+        }
+        return val + sigma(v) * ko;
     };
     const double l1 = A.prm.lambda[0], l2 = A.prm.lambda[1], l3 = A.prm.lambda[2],
                  l4 = A.prm.lambda[3];
@@ -650,6 +665,78 @@ int prepare_all_tiles() {
         if (st) return st;
     }
     return 0;
+}
+
+// Host replay of the brick kernel's shared-memory indexing: for a tile
+// shape, every brick extent the splitter can produce (3..B per axis), every
+// block-face combination and every thread, check that each tile and mixed-
+// scratch element a thread reads lies inside its array.  Returns the number
+// of out-of-range reads (0 = the kernel's smem accesses are all in bounds).
+namespace {
+// positions along one axis read by the d1/d2/KO stencils at coordinate a
+void read_span(int a, int s, bool lo, bool hi, int& pmin, int& pmax) {
+    const int ie = s - 3;
+    if (lo && a <= 5) {
+        pmin = 3;
+        pmax = 8;
+        return;
+    }
+    if (hi && a >= ie - 3) {
+        pmin = ie - 6;
+        pmax = ie - 1;
+        return;
+    }
+    pmin = a - 3;
+    pmax = a + 3;
+}
+
+template <int BX, int BY, int BZ>
+long check_tile_shape() {
+    using Bk = Brick<BX, BY, BZ>;
+    const int B[3] = {BX, BY, BZ};
+    const int T[3] = {Bk::TX, Bk::TY, Bk::TZ};
+    long bad = 0;
+    for (int e0 = 3; e0 <= BX; e0++)
+        for (int e1 = 3; e1 <= BY; e1++)
+            for (int e2 = 3; e2 <= BZ; e2++)
+                for (int face = 0; face < 4; face++) {
+                    // brick at the lower faces (o = 0) or upper faces of a 55 block
+                    const int s = 55;
+                    const int e[3] = {e0, e1, e2};
+                    int o[3];
+                    for (int d = 0; d < 3; d++) o[d] = (face & 1) ? (s - 6 - e[d]) : 0;
+                    const bool blo = (face & 2) != 0, bhi = (face & 2) != 0;
+                    for (int tid = 0; tid < Bk::THREADS; tid++) {
+                        const bool in_brick = tid < Bk::NZ;
+                        const int t3[3] = {in_brick ? tid % BX : 0,
+                                           in_brick ? (tid / BX) % BY : 0,
+                                           in_brick ? tid / (BX * BY) : 0};
+                        const bool active = in_brick && t3[0] < e[0] && t3[1] < e[1] && t3[2] < e[2];
+                        for (int d = 0; d < 3; d++) {
+                            const int a = o[d] + PW + t3[d];
+                            int pmin, pmax;
+                            read_span(a, s, blo, bhi, pmin, pmax);
+                            // tile coordinate = position - o: inside the array
+                            // for every thread (tile and mixed scratch share the
+                            // extent T along the axis), inside the staged region
+                            // [0, e+6) for threads that own a zone
+                            if (pmin - o[d] < 0 || pmax - o[d] >= T[d]) bad++;
+                            if (active && pmax - o[d] >= e[d] + 2 * PW) bad++;
+                            if (t3[d] >= B[d]) bad++;
+                        }
+                    }
+                }
+    return bad;
+}
+}  // namespace
+
+long tile_selfcheck(int tile) {
+    switch (tile) {
+        case 0: return check_tile_shape<8, 8, 4>();
+        case 1: return check_tile_shape<7, 7, 4>();
+        case 2: return check_tile_shape<8, 4, 4>();
+        default: return -1;
+    }
 }
 
 int tile_count() {

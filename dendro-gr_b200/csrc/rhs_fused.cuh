@@ -23,6 +23,7 @@ struct BrickTask {
 };
 
 int tile_count();
+long tile_selfcheck(int tile);
 int prepare_all_tiles();
 int tile_info(int tile, int info[4]);
 void build_tasks(const BssnBlockDesc* blocks, int nblocks, int tile,

@@ -227,6 +227,10 @@ int bssn_mesh_generate(int mode, const int32_t dims[3], const double p[4],
  * threads) for the fused RHS kernel. */
 int bssn_tile_count(void);
 int bssn_tile_info(int tile, int info[4]);
+/* Host-only replay of a tile's shared-memory indexing over every brick
+ * extent, face case and thread: the number of out-of-range reads (0 when
+ * every access is in bounds), or -1 for an unknown tile. */
+long bssn_tile_selfcheck(int tile);
 
 const char* bssn_version(void);
 

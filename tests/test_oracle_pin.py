@@ -1,0 +1,99 @@
+"""CPU tests: the oracle (this repository's CPU restatement) pinned against
+the reference's own compiled arithmetic and against the committed golden
+fixtures generated from it."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden", "rhs_golden.json")
+
+
+@pytest.fixture(scope="module")
+def O():
+    return ol.oracle()
+
+
+@pytest.fixture(scope="module")
+def REF():
+    r = ol.reference()
+    if r is None:
+        pytest.skip("oracle/_ref/libbssn_ref.so not built (reference tree absent)")
+    return r
+
+
+@pytest.mark.parametrize("side", [13, 19])
+def test_stencils_bit_exact_vs_reference(O, REF, side):
+    rng = np.random.default_rng(side)
+    u = 1.0 + 1e-8 * rng.standard_normal(side ** 3)   # O(1) mean, tiny noise
+    for kind in range(9):
+        for bflag in range(64):
+            a = REF.stencil(kind, u, 0.21, (side, side, side), bflag)
+            b = O.stencil(kind, u, 0.21, (side, side, side), bflag)
+            assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), (kind, bflag)
+
+
+def _load_golden():
+    with open(GOLD) as f:
+        return json.load(f)["cases"]
+
+
+@pytest.mark.parametrize("ci", range(5))
+def test_rhs_vs_golden(O, ci):
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import make_golden as mg
+    c = _load_golden()[ci]
+    U, pmin, pmax = mg.golden_input(c["side"], c["h"], tuple(c["shift"]), c["noise"], c["seed"])
+    R = O.bssnrhs(U, 0, pmin, pmax, c["side"], c["bflag"], ol.params())
+    Ri = mg.interior(R, c["side"])
+    for v in range(24):
+        mx = float.fromhex(c["maxnorm"][v])
+        got_mx = np.abs(Ri[v]).max()
+        assert abs(got_mx - mx) <= 1e-12 * mx, (v, got_mx, mx)
+        l2 = float.fromhex(c["l2"][v])
+        assert abs(np.sqrt((Ri[v] ** 2).sum()) - l2) <= 1e-12 * l2, v
+        for p, hv in zip(c["points"], c["values"][v]):
+            ref = float.fromhex(hv)
+            assert abs(R[v, p] - ref) <= 1e-12 * mx, (v, p)
+
+
+@pytest.mark.parametrize("side,bflag", [(13, 0), (13, 63), (19, 21), (31, 42)])
+def test_rhs_vs_reference_live(O, REF, side, bflag):
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import make_golden as mg
+    U, pmin, pmax = mg.golden_input(side, 2.0 / (side - 7), (0.1, -1.1, -0.95), 1e-8, side + bflag)
+    a = mg.interior(REF.bssnrhs(U, 0, pmin, pmax, side, bflag, ol.params()), side)
+    b = mg.interior(O.bssnrhs(U, 0, pmin, pmax, side, bflag, ol.params()), side)
+    err = ol.rel_err(a, b)
+    assert err.max() <= 1e-12, (err.max(), int(err.argmax()))
+
+
+def test_flat_space_rhs_is_zero(O):
+    side = 13
+    U = np.zeros((24, side ** 3))
+    U[[0, 1, 12, 15, 17]] = 1.0
+    pmin = np.array([2.0, 2.0, 2.0])
+    R = O.bssnrhs(U, 0, pmin, pmin + 12 * 0.1, side, 0, ol.params())
+    assert np.abs(R).max() == 0.0
+
+
+def test_enforce_invariants(O):
+    rng = np.random.default_rng(0)
+    n = 1000
+    Z = np.zeros((24, n))
+    Z[[12, 15, 17]] = 1.0
+    Z += 1e-3 * rng.standard_normal(Z.shape)
+    Z[[0, 1]] = rng.uniform(1e-6, 1.0, (2, n))
+    O.lib.orc_enforce.restype = ol.C.c_int64
+    bad = O.lib.orc_enforce(ol.rows(Z), ol.C.c_int64(n), ol.C.c_double(1e-4))
+    assert bad == 0
+    g = Z[12:18]
+    det = g[0] * (g[3] * g[5] - g[4] ** 2) - g[1] ** 2 * g[5] + 2 * g[1] * g[2] * g[4] - g[2] ** 2 * g[3]
+    assert np.abs(det - 1).max() < 1e-6
+    assert Z[0].min() >= 1e-4 and Z[1].min() >= 1e-4
