@@ -76,6 +76,10 @@ def _sig():
     lib.bssn_rk4_plan_tile.argtypes = [vp, i]
     lib.bssn_rk4_plan_violations.argtypes = [vp, P(i)]
     lib.bssn_rk4_plan_destroy.argtypes = [vp]
+    lib.bssn_constraints_f64.argtypes = [vp, vp, vp, vp]
+    lib.bssn_constraint_norms_f64.argtypes = [vp, vp, i, P(d), d, P(d), P(d), vp, vp]
+    lib.bssn_rk4_plan_time_rhs.argtypes = [vp, i, vp, P(C.c_float)]
+    lib.bssn_fp64_probe.argtypes = [vp, i, vp, P(d)]
     lib.bssn_tile_count.argtypes = []
     lib.bssn_tile_info.argtypes = [i, P(i)]
 
@@ -307,3 +311,27 @@ class RK4Plan:
             self.close()
         except Exception:
             pass
+
+
+def _cons_ptrs(cons):
+    assert cons.is_cuda and cons.dtype.is_floating_point and cons.is_contiguous()
+    return (C.c_void_p * 4)(*[cons.data_ptr() + c * cons.shape[1] * 8 for c in range(4)])
+
+
+def constraints(mesh: Mesh, cons, unz, stream=None):
+    """ham, mom0..2 of the padded stage state `unz` into the zipped (4, n)
+    tensor `cons` (owned nodes)."""
+    check(lib.bssn_constraints_f64(mesh.h, ptrs(unz), _cons_ptrs(cons), stream_ptr(stream)), "constraints")
+
+
+def constraint_norms(mesh: Mesh, cons, norms, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0),
+                     radii=(0.5, 0.5), ncons=4, stream=None):
+    """Masked L2 norms sqrt(sum c^2 / N) of the 4 zipped constraint fields
+    into the CUDA tensor `norms` (>= ncons doubles)."""
+    spec = mesh.spec
+    xm = (C.c_double * 3)(spec.xmin, spec.xmin, spec.xmin)
+    b = (C.c_double * 6)(*bh)
+    r = (C.c_double * 2)(*radii)
+    check(lib.bssn_constraint_norms_f64(mesh.h, _cons_ptrs(cons), ncons, xm, spec.h, b, r,
+                                        C.c_void_p(norms.data_ptr()), stream_ptr(stream)),
+          "constraint_norms")

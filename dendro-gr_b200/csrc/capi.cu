@@ -10,6 +10,7 @@
 #include "kernels.cuh"
 #include "mesh.h"
 #include "plan.h"
+#include "constraints.h"
 #include "rhs_fused.cuh"
 
 struct bssn_mesh_s {
@@ -212,6 +213,35 @@ int bssn_rk4_plan_destroy(bssn_rk4_plan plan) {
     bssn::plan_destroy(plan->p);
     delete plan;
     return 0;
+}
+
+int bssn_constraints_f64(bssn_mesh mesh, const double* const* unzip_dev, double* const* cons_dev,
+                         bssn_stream_t stream) {
+    if (!mesh || !unzip_dev || !cons_dev) return BSSN_EINVAL;
+    for (int c = 0; c < 4; c++)
+        if (!cons_dev[c]) return BSSN_EINVAL;
+    for (int v = 0; v < bssn::NVARS; v++)
+        if (!unzip_dev[v]) return BSSN_EINVAL;
+    return bssn::launch_constraints(mesh->st, unzip_dev, cons_dev, S(stream));
+}
+
+int bssn_constraint_norms_f64(bssn_mesh mesh, const double* const* cons_dev, int ncons,
+                              const double xmin[3], double h, const double bh[6],
+                              const double radii[2], double* norms_dev, bssn_stream_t stream) {
+    if (!mesh || !cons_dev || ncons < 1 || ncons > 4 || !xmin || !bh || !radii || !norms_dev)
+        return BSSN_EINVAL;
+    for (int c = 0; c < ncons; c++)
+        if (!cons_dev[c]) return BSSN_EINVAL;
+    // the reduction's partial sums live in a device buffer owned by the mesh
+    // handle, allocated on the first call (5 doubles per reduction CTA)
+    bssn::MeshState* m = mesh->st;
+    const int npartial = bssn::kNormPartials;
+    if (!m->d_partial) {
+        if (cudaMalloc((void**)&m->d_partial, sizeof(double) * 5 * npartial) != cudaSuccess)
+            return BSSN_ENOMEM;
+    }
+    return bssn::launch_l2_norms(m, cons_dev, ncons, xmin, h, bh, radii, m->d_partial, npartial,
+                                 norms_dev, S(stream));
 }
 
 int bssn_tile_count(void) { return bssn::tile_count(); }

@@ -126,6 +126,7 @@ void mesh_destroy(MeshState* m) {
     cudaFree(m->d_blocks);
     cudaFree(m->d_pad_chunks);
     cudaFree(m->d_int_chunks);
+    cudaFree(m->d_partial);
     for (auto& t : m->tasks) cudaFree(t.second.first);
     delete m;
 }

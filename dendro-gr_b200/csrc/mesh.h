@@ -31,6 +31,8 @@ struct MeshState {
     // brick task lists per (tile shape, block side; side 0 = all blocks):
     // (device pointer, count)
     std::map<std::pair<int, int>, std::pair<BrickTask*, int>> tasks;
+    // partial sums of the constraint-norm reduction (allocated on first use)
+    double* d_partial = nullptr;
     // autotuned tile per padded side (0 = not tuned)
     std::map<int, int> tuned;
 };

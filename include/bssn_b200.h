@@ -168,6 +168,24 @@ int bssn_initial_data_f64(double* const* u_dev, const int32_t G[3],
                           uint64_t seed, bssn_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* Hamiltonian and momentum constraints (CodeGen/constraints.py:250-283,
+ * per block as physical_constraints, BSSN_GR/src/physcon.cpp:12-89) from
+ * the padded stage state of every block, written to the zipped node arrays
+ * cons_dev[0..3] = ham, mom0, mom1, mom2 (owned nodes only). */
+int bssn_constraints_f64(bssn_mesh mesh, const double* const* unzip_dev,
+                         double* const* cons_dev, bssn_stream_t stream);
+/* Masked L2 norms sqrt(sum c^2 / N) over the zipped nodes farther than
+ * radii[0] / radii[1] from the punctures bh = {x1,y1,z1,x2,y2,z2}
+ * (computeConstraintL2Norm, BSSN_GR/include/grUtils.tcc:36-134); node
+ * coordinates xmin + g*h.  Writes ncons (<= 4) doubles to norms_dev.  The
+ * reduction's partial sums live in a buffer the mesh handle allocates on
+ * the first call. */
+int bssn_constraint_norms_f64(bssn_mesh mesh, const double* const* cons_dev,
+                              int ncons, const double xmin[3], double h,
+                              const double bh[6], const double radii[2],
+                              double* norms_dev, bssn_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
 /* One whole RK4 step as a plan over a mesh (the reference's per-step
  * sequence rkBSSN.cpp:764-860: per stage unzip -> bssnRHS -> zip -> stage
  * update).  The plan owns its scratch buffers (two padded 24-variable

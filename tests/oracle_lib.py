@@ -157,3 +157,35 @@ def rel_err(ref, got):
     num = np.abs(got - ref).max(axis=1)
     den = np.abs(ref).max(axis=1)
     return np.where(den > 0, num / np.where(den > 0, den, 1), num)
+
+
+def oracle_constraints(spec, Uz, lib=None):
+    """ham, mom0..2 on every zipped node from the padded state Uz, by
+    orc_physical_constraints per block (physcon.cpp:12-89 restated) and the
+    oracle's zip."""
+    O = lib or oracle()
+    Cz = np.zeros((NVARS, spec.n_unzip))
+    ws = np.zeros(288 * 55 ** 3)
+    for b in range(spec.nblocks):
+        blk = spec.blocks[b]
+        s = int(blk.sz)
+        pm = np.array(blk.ptmin[:])
+        px = np.array(blk.ptmax[:])
+        sz = (C.c_uint * 3)(s, s, s)
+        O.lib.orc_physical_constraints(rows(Cz), rows(Uz), C.c_uint(int(blk.offset)), P(pm), P(px), sz,
+                                       C.c_uint(int(blk.bflag)), P(ws))
+    return MeshOracle(spec, O).zip(Cz, nvars=4)[:4]
+
+
+def l2_norms(spec, Cn, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0), radii=(0.5, 0.5)):
+    """sqrt(sum c^2 / N) over nodes outside both puncture radii
+    (grUtils.tcc:36-134)."""
+    G = spec.G
+    g = np.arange(spec.n_nodes)
+    x = spec.xmin + (g % G[0]) * spec.h
+    y = spec.xmin + ((g // G[0]) % G[1]) * spec.h
+    z = spec.xmin + (g // (G[0] * G[1])) * spec.h
+    d1 = np.sqrt((x - bh[0]) ** 2 + (y - bh[1]) ** 2 + (z - bh[2]) ** 2)
+    d2 = np.sqrt((x - bh[3]) ** 2 + (y - bh[4]) ** 2 + (z - bh[5]) ** 2)
+    keep = ~((d1 < radii[0]) | (d2 < radii[1]))
+    return np.sqrt((Cn[:, keep] ** 2).sum(axis=1) / keep.sum())

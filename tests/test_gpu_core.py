@@ -207,3 +207,23 @@ def test_autotune_picks_a_tile_per_bucket(B):
     for side, t in chosen.items():
         assert 0 <= t < nt
         assert table[side][t] == min(table[side])
+
+
+@pytest.mark.parametrize("mesh", ["uniform", "mix"])
+def test_constraints_and_norms_vs_oracle(B, O, mesh):
+    spec = B.generate_mesh(0, (4, 4, 4)) if mesh == "uniform" else B.generate_mesh(1, (1, 1, 1), seed=5)
+    mo = ol.MeshOracle(spec, O)
+    Z = mo.initial_data(eps=1e-6)
+    Uz = mo.unzip(Z)
+    ref = ol.oracle_constraints(spec, Uz, O)
+    m = B.Mesh(spec)
+    cons = torch.zeros((4, spec.n_nodes), dtype=torch.float64, device="cuda")
+    B.constraints(m, cons, dev(Uz))
+    norms = torch.zeros(4, dtype=torch.float64, device="cuda")
+    B.constraint_norms(m, cons, norms)
+    torch.cuda.synchronize()
+    got = cons.cpu().numpy()
+    err = ol.rel_err(ref, got)
+    assert err.max() <= 1e-12, err
+    nref = ol.l2_norms(spec, ref)
+    assert np.allclose(norms.cpu().numpy(), nref, rtol=1e-12, atol=0), (norms, nref)

@@ -97,3 +97,25 @@ def test_enforce_invariants(O):
     det = g[0] * (g[3] * g[5] - g[4] ** 2) - g[1] ** 2 * g[5] + 2 * g[1] * g[2] * g[4] - g[2] ** 2 * g[3]
     assert np.abs(det - 1).max() < 1e-6
     assert Z[0].min() >= 1e-4 and Z[1].min() >= 1e-4
+
+
+@pytest.mark.parametrize("side,bflag", [(13, 0), (19, 63), (31, 21)])
+def test_constraints_vs_reference_live(O, REF, side, bflag):
+    """Hamiltonian / momentum constraints of the restatement against the
+    reference's own physconeqs.cpp (physcon.cpp:12-89 control flow)."""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import make_golden as mg
+    U, pmin, pmax = mg.golden_input(side, 2.0 / (side - 7), (0.1, -1.1, -0.95), 1e-6, 40 + side)
+    n = side ** 3
+    sz = (ol.C.c_uint * 3)(side, side, side)
+    cr = np.zeros((24, n))
+    co = np.zeros((24, n))
+    REF.lib.ref_physical_constraints(ol.rows(cr), ol.rows(U), ol.C.c_uint(0), ol.P(pmin), ol.P(pmax), sz,
+                                     ol.C.c_uint(bflag), ol.P(np.zeros(138 * n)))
+    O.lib.orc_physical_constraints(ol.rows(co), ol.rows(U), ol.C.c_uint(0), ol.P(pmin), ol.P(pmax), sz,
+                                   ol.C.c_uint(bflag), ol.P(np.zeros(288 * n)))
+    a = mg.interior(cr, side)[:4]
+    b = mg.interior(co, side)[:4]
+    err = np.abs(a - b).max(axis=1) / np.abs(a).max(axis=1)
+    assert err.max() <= 1e-12, err
