@@ -89,14 +89,9 @@ __device__ __forceinline__ double Dmix(const Blk& b, const double* u, int inner,
                b.bflag & (1u << (2 * outer + 1)), b.cf[outer]);
 }
 
-__global__ void constraints_kernel(ConstVars P, MutVars out, const BssnBlockDesc* __restrict__ blocks,
-                                   const Chunk* __restrict__ chunks, int gx, int gy, int gz) {
-    const Chunk ck = chunks[blockIdx.x];
-    const BssnBlockDesc bd = blocks[ck.blk];
+__device__ void constraints_node(const ConstVars& P, const MutVars& out, const BssnBlockDesc& bd,
+                                 int64_t q, int gx, int gy, int gz) {
     const int s = bd.sz, N = s - 6;
-    const int64_t n = (int64_t)N * N * N;
-    const int64_t q = ck.start + threadIdx.x;
-    if (q >= n || threadIdx.x >= ck.count) return;
     const int i = (int)(q % N), j = (int)((q / N) % N), k = (int)(q / ((int64_t)N * N));
     const int64_t x = bd.g0[0] + i, y = bd.g0[1] + j, z = bd.g0[2] + k;
     const bool own = (i < N - 1 || x == gx - 1) && (j < N - 1 || y == gy - 1) &&
@@ -244,12 +239,24 @@ __global__ void constraints_kernel(ConstVars P, MutVars out, const BssnBlockDesc
     }
 }
 
+// One CTA per chunk of up to 1024 interior points of a block, 256 threads
+// striding over it (the node function needs up to 255 registers).
+__global__ void __launch_bounds__(256) constraints_kernel(ConstVars P, MutVars out,
+                                                          const BssnBlockDesc* __restrict__ blocks,
+                                                          const Chunk* __restrict__ chunks, int gx,
+                                                          int gy, int gz) {
+    const Chunk ck = chunks[blockIdx.x];
+    const BssnBlockDesc bd = blocks[ck.blk];
+    for (int r = threadIdx.x; r < ck.count; r += blockDim.x)
+        constraints_node(P, out, bd, ck.start + r, gx, gy, gz);
+}
+
 }  // namespace
 
 // Per-CTA partial sums of c^2 and node counts over nodes outside both
 // puncture radii, then one thread sums the partials in CTA order: a fixed
 // grid and a fixed order, so the result is deterministic.
-__global__ void l2_partial_kernel(ConstVars C, int nc, int64_t n, int gx, int gy, double x0,
+__global__ void __launch_bounds__(256) l2_partial_kernel(ConstVars C, int nc, int64_t n, int gx, int gy, double x0,
                                   double y0, double z0, double h, double b0, double b1, double b2,
                                   double b3, double b4, double b5, double r1, double r2,
                                   double* partial) {
@@ -296,7 +303,7 @@ int launch_constraints(const MeshState* m, const double* const* P, double* const
     for (int v = 0; v < NVARS; v++) p.p[v] = P[v];
     for (int c = 0; c < 4; c++) o.p[c] = out[c];
     if (m->n_int_chunks == 0) return 0;
-    constraints_kernel<<<m->n_int_chunks, 1024, 0, s>>>(p, o, m->d_blocks, m->d_int_chunks,
+    constraints_kernel<<<m->n_int_chunks, 256, 0, s>>>(p, o, m->d_blocks, m->d_int_chunks,
                                                         m->G[0], m->G[1], m->G[2]);
     return cuda_status(cudaGetLastError());
 }

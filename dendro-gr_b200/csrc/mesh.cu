@@ -27,7 +27,7 @@ constexpr int CHUNK = 1024;
 // Ghost fill.  One CTA per chunk of consecutive padded points of one block:
 // consecutive threads read consecutive nodes of a grid row and write
 // consecutive padded points.
-__global__ void unzip_kernel(MutVars unz, ConstVars zip, int nvars,
+__global__ void __launch_bounds__(CHUNK) unzip_kernel(MutVars unz, ConstVars zip, int nvars,
                              const BssnBlockDesc* __restrict__ blocks,
                              const Chunk* __restrict__ chunks, int gx, int gy,
                              int gz) {
@@ -47,7 +47,7 @@ __global__ void unzip_kernel(MutVars unz, ConstVars zip, int nvars,
 // Gather back.  Each interior node of a block is written only if the block
 // owns it: a node on the block's upper face belongs to the next block unless
 // the face lies on the grid's upper boundary.
-__global__ void zip_kernel(MutVars zip, ConstVars unz, int nvars,
+__global__ void __launch_bounds__(CHUNK) zip_kernel(MutVars zip, ConstVars unz, int nvars,
                            const BssnBlockDesc* __restrict__ blocks,
                            const Chunk* __restrict__ chunks, int gx, int gy,
                            int gz) {

@@ -264,7 +264,7 @@ int plan_time_rhs(Plan* p, int reps, cudaStream_t s, float* ms) {
 
 namespace {
 // FP64 multiply-add throughput probe: 8 independent chains per thread.
-__global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
+__global__ void __launch_bounds__(256) fp64_probe_kernel(double* out, int iters, double a, double b) {
     double x[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) x[q] = threadIdx.x * 1e-3 + q;

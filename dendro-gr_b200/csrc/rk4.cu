@@ -77,7 +77,7 @@ __device__ int enforce_regs(double v[NVARS], double chi_floor) {
 
 struct KPtrs { const double* p[4 * NVARS]; };
 
-__global__ void rk4_stage_kernel(int stage, MutVars out, ConstVars prev, KPtrs k,
+__global__ void __launch_bounds__(256) rk4_stage_kernel(int stage, MutVars out, ConstVars prev, KPtrs k,
                                  int64_t n, double dt, int enforce,
                                  double chi_floor, int* status) {
     int bad = 0;
@@ -104,7 +104,7 @@ __global__ void rk4_stage_kernel(int stage, MutVars out, ConstVars prev, KPtrs k
     if (status && bad) atomicAdd(status, bad);
 }
 
-__global__ void enforce_kernel(MutVars u, int64_t n, double chi_floor, int* status) {
+__global__ void __launch_bounds__(256) enforce_kernel(MutVars u, int64_t n, double chi_floor, int* status) {
     int bad = 0;
     for (int64_t node = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; node < n;
          node += (int64_t)gridDim.x * blockDim.x) {
@@ -127,7 +127,7 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 // Brill-Lindquist data with zero momenta and spins
 // (BSSN_GR/src/grUtils.cpp:1033-1035, 1082-1100), then a seeded uniform
 // perturbation and enforcement.
-__global__ void initial_data_kernel(MutVars u, int gx, int gy, int gz, double x0,
+__global__ void __launch_bounds__(256) initial_data_kernel(MutVars u, int gx, int gy, int gz, double x0,
                                     double y0, double z0, double h, double b0,
                                     double b1, double b2, double b3, double b4,
                                     double b5, double m1, double m2,
@@ -170,17 +170,16 @@ __global__ void initial_data_kernel(MutVars u, int gx, int gy, int gz, double x0
 //                 acc = (s == 0 ? u : acc) + RK4_C[s]*dt*k
 //   stage 3:      u   = acc + RK4_C[3]*dt*k   (then enforce)
 // The accumulation order equals rkBSSN.cpp:851-858 term by term.
-__global__ void zip_stage_kernel(int stage, MutVars im, MutVars acc, MutVars u,
+__global__ void __launch_bounds__(256) zip_stage_kernel(int stage, MutVars im, MutVars acc, MutVars u,
                                  ConstVars R, const BssnBlockDesc* __restrict__ blocks,
                                  const Chunk* __restrict__ chunks, int gx, int gy, int gz,
                                  double dt, int enforce, double chi_floor, int* status) {
     const Chunk c = chunks[blockIdx.x];
     const BssnBlockDesc b = blocks[c.blk];
     const int s = b.sz, N = s - 6;
-    const int64_t n = (int64_t)N * N * N;
-    const int64_t q = c.start + threadIdx.x;
     int bad = 0;
-    if (q < n && threadIdx.x < c.count) {
+    for (int r = threadIdx.x; r < c.count; r += blockDim.x) {
+        const int64_t q = c.start + r;
         const int i = (int)(q % N), j = (int)((q / N) % N), k = (int)(q / ((int64_t)N * N));
         const int64_t x = b.g0[0] + i, y = b.g0[1] + j, z = b.g0[2] + k;
         const bool own = (i < N - 1 || x == gx - 1) && (j < N - 1 || y == gy - 1) &&
@@ -200,7 +199,7 @@ __global__ void zip_stage_kernel(int stage, MutVars im, MutVars acc, MutVars u,
                     acc.p[q2][node] = A_(a0, M_(cc, kk));
                     v[q2] = A_(u0, M_(cu, kk));
                 }
-                if (enforce) bad = enforce_regs(v, chi_floor);
+                if (enforce) bad += enforce_regs(v, chi_floor);
 #pragma unroll
                 for (int q2 = 0; q2 < NVARS; q2++) im.p[q2][node] = v[q2];
             } else {
@@ -208,7 +207,7 @@ __global__ void zip_stage_kernel(int stage, MutVars im, MutVars acc, MutVars u,
 #pragma unroll
                 for (int q2 = 0; q2 < NVARS; q2++)
                     v[q2] = A_(acc.p[q2][node], M_(cc, __ldg(R.p[q2] + p)));
-                bad = enforce_regs(v, chi_floor);
+                bad += enforce_regs(v, chi_floor);
 #pragma unroll
                 for (int q2 = 0; q2 < NVARS; q2++) u.p[q2][node] = v[q2];
             }
@@ -273,7 +272,7 @@ int launch_zip_stage(const MeshState* m, int stage, double* const* im, double* c
         Rr.p[q] = R[q];
     }
     if (m->n_int_chunks == 0) return 0;
-    zip_stage_kernel<<<m->n_int_chunks, 1024, 0, s>>>(stage, I, Ac, U, Rr, m->d_blocks,
+    zip_stage_kernel<<<m->n_int_chunks, 256, 0, s>>>(stage, I, Ac, U, Rr, m->d_blocks,
                                                       m->d_int_chunks, m->G[0], m->G[1],
                                                       m->G[2], dt, enforce, chi_floor, status);
     return cuda_status(cudaGetLastError());

@@ -18,7 +18,7 @@
 namespace bssn {
 namespace {
 
-__global__ void stencil_kernel(int kind, double* __restrict__ D,
+__global__ void __launch_bounds__(256) stencil_kernel(int kind, double* __restrict__ D,
                                const double* __restrict__ u, AxisCoef cf,
                                int nx, int ny, int nz, unsigned bflag) {
     const int dir = kind % 3;

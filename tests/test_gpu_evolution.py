@@ -1,0 +1,49 @@
+"""GPU: 100 RK4 steps of the uniform 512-block 13^3 workload through the
+batched, graph-captured plan; the Hamiltonian and momentum constraint L2
+norms every 10 steps must match, to 1e-10 relative, the history the
+reference's own right-hand side produced on the CPU
+(tests/golden/constraint_history.json, make_constraint_golden.py)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def test_constraint_norm_history_100_steps():
+    import bssn_b200 as B
+    with open(os.path.join(HERE, "golden", "constraint_history.json")) as f:
+        gold = json.load(f)
+    spec = B.generate_mesh(0, (8, 8, 8))
+    m = B.Mesh(spec)
+    U = torch.zeros((24, spec.n_nodes), dtype=torch.float64, device="cuda")
+    B.initial_data(U, spec)
+    dt = 0.25 * spec.h
+    plan = B.RK4Plan(m, B.default_params(), B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
+    Pz = torch.zeros((24, m.n_unzip), dtype=torch.float64, device="cuda")
+    cons = torch.zeros((4, spec.n_nodes), dtype=torch.float64, device="cuda")
+    norms = torch.zeros(4, dtype=torch.float64, device="cuda")
+
+    def measure():
+        m.unzip(Pz, U)
+        B.constraints(m, cons, Pz)
+        B.constraint_norms(m, cons, norms, radii=(0.5, 0.5))
+        torch.cuda.synchronize()
+        return norms.cpu().numpy().copy()
+
+    got = {0: measure()}
+    for step in range(1, 101):
+        plan.step(U, dt)
+        if step % 10 == 0:
+            got[step] = measure()
+    assert plan.violations() == gold["enforce_violations"]
+    worst = 0.0
+    for h in gold["history"]:
+        ref = np.array([float.fromhex(x) for x in h["norms"]])
+        rel = np.abs(got[h["step"]] - ref) / np.abs(ref)
+        worst = max(worst, rel.max())
+    assert worst <= 1e-10, worst

@@ -119,3 +119,23 @@ def test_constraints_vs_reference_live(O, REF, side, bflag):
     b = mg.interior(co, side)[:4]
     err = np.abs(a - b).max(axis=1) / np.abs(a).max(axis=1)
     assert err.max() <= 1e-12, err
+
+
+def test_oracle_rk4_matches_reference_history_10_steps(O, REF):
+    """The restated RHS inside the restated RK4 reproduces, after 10 steps,
+    the constraint norms of the reference-RHS evolution in the committed
+    history (to 1e-10 relative)."""
+    import json
+    import bssn_b200 as B  # mesh generator only (host code)
+    with open(os.path.join(HERE, "golden", "constraint_history.json")) as f:
+        gold = json.load(f)
+    spec = B.generate_mesh(0, (8, 8, 8))
+    mo = ol.MeshOracle(spec, O)
+    Z = mo.initial_data()
+    for _ in range(10):
+        assert mo.rk4_step(Z, 0.25 * spec.h, ol.params()) == 0
+    c = ol.oracle_constraints(spec, mo.unzip(Z), O)
+    got = ol.l2_norms(spec, c, radii=(0.5, 0.5))
+    ref = np.array([float.fromhex(x) for x in gold["history"][1]["norms"]])
+    assert gold["history"][1]["step"] == 10
+    assert np.abs(got - ref).max() / np.abs(ref).min() <= 1e-10, (got, ref)
