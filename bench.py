@@ -36,7 +36,7 @@ WORKLOADS = {
     "mix20k": (1, (10, 10, 7), "batched form: ~20,000 blocks, seeded size mix"),
     "mix4k": (1, (7, 5, 4), "mixed-level plain-path size: ~4,000 blocks"),
     "uniform512": (0, (8, 8, 8), "uniform octree of 512 blocks of 13^3"),
-    "small": (1, (2, 2, 1), "small mix for profiler captures"),
+    "small": (1, (2, 2, 2), "small mix for profiler captures"),
 }
 SEED_MESH = 20261203
 MIX = (0.7, 0.2, 0.08, 0.02)

@@ -266,9 +266,16 @@ __global__ void __launch_bounds__(256) l2_partial_kernel(ConstVars C, int nc, in
     for (int64_t node = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; node < n;
          node += (int64_t)gridDim.x * blockDim.x) {
         const int64_t ix = node % gx, iy = (node / gx) % gy, iz = node / ((int64_t)gx * gy);
-        const double x = x0 + ix * h, y = y0 + iy * h, z = z0 + iz * h;
-        const double d1 = sqrt((x - b0) * (x - b0) + (y - b1) * (y - b1) + (z - b2) * (z - b2));
-        const double d2 = sqrt((x - b3) * (x - b3) + (y - b4) * (y - b4) + (z - b5) * (z - b5));
+        // coordinates and distances rounded step by step (no contraction), so
+        // a node at exactly the excision radius is classified as on the CPU
+        const double x = __dadd_rn(x0, __dmul_rn((double)ix, h));
+        const double y = __dadd_rn(y0, __dmul_rn((double)iy, h));
+        const double z = __dadd_rn(z0, __dmul_rn((double)iz, h));
+        auto dist = [](double ax, double ay, double az) {
+            return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay)), __dmul_rn(az, az)));
+        };
+        const double d1 = dist(__dsub_rn(x, b0), __dsub_rn(y, b1), __dsub_rn(z, b2));
+        const double d2 = dist(__dsub_rn(x, b3), __dsub_rn(y, b4), __dsub_rn(z, b5));
         if (d1 < r1 || d2 < r2) continue;
         for (int c = 0; c < nc; c++) {
             const double v = C.p[c][node];

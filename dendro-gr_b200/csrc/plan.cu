@@ -84,6 +84,7 @@ void plan_destroy(Plan* p) {
     if (!p) return;
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
     cudaFree(p->P);
     cudaFree(p->R);
     cudaFree(p->im);
@@ -158,19 +159,33 @@ int plan_step(Plan* p, double* const* u, double dt, cudaStream_t s) {
         if (p->graph) cudaGraphDestroy(p->graph);
         p->exec = nullptr;
         p->graph = nullptr;
-        cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) return cuda_status(e);
-        int st = plan_enqueue(p, u, dt, s);
-        cudaGraph_t g = nullptr;
-        e = cudaStreamEndCapture(s, &g);
-        if (st) {
-            if (g) cudaGraphDestroy(g);
-            return st;
+        // capture on the plan's own stream: the caller's stream may be the
+        // legacy default stream, which cannot be captured; the graph is then
+        // launched onto the caller's stream, which orders it after prior work
+        if (!p->cap_stream &&
+            cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            return BSSN_ENOMEM;
         }
-        if (e != cudaSuccess) return cuda_status(e);
+        cudaError_t e = cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) {
+            cudaGetLastError();  // do not leave the failure for a later launch check
+            return cuda_status(e);
+        }
+        int st = plan_enqueue(p, u, dt, p->cap_stream);
+        cudaGraph_t g = nullptr;
+        e = cudaStreamEndCapture(p->cap_stream, &g);
+        if (st || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return st ? st : cuda_status(e);
+        }
         p->graph = g;
         e = cudaGraphInstantiate(&p->exec, g, 0);
-        if (e != cudaSuccess) return cuda_status(e);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return cuda_status(e);
+        }
         for (int v = 0; v < NVARS; v++) p->graph_u[v] = u[v];
         p->graph_dt = dt;
     }

@@ -23,6 +23,7 @@ struct Plan {
     std::vector<int> sides; // block-size buckets present
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    cudaStream_t cap_stream = nullptr;  // capture stream of the graph
     double* graph_u[NVARS] = {nullptr};
     double graph_dt = 0.0;
 };

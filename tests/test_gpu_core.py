@@ -88,7 +88,7 @@ def test_bssnrhs_single_block(B, O, side, bflag):
 
 
 def test_mesh_unzip_zip_bit_exact(B, O):
-    spec = B.generate_mesh(1, (2, 1, 1), seed=7)
+    spec = B.generate_mesh(1, (2, 1, 1), seed=7, xmin=-8.25)
     mo = ol.MeshOracle(spec, O)
     rng = np.random.default_rng(3)
     Z = rng.standard_normal((24, spec.n_nodes))
@@ -116,7 +116,7 @@ def test_mesh_unzip_zip_bit_exact(B, O):
 
 
 def test_mesh_rhs_mixed_sizes(B, O):
-    spec = B.generate_mesh(1, (2, 1, 1), seed=1)
+    spec = B.generate_mesh(1, (2, 1, 1), seed=1, xmin=-8.25)
     assert set(spec.sides.tolist()) == {13, 19, 31, 55}
     mo = ol.MeshOracle(spec, O)
     Z = mo.initial_data()
@@ -153,7 +153,7 @@ def test_rk4_step_vs_oracle(B, O, path, mesh):
     """One RK4 step from the same state on the GPU paths and on the CPU
     oracle (rkBSSN.cpp:764-860 restated); states compared per variable
     relative to the variable's largest magnitude."""
-    spec = B.generate_mesh(0, (4, 4, 4)) if mesh == "uniform" else B.generate_mesh(1, (2, 1, 1), seed=1)
+    spec = B.generate_mesh(0, (4, 4, 4)) if mesh == "uniform" else B.generate_mesh(1, (2, 1, 1), seed=1, xmin=-8.25)
     mo = ol.MeshOracle(spec, O)
     Z0 = mo.initial_data(eps=1e-8)
     dt = 0.25 * spec.h
@@ -185,7 +185,7 @@ def test_rk4_step_vs_oracle(B, O, path, mesh):
 
 
 def test_graph_replay_matches_eager(B):
-    spec = B.generate_mesh(1, (1, 1, 1), seed=8)
+    spec = B.generate_mesh(1, (1, 1, 1), seed=8, xmin=-8.25)
     m = B.Mesh(spec)
     U = torch.zeros((24, spec.n_nodes), dtype=torch.float64, device="cuda")
     B.initial_data(U, spec)
@@ -202,7 +202,7 @@ def test_graph_replay_matches_eager(B):
 
 
 def test_autotune_picks_a_tile_per_bucket(B):
-    spec = B.generate_mesh(1, (2, 1, 1), seed=1)
+    spec = B.generate_mesh(1, (2, 1, 1), seed=1, xmin=-8.25)
     m = B.Mesh(spec)
     U = torch.zeros((24, spec.n_nodes), dtype=torch.float64, device="cuda")
     B.initial_data(U, spec)
@@ -217,7 +217,7 @@ def test_autotune_picks_a_tile_per_bucket(B):
 
 @pytest.mark.parametrize("mesh", ["uniform", "mix"])
 def test_constraints_and_norms_vs_oracle(B, O, mesh):
-    spec = B.generate_mesh(0, (4, 4, 4)) if mesh == "uniform" else B.generate_mesh(1, (2, 1, 1), seed=1)
+    spec = B.generate_mesh(0, (4, 4, 4)) if mesh == "uniform" else B.generate_mesh(1, (2, 1, 1), seed=1, xmin=-8.25)
     mo = ol.MeshOracle(spec, O)
     Z = mo.initial_data(eps=1e-6)
     Uz = mo.unzip(Z)
