@@ -46,15 +46,16 @@ FLOP_PER_ZONE_STAGE = 6535.0  # 6,439 RHS + 96 RK axpy (per zone, per stage)
 def fused_rhs_bytes(sides):
     """Compulsory HBM bytes of one fused-RHS pass: read the 24 padded
     variables, write the 24 interior right-hand sides."""
-    return sum(8 * 24 * (s ** 3 + (s - 6) ** 3) for s in sides)
+    return sum(8 * 24 * (int(s) ** 3 + (int(s) - 6) ** 3) for s in sides)
 
 
 def step_bytes(sides, n_nodes):
     """Compulsory bytes of one RK stage of this implementation: ghost fill
     (read zipped, write padded), fused RHS (read padded, write interior),
     zip + update (read RHS, u, acc; write stage state and acc)."""
-    pad = sum(s ** 3 for s in sides)
-    inner = sum((s - 6) ** 3 for s in sides)
+    pad = sum(int(s) ** 3 for s in sides)
+    inner = sum((int(s) - 6) ** 3 for s in sides)
+    n_nodes = int(n_nodes)
     return 8 * 24 * (n_nodes + pad + pad + inner + inner + 4 * n_nodes)
 
 
@@ -109,6 +110,14 @@ class Clocks:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _plain(o):
+    """JSON fallback for numpy scalars."""
+    try:
+        return o.item()
+    except AttributeError:
+        return str(o)
 
 
 def measured_peaks():
@@ -215,7 +224,7 @@ def run_reference(args, wl):
            "cpu_baseline": dict(info, value=rate, unit="zone-updates/s"),
            "e2e": {"value": rate, "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
-    print(json.dumps(out))
+    print(json.dumps(out, default=_plain))
 
 
 # ---------------------------------------------------------------------------
@@ -385,7 +394,7 @@ def main():
                       "zones": zones, "sides": {str(s): int((spec.sides == s).sum()) for s in sorted(set(spec.sides.tolist()))},
                       "nodes": spec.n_nodes, "dt_over_dx": 0.25,
                       "l2": "inputs larger than L2 (24 x %.3g nodes x 8 B)" % spec.n_nodes,
-                      "parallelism": f"replicas x{world}", "tiles": {str(k): v for k, v in chosen.items()}},
+                      "parallelism": f"replicas x{world}", "tiles": {str(k): int(v) for k, v in chosen.items()}},
            "roofline": roofline,
            "step_hbm": {"bytes_per_step": sb, "achieved_gbs": sb / (ms_step * 1e-3) / 1e9,
                         "frac": sb / (ms_step * 1e-3) / 1e9 / hbm_peak},
@@ -397,7 +406,7 @@ def main():
     if not args.no_cpu:
         rate, info = cpu_reference_rate(spec.sides, seconds=15.0)
         out["cpu_baseline"] = dict(info, value=rate, unit="zone-updates/s")
-    print(json.dumps(out))
+    print(json.dumps(out, default=_plain))
     if dist is not None:
         dist.destroy_process_group()
 

@@ -11,6 +11,7 @@
 #include "mesh.h"
 #include "plan.h"
 #include "constraints.h"
+#include "remesh.h"
 #include "rhs_fused.cuh"
 
 struct bssn_mesh_s {
@@ -242,6 +243,102 @@ int bssn_constraint_norms_f64(bssn_mesh mesh, const double* const* cons_dev, int
     }
     return bssn::launch_l2_norms(m, cons_dev, ncons, xmin, h, bh, radii, m->d_partial, npartial,
                                  norms_dev, S(stream));
+}
+
+int64_t bssn_mesh_num_elements(bssn_mesh mesh) {
+    if (!mesh) return -1;
+    int64_t n = 0;
+    for (auto& b : mesh->st->blocks) {
+        const int64_t w = (b.sz - 7) / 6;
+        n += w * w * w;
+    }
+    return n;
+}
+
+int bssn_remesh_wavelet_f64(bssn_mesh mesh, const double* const* unzip_dev, int nvars, double tol,
+                            double* scores_dev, double* ratio_dev, uint8_t* flags_dev,
+                            bssn_stream_t stream) {
+    if (!mesh || !unzip_dev || nvars < 1 || nvars > bssn::NVARS || !(tol > 0) || !scores_dev)
+        return BSSN_EINVAL;
+    int st = bssn::launch_wavelet_scores(mesh->st, unzip_dev, nvars, scores_dev, nullptr, S(stream));
+    if (!st && (ratio_dev || flags_dev))
+        st = bssn::launch_block_flags(mesh->st, scores_dev, nvars, tol, ratio_dev, flags_dev, nullptr,
+                                      S(stream));
+    return st;
+}
+
+int bssn_remesh_features_f64(bssn_mesh mesh, const double* const* unzip_dev, float* feats_dev,
+                             bssn_stream_t stream) {
+    if (!mesh || !unzip_dev || !feats_dev) return BSSN_EINVAL;
+    return bssn::launch_features(mesh->st, unzip_dev, feats_dev, S(stream));
+}
+
+int bssn_remesh_mlp_fwd_bf16(const void* wq_dev, const float* norm_dev, const float* x_dev, int n,
+                             float* logits_dev, bssn_stream_t stream) {
+    if (!wq_dev || !x_dev || !logits_dev || n < 0) return BSSN_EINVAL;
+    return bssn::launch_mlp_fwd(wq_dev, norm_dev, x_dev, n, logits_dev, S(stream));
+}
+
+size_t bssn_remesh_mlp_grad_scratch(int n) { return n > 0 ? bssn::mlp_grad_scratch_floats(n) : 0; }
+
+int bssn_remesh_mlp_bwd_bf16(const void* wq_dev, const float* norm_dev, const float* x_dev,
+                             const float* y_dev, const float* c_dev, int n, float* grad_dev,
+                             float* loss_dev, float* scratch_dev, bssn_stream_t stream) {
+    if (!wq_dev || !x_dev || !y_dev || !grad_dev || !scratch_dev || n < 1) return BSSN_EINVAL;
+    return bssn::launch_mlp_grad(wq_dev, norm_dev, x_dev, y_dev, c_dev, n, grad_dev, loss_dev,
+                                 scratch_dev, S(stream));
+}
+
+int bssn_remesh_mlp_step_bf16(float* master_dev, void* wq_dev, const float* grad_dev, float* m_dev,
+                              float* v_dev, float lr, float beta1, float beta2, float eps, int t,
+                              bssn_stream_t stream) {
+    if (!master_dev || !wq_dev || !grad_dev || !m_dev || !v_dev || t < 1) return BSSN_EINVAL;
+    return bssn::launch_adam(master_dev, wq_dev, grad_dev, m_dev, v_dev, lr, beta1, beta2, eps, t,
+                             S(stream));
+}
+
+size_t bssn_remesh_decide_work_bytes(bssn_mesh mesh) {
+    if (!mesh) return 0;
+    const size_t nb = mesh->st->blocks.size();
+    const size_t ne = (size_t)bssn_mesh_num_elements(mesh);
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    return al(nb * 16 * sizeof(float)) + al(nb * sizeof(float)) + 3 * al(nb) +
+           al(ne * bssn::NVARS * sizeof(double));
+}
+
+int bssn_remesh_decide_f64(bssn_mesh mesh, const double* const* unzip_dev, const void* wq_dev,
+                           const float* norm_dev, float lo, float hi, double audit_frac,
+                           uint64_t seed, double tol, uint8_t* flags_dev, int* stats_dev,
+                           void* work_dev, size_t work_bytes, bssn_stream_t stream) {
+    if (!mesh || !unzip_dev || !wq_dev || !flags_dev || !stats_dev || !work_dev) return BSSN_EINVAL;
+    if (!(lo <= hi) || audit_frac < 0 || audit_frac > 1 || !(tol > 0)) return BSSN_EINVAL;
+    if (work_bytes < bssn_remesh_decide_work_bytes(mesh)) return BSSN_EINVAL;
+    bssn::MeshState* m = mesh->st;
+    const int nb = (int)m->blocks.size();
+    const int64_t ne = bssn_mesh_num_elements(mesh);
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    char* w = (char*)work_dev;
+    float* feats = (float*)w;
+    w += al((size_t)nb * 16 * sizeof(float));
+    float* logits = (float*)w;
+    w += al((size_t)nb * sizeof(float));
+    uint8_t* need = (uint8_t*)w;
+    w += al(nb);
+    uint8_t* decided = (uint8_t*)w;
+    w += al(nb);
+    uint8_t* exact = (uint8_t*)w;
+    w += al(nb);
+    double* scores = (double*)w;
+    (void)ne;
+    cudaStream_t s = S(stream);
+    int st = cudaMemsetAsync(stats_dev, 0, 4 * sizeof(int), s) == cudaSuccess ? 0 : BSSN_EINVAL;
+    if (!st) st = bssn::launch_features(m, unzip_dev, feats, s);
+    if (!st) st = bssn::launch_mlp_fwd(wq_dev, norm_dev, feats, nb, logits, s);
+    if (!st) st = bssn::launch_remesh_select(logits, nb, lo, hi, audit_frac, seed, need, decided, stats_dev, s);
+    if (!st) st = bssn::launch_wavelet_scores(m, unzip_dev, bssn::NVARS, scores, need, s);
+    if (!st) st = bssn::launch_block_flags(m, scores, bssn::NVARS, tol, nullptr, exact, need, s);
+    if (!st) st = bssn::launch_remesh_merge(nb, need, decided, exact, logits, lo, stats_dev, flags_dev, s);
+    return st;
 }
 
 int bssn_tile_count(void) { return bssn::tile_count(); }

@@ -127,6 +127,8 @@ void mesh_destroy(MeshState* m) {
     cudaFree(m->d_pad_chunks);
     cudaFree(m->d_int_chunks);
     cudaFree(m->d_partial);
+    cudaFree(m->d_elems);
+    cudaFree(m->d_elem_first);
     for (auto& t : m->tasks) cudaFree(t.second.first);
     delete m;
 }

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "bssn_b200.h"
+#include "remesh.h"
 #include "rhs_fused.cuh"
 
 namespace bssn {
@@ -33,6 +34,11 @@ struct MeshState {
     std::map<std::pair<int, int>, std::pair<BrickTask*, int>> tasks;
     // partial sums of the constraint-norm reduction (allocated on first use)
     double* d_partial = nullptr;
+    // elements (octants) of all blocks and the first element of each block
+    // (remesh test; built on first use)
+    ElemRef* d_elems = nullptr;
+    int64_t* d_elem_first = nullptr;
+    int64_t n_elems = 0;
     // autotuned tile per padded side (0 = not tuned)
     std::map<int, int> tuned;
 };

@@ -1,0 +1,510 @@
+// Remesh decision: the exact wavelet refinement test, cheap per-block
+// features, and a small BF16 MLP (16 -> 64 -> 64 -> 1, GELU, FP32
+// accumulation) that predicts the test, with hand-written forward, backward
+// and Adam kernels.
+//
+// Wavelet test: the reference scores every element with the interpolating
+// wavelet transform of dendrolib (isReMeshWAMR, BSSN_GR/src/dataUtils.cpp:
+// 511-624; the transform itself is absent from the reference tree).  This
+// file's definition: for every node of an element (octant, 7^3 nodes) with
+// an odd local index along some axis, w = u - (degree-5 Lagrange
+// interpolation from the coarse nodes at patch positions 1,3,5,7,9,11 of the
+// element's 13^3 patch along each odd axis); score = sqrt(sum w^2 / 279);
+// the element asks for refinement when the score of any variable exceeds
+// the tolerance.  Products and sums are explicitly rounded in a fixed order
+// (inner x, then y, then z; squares summed into 32 partials by node index mod
+// 32, partials added in order), identical to the CPU restatement.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "bssn_common.cuh"
+#include "mesh.h"
+#include "remesh.h"
+
+namespace bssn {
+namespace {
+
+__constant__ double kWfine[3][6] = {
+    {-7.0 / 256, 105.0 / 256, 105.0 / 128, -35.0 / 128, 21.0 / 256, -3.0 / 256},
+    {3.0 / 256, -25.0 / 256, 75.0 / 128, 75.0 / 128, -25.0 / 256, 3.0 / 256},
+    {-3.0 / 256, 21.0 / 256, -35.0 / 128, 105.0 / 128, 105.0 / 256, -7.0 / 256}};
+
+__device__ double wavelet_interp(const double* __restrict__ p, int s, int a, int b, int c) {
+    const int loc[3] = {a, b, c};
+    int n[3], base[3], step[3], wrow[3];
+    for (int d = 0; d < 3; d++) {
+        if (loc[d] & 1) {
+            n[d] = 6;
+            base[d] = 1;
+            step[d] = 2;
+            wrow[d] = (loc[d] - 1) / 2;
+        } else {
+            n[d] = 1;
+            base[d] = loc[d] + 3;
+            step[d] = 0;
+            wrow[d] = -1;
+        }
+    }
+    double az = 0.0;
+    for (int k = 0; k < n[2]; k++) {
+        const int pz = base[2] + step[2] * k;
+        double ay = 0.0;
+        for (int j = 0; j < n[1]; j++) {
+            const int py = base[1] + step[1] * j;
+            double ax = 0.0;
+            const double* row = p + (int64_t)s * (py + (int64_t)s * pz);
+            for (int i = 0; i < n[0]; i++) {
+                const double wx = wrow[0] < 0 ? 1.0 : kWfine[wrow[0]][i];
+                ax = __dadd_rn(ax, __dmul_rn(wx, __ldg(row + base[0] + step[0] * i)));
+            }
+            const double wy = wrow[1] < 0 ? 1.0 : kWfine[wrow[1]][j];
+            ay = __dadd_rn(ay, __dmul_rn(wy, ax));
+        }
+        const double wz = wrow[2] < 0 ? 1.0 : kWfine[wrow[2]][k];
+        az = __dadd_rn(az, __dmul_rn(wz, ay));
+    }
+    return az;
+}
+
+// One warp per (element, variable): lane l sums the squares of the wavelet
+// nodes q = l, l+32, ... (q in z,y,x order), lane 0 adds the 32 partials.
+__global__ void __launch_bounds__(256) wavelet_kernel(ConstVars U, int nvars,
+                                                      const BssnBlockDesc* __restrict__ blocks,
+                                                      const ElemRef* __restrict__ elems,
+                                                      int64_t nelem, double* __restrict__ scores,
+                                                      const uint8_t* __restrict__ need) {
+    const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (wid >= nelem * nvars) return;
+    const int64_t e = wid / nvars;
+    const int v = (int)(wid % nvars);
+    const ElemRef er = elems[e];
+    if (need && !need[er.blk]) return;  // whole warp: same element
+    const BssnBlockDesc b = blocks[er.blk];
+    const int s = b.sz;
+    const double* p = U.p[v] + b.offset + 6 * er.o[0] + (int64_t)s * (6 * er.o[1] + (int64_t)s * 6 * er.o[2]);
+    double part = 0.0;
+    // node q -> (a,b,c): enumerate the 343 element nodes in z,y,x order and
+    // keep those with an odd coordinate; lane l handles every 32nd kept node
+    int q = 0;
+    for (int c = 0; c < 7; c++)
+        for (int bb = 0; bb < 7; bb++)
+            for (int a = 0; a < 7; a++) {
+                if (!((a | bb | c) & 1)) continue;
+                if ((q & 31) == lane) {
+                    const double u = __ldg(p + (a + 3) + (int64_t)s * ((bb + 3) + (int64_t)s * (c + 3)));
+                    const double w = __dsub_rn(u, wavelet_interp(p, s, a, bb, c));
+                    part = __dadd_rn(part, __dmul_rn(w, w));
+                }
+                q++;
+            }
+    double tot = 0.0;
+    for (int l = 0; l < 32; l++) tot = __dadd_rn(tot, __shfl_sync(0xffffffffu, part, l));
+    if (lane == 0) scores[e * nvars + v] = __dsqrt_rn(__ddiv_rn(tot, 279.0));
+}
+
+// Per block: the largest score over its elements and variables divided by
+// the tolerance, and the refine flag (ratio > 1).
+__global__ void __launch_bounds__(256) block_flags_kernel(const double* __restrict__ scores, int nvars,
+                                                          const int64_t* __restrict__ first,
+                                                          int nblk, double tol, double* ratio,
+                                                          uint8_t* flags, const uint8_t* need) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblk || (need && !need[b])) return;
+    double m = 0.0;
+    for (int64_t e = first[b]; e < first[b + 1]; e++)
+        for (int v = 0; v < nvars; v++) m = fmax(m, scores[e * nvars + v]);
+    const double r = m / tol;
+    if (ratio) ratio[b] = r;
+    if (flags) flags[b] = r > 1.0 ? 1 : 0;
+}
+
+// Block features (16 floats), one CTA per block.
+__global__ void __launch_bounds__(256) features_kernel(ConstVars U, const BssnBlockDesc* __restrict__ blocks,
+                                                       float* __restrict__ feats) {
+    const BssnBlockDesc b = blocks[blockIdx.x];
+    const int s = b.sz, N = s - 6;
+    const int64_t st[3] = {1, s, (int64_t)s * s};
+    double mx[15];
+    for (int f = 0; f < 15; f++) mx[f] = 0.0;
+    double chimin = 1e300;
+    const int64_t n = (int64_t)N * N * N;
+    for (int64_t q = threadIdx.x; q < n; q += blockDim.x) {
+        const int i = 3 + (int)(q % N), j = 3 + (int)((q / N) % N), k = 3 + (int)(q / ((int64_t)N * N));
+        const int64_t p = b.offset + i + s * (j + (int64_t)s * k);
+        const double* chi = U.p[U_CHI];
+        const double* al = U.p[U_ALPHA];
+        const double c0 = chi[p];
+        for (int d = 0; d < 3; d++) {
+            const double cp = chi[p + st[d]], cm = chi[p - st[d]];
+            mx[d] = fmax(mx[d], fabs(__dmul_rn(__dsub_rn(cp, cm), 0.5)));
+            mx[3 + d] = fmax(mx[3 + d], fabs(__dmul_rn(__dsub_rn(al[p + st[d]], al[p - st[d]]), 0.5)));
+            mx[7 + d] = fmax(mx[7 + d], fabs(U.p[U_GT0 + d][p]));
+            mx[13] = fmax(mx[13], fabs(__dsub_rn(__dsub_rn(cp, c0), __dsub_rn(c0, cm))));
+        }
+        mx[6] = fmax(mx[6], fabs(U.p[U_K][p]));
+        for (int c = 0; c < 6; c++) mx[14] = fmax(mx[14], fabs(U.p[U_SYMAT0 + c][p]));
+        chimin = fmin(chimin, c0);
+    }
+    __shared__ double red[256][16];
+    for (int f = 0; f < 15; f++) red[threadIdx.x][f] = mx[f];
+    red[threadIdx.x][15] = chimin;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            for (int f = 0; f < 15; f++) red[threadIdx.x][f] = fmax(red[threadIdx.x][f], red[threadIdx.x + w][f]);
+            red[threadIdx.x][15] = fmin(red[threadIdx.x][15], red[threadIdx.x + w][15]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        float* f = feats + (int64_t)blockIdx.x * 16;
+        for (int q = 0; q < 10; q++) f[q] = (float)log10(red[0][q] + 1e-30);
+        const double h = (b.ptmax[0] - b.ptmin[0]) / (s - 1);
+        f[10] = (float)b.level;
+        f[11] = (float)(s / 55.0);
+        f[12] = (float)log10(red[0][15]);
+        f[13] = (float)log10(red[0][13] + 1e-30);
+        f[14] = (float)log10(red[0][14] + 1e-30);
+        f[15] = (float)log10(h);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// MLP 16 -> 64 -> 64 -> 1.  Parameter layout (MLP_NPARAM values):
+//   W1[64][16], b1[64], W2[64][64], b2[64], W3[64], b3
+// Compute copies are BF16; all arithmetic accumulates in FP32.
+// ---------------------------------------------------------------------------
+constexpr int IN = 16, HID = 64;
+constexpr int OW1 = 0, OB1 = OW1 + HID * IN, OW2 = OB1 + HID, OB2 = OW2 + HID * HID,
+              OW3 = OB2 + HID, OB3 = OW3 + HID;
+
+__device__ __forceinline__ float gelu(float a) { return 0.5f * a * (1.0f + erff(a * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float a) {
+    const float cdf = 0.5f * (1.0f + erff(a * 0.70710678118654752f));
+    const float pdf = 0.39894228040143268f * expf(-0.5f * a * a);
+    return cdf + a * pdf;
+}
+
+constexpr int MLP_THREADS = 128;
+
+// Forward for one sample per thread; parameters staged into shared memory
+// as FP32 (converted from BF16 once per CTA).
+__global__ void __launch_bounds__(MLP_THREADS) mlp_fwd_kernel(const __nv_bfloat16* __restrict__ wq,
+                                                              const float* __restrict__ norm,
+                                                              const float* __restrict__ X, int n,
+                                                              float* __restrict__ logits) {
+    __shared__ float w[MLP_NPARAM];
+    for (int q = threadIdx.x; q < MLP_NPARAM; q += blockDim.x) w[q] = __bfloat162float(wq[q]);
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float x[IN], h1[HID];
+    for (int k = 0; k < IN; k++) {
+        const float xv = X[(int64_t)i * IN + k];
+        x[k] = norm ? (xv - norm[k]) * norm[IN + k] : xv;
+    }
+    for (int o = 0; o < HID; o++) {
+        float a = w[OB1 + o];
+        for (int k = 0; k < IN; k++) a = fmaf(w[OW1 + o * IN + k], x[k], a);
+        h1[o] = gelu(a);
+    }
+    float out = w[OB3];
+    for (int o = 0; o < HID; o++) {
+        float a = w[OB2 + o];
+        for (int k = 0; k < HID; k++) a = fmaf(w[OW2 + o * HID + k], h1[k], a);
+        out = fmaf(w[OW3 + o], gelu(a), out);
+    }
+    logits[i] = out;
+}
+
+// Forward + backward of the weighted binary cross-entropy
+//   L = sum_i c_i * BCE(sigmoid(z_i), y_i) / n
+// for MLP_THREADS samples per CTA (one per thread).  Each CTA writes its
+// gradient partial (MLP_NPARAM floats, summed over its samples in sample
+// order) and its loss partial; mlp_reduce_kernel adds the partials in CTA
+// order, so a training run is deterministic.
+__global__ void __launch_bounds__(MLP_THREADS) mlp_grad_kernel(const __nv_bfloat16* __restrict__ wq,
+                                                               const float* __restrict__ norm,
+                                                               const float* __restrict__ X,
+                                                               const float* __restrict__ Y,
+                                                               const float* __restrict__ C, int n,
+                                                               float* __restrict__ gpart,
+                                                               float* __restrict__ lpart) {
+    extern __shared__ float sm[];
+    float* w = sm;                          // MLP_NPARAM
+    float* XS = w + MLP_NPARAM;             // [T][IN]   inputs
+    float* H1 = XS + MLP_THREADS * IN;      // [T][HID]  gelu(a1)
+    float* D1 = H1 + MLP_THREADS * HID;     // [T][HID]  dL/da1
+    float* D2 = D1 + MLP_THREADS * HID;     // [T][HID]  a2, then dL/da2
+    float* H2 = D2 + MLP_THREADS * HID;     // [T][HID]  gelu(a2), then dz*gelu(a2)
+    float* DZ = H2 + MLP_THREADS * HID;     // [T]       dL/dz
+    float* LS = DZ + MLP_THREADS;           // [T]       loss terms
+    const int t = threadIdx.x;
+    for (int q = t; q < MLP_NPARAM; q += blockDim.x) w[q] = __bfloat162float(wq[q]);
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + t;
+    const bool valid = i < n;
+    float* xs = XS + t * IN;
+    float* h1 = H1 + t * HID;
+    float* d1 = D1 + t * HID;
+    float* d2 = D2 + t * HID;
+    float* h2 = H2 + t * HID;
+    for (int k = 0; k < IN; k++) {
+        const float xv = valid ? X[(int64_t)i * IN + k] : 0.0f;
+        xs[k] = norm ? (xv - norm[k]) * norm[IN + k] : xv;
+    }
+    for (int o = 0; o < HID; o++) {
+        float a = w[OB1 + o];
+        for (int k = 0; k < IN; k++) a = fmaf(w[OW1 + o * IN + k], xs[k], a);
+        d1[o] = a;  // a1 for now
+        h1[o] = gelu(a);
+    }
+    float z = w[OB3];
+    for (int o = 0; o < HID; o++) {
+        float a = w[OB2 + o];
+        for (int k = 0; k < HID; k++) a = fmaf(w[OW2 + o * HID + k], h1[k], a);
+        d2[o] = a;
+        h2[o] = gelu(a);
+        z = fmaf(w[OW3 + o], h2[o], z);
+    }
+    float dz = 0.0f, loss = 0.0f;
+    if (valid) {
+        const float y = Y[i], c = C ? C[i] : 1.0f;
+        // numerically stable BCE with logits
+        loss = c * (fmaxf(z, 0.0f) - z * y + log1pf(expf(-fabsf(z)))) / n;
+        dz = c * (1.0f / (1.0f + expf(-z)) - y) / n;
+    }
+    DZ[t] = dz;
+    LS[t] = loss;
+    for (int o = 0; o < HID; o++) {
+        d2[o] = dz * w[OW3 + o] * gelu_grad(d2[o]);  // dL/da2
+        h2[o] *= dz;                                 // dL/dW3[o] contribution
+    }
+    for (int k = 0; k < HID; k++) {
+        float g = 0.0f;
+        for (int o = 0; o < HID; o++) g = fmaf(w[OW2 + o * HID + k], d2[o], g);
+        d1[k] = g * gelu_grad(d1[k]);  // dL/da1
+    }
+    __syncthreads();
+    // thread t owns parameters t, t+T, ...: sums over the CTA's samples
+    float* gp = gpart + (int64_t)blockIdx.x * MLP_NPARAM;
+    for (int q = t; q < MLP_NPARAM; q += blockDim.x) {
+        float g = 0.0f;
+        if (q < OB1) {
+            const int o = q / IN, k = q % IN;
+            for (int r = 0; r < MLP_THREADS; r++) g = fmaf(D1[r * HID + o], XS[r * IN + k], g);
+        } else if (q < OW2) {
+            const int o = q - OB1;
+            for (int r = 0; r < MLP_THREADS; r++) g += D1[r * HID + o];
+        } else if (q < OB2) {
+            const int o = (q - OW2) / HID, k = (q - OW2) % HID;
+            for (int r = 0; r < MLP_THREADS; r++) g = fmaf(D2[r * HID + o], H1[r * HID + k], g);
+        } else if (q < OW3) {
+            const int o = q - OB2;
+            for (int r = 0; r < MLP_THREADS; r++) g += D2[r * HID + o];
+        } else if (q < OB3) {
+            const int o = q - OW3;
+            for (int r = 0; r < MLP_THREADS; r++) g += H2[r * HID + o];
+        } else {
+            for (int r = 0; r < MLP_THREADS; r++) g += DZ[r];
+        }
+        gp[q] = g;
+    }
+    if (t == 0) {
+        float l = 0.0f;
+        for (int r = 0; r < MLP_THREADS; r++) l += LS[r];
+        lpart[blockIdx.x] = l;
+    }
+}
+
+__global__ void __launch_bounds__(MLP_THREADS) mlp_reduce_kernel(const float* __restrict__ gpart, int nparts,
+                                                                  float* __restrict__ grad) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= MLP_NPARAM) return;
+    float g = 0.0f;
+    for (int p = 0; p < nparts; p++) g += gpart[(int64_t)p * MLP_NPARAM + q];
+    grad[q] = g;
+}
+
+__global__ void mlp_loss_reduce_kernel(const float* lpart, int nparts, float* loss) {
+    if (threadIdx.x || blockIdx.x) return;
+    float l = 0.0f;
+    for (int p = 0; p < nparts; p++) l += lpart[p];
+    *loss = l;
+}
+
+__global__ void __launch_bounds__(256) adam_kernel(float* __restrict__ master, __nv_bfloat16* __restrict__ wq,
+                                                   const float* __restrict__ grad, float* __restrict__ m,
+                                                   float* __restrict__ v, float lr, float b1, float b2,
+                                                   float eps, float bc1, float bc2) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= MLP_NPARAM) return;
+    const float g = grad[q];
+    const float mq = b1 * m[q] + (1.0f - b1) * g;
+    const float vq = b2 * v[q] + (1.0f - b2) * g * g;
+    m[q] = mq;
+    v[q] = vq;
+    const float p = master[q] - lr * (mq / bc1) / (sqrtf(vq / bc2) + eps);
+    master[q] = p;
+    wq[q] = __float2bfloat16_rn(p);
+}
+
+
+__device__ __forceinline__ uint64_t hmix(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// Decide from the network where it is confident; mark for the exact test
+// the uncertain blocks (lo < p < hi) and a seeded audit sample.
+// stats[0] += uncertain, stats[1] += audited.
+__global__ void __launch_bounds__(256) remesh_select_kernel(const float* __restrict__ logits, int nblk,
+                                                            float lo, float hi, double audit_frac,
+                                                            uint64_t seed, uint8_t* need,
+                                                            uint8_t* decided, int* stats) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblk) return;
+    const float p = 1.0f / (1.0f + expf(-logits[b]));
+    const bool unsure = p > lo && p < hi;
+    const double u = (double)(hmix(seed + 0x9E3779B97F4A7C15ULL * (uint64_t)(b + 1)) >> 11) *
+                     (1.0 / 9007199254740992.0);
+    const bool audit = u < audit_frac;
+    need[b] = (unsure || audit) ? 1 : 0;
+    decided[b] = p >= hi ? 1 : 0;
+    if (unsure) atomicAdd(&stats[0], 1);
+    if (audit && !unsure) atomicAdd(&stats[1], 1);
+}
+
+// Final flags: the exact result where the exact test ran, the network's
+// decision elsewhere.  stats[2] += audited blocks the network alone would
+// have missed (p <= lo but the exact test refines), stats[3] += audited
+// blocks the exact test refines.
+__global__ void __launch_bounds__(256) remesh_merge_kernel(int nblk, const uint8_t* need,
+                                                           const uint8_t* decided,
+                                                           const uint8_t* exact,
+                                                           const float* logits, float lo,
+                                                           int* stats, uint8_t* flags) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblk) return;
+    if (need[b]) {
+        flags[b] = exact[b];
+        const float p = 1.0f / (1.0f + expf(-logits[b]));
+        if (p <= lo && exact[b]) atomicAdd(&stats[2], 1);
+        if (exact[b]) atomicAdd(&stats[3], 1);
+    } else {
+        flags[b] = decided[b];
+    }
+}
+
+}  // namespace
+
+int remesh_elements(MeshState* m) {
+    if (m->d_elems) return 0;
+    std::vector<ElemRef> e;
+    std::vector<int64_t> first(m->blocks.size() + 1, 0);
+    for (size_t b = 0; b < m->blocks.size(); b++) {
+        const int w = (m->blocks[b].sz - 7) / 6;
+        for (int oz = 0; oz < w; oz++)
+            for (int oy = 0; oy < w; oy++)
+                for (int ox = 0; ox < w; ox++)
+                    e.push_back(ElemRef{(int32_t)b, {(int16_t)ox, (int16_t)oy, (int16_t)oz}, 0});
+        first[b + 1] = (int64_t)e.size();
+    }
+    if (cudaMalloc((void**)&m->d_elems, e.size() * sizeof(ElemRef)) != cudaSuccess) return BSSN_ENOMEM;
+    if (cudaMalloc((void**)&m->d_elem_first, first.size() * sizeof(int64_t)) != cudaSuccess) return BSSN_ENOMEM;
+    cudaMemcpy(m->d_elems, e.data(), e.size() * sizeof(ElemRef), cudaMemcpyHostToDevice);
+    cudaMemcpy(m->d_elem_first, first.data(), first.size() * sizeof(int64_t), cudaMemcpyHostToDevice);
+    m->n_elems = (int64_t)e.size();
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_wavelet_scores(MeshState* m, const double* const* U, int nvars, double* scores,
+                          const uint8_t* need, cudaStream_t s) {
+    int st = remesh_elements(m);
+    if (st) return st;
+    ConstVars u = {};
+    for (int v = 0; v < nvars; v++) u.p[v] = U[v];
+    const int64_t warps = m->n_elems * nvars;
+    const int64_t blocks = (warps * 32 + 255) / 256;
+    wavelet_kernel<<<(unsigned)blocks, 256, 0, s>>>(u, nvars, m->d_blocks, m->d_elems, m->n_elems, scores, need);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_block_flags(MeshState* m, const double* scores, int nvars, double tol, double* ratio,
+                       uint8_t* flags, const uint8_t* need, cudaStream_t s) {
+    int st = remesh_elements(m);
+    if (st) return st;
+    const int nb = (int)m->blocks.size();
+    block_flags_kernel<<<(nb + 255) / 256, 256, 0, s>>>(scores, nvars, m->d_elem_first, nb, tol, ratio, flags, need);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_features(const MeshState* m, const double* const* U, float* feats, cudaStream_t s) {
+    ConstVars u = {};
+    for (int v = 0; v < NVARS; v++) u.p[v] = U[v];
+    features_kernel<<<(unsigned)m->blocks.size(), 256, 0, s>>>(u, m->d_blocks, feats);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_mlp_fwd(const void* wq, const float* norm, const float* X, int n, float* logits,
+                   cudaStream_t s) {
+    if (n <= 0) return 0;
+    mlp_fwd_kernel<<<(n + MLP_THREADS - 1) / MLP_THREADS, MLP_THREADS, 0, s>>>(
+        (const __nv_bfloat16*)wq, norm, X, n, logits);
+    return cuda_status(cudaGetLastError());
+}
+
+size_t mlp_grad_scratch_floats(int n) {
+    const int parts = (n + MLP_THREADS - 1) / MLP_THREADS;
+    return (size_t)parts * (MLP_NPARAM + 1);
+}
+
+int launch_mlp_grad(const void* wq, const float* norm, const float* X, const float* Y,
+                    const float* C, int n, float* grad, float* loss, float* scratch,
+                    cudaStream_t s) {
+    if (n <= 0) return BSSN_EINVAL;
+    const int parts = (n + MLP_THREADS - 1) / MLP_THREADS;
+    float* gpart = scratch;
+    float* lpart = gpart + (size_t)parts * MLP_NPARAM;
+    const size_t smem = sizeof(float) * (MLP_NPARAM + MLP_THREADS * (IN + 4 * HID + 2));
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return cuda_status(e);
+        attr = true;
+    }
+    mlp_grad_kernel<<<parts, MLP_THREADS, smem, s>>>((const __nv_bfloat16*)wq, norm, X, Y, C, n, gpart, lpart);
+    mlp_reduce_kernel<<<(MLP_NPARAM + MLP_THREADS - 1) / MLP_THREADS, MLP_THREADS, 0, s>>>(gpart, parts, grad);
+    if (loss) mlp_loss_reduce_kernel<<<1, 32, 0, s>>>(lpart, parts, loss);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_adam(float* master, void* wq, const float* grad, float* m, float* v, float lr, float b1,
+                float b2, float eps, int t, cudaStream_t s) {
+    const float bc1 = 1.0f - powf(b1, (float)t), bc2 = 1.0f - powf(b2, (float)t);
+    adam_kernel<<<(MLP_NPARAM + 255) / 256, 256, 0, s>>>(master, (__nv_bfloat16*)wq, grad, m, v, lr, b1,
+                                                         b2, eps, bc1, bc2);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_remesh_select(const float* logits, int nblk, float lo, float hi, double audit_frac,
+                         uint64_t seed, uint8_t* need, uint8_t* decided, int* stats,
+                         cudaStream_t s) {
+    remesh_select_kernel<<<(nblk + 255) / 256, 256, 0, s>>>(logits, nblk, lo, hi, audit_frac, seed,
+                                                            need, decided, stats);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_remesh_merge(int nblk, const uint8_t* need, const uint8_t* decided,
+                        const uint8_t* exact, const float* logits, float lo, int* stats,
+                        uint8_t* flags, cudaStream_t s) {
+    remesh_merge_kernel<<<(nblk + 255) / 256, 256, 0, s>>>(nblk, need, decided, exact, logits, lo,
+                                                           stats, flags);
+    return cuda_status(cudaGetLastError());
+}
+
+}  // namespace bssn

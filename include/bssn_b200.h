@@ -186,6 +186,67 @@ int bssn_constraint_norms_f64(bssn_mesh mesh, const double* const* cons_dev,
                               double* norms_dev, bssn_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* Remesh decision.  The reference scores each element with dendrolib's
+ * wavelet transform inside isReMeshWAMR (BSSN_GR/src/dataUtils.cpp:511-624;
+ * the transform is absent from the reference tree, so this library defines
+ * it: for every node of an element (octant, 7^3 nodes) with an odd local
+ * index on some axis, w = u - degree-5 Lagrange interpolation from the
+ * element patch's coarse nodes at positions 1,3,5,7,9,11 along each odd
+ * axis; score = sqrt(sum w^2 / 279); an element asks for refinement when
+ * the score of any variable exceeds tol).  Elements are numbered block by
+ * block, octant x fastest. */
+int64_t bssn_mesh_num_elements(bssn_mesh mesh);
+/* Exact test: scores_dev (num_elements x nvars doubles) always; optionally
+ * per-block max score / tol (ratio_dev) and refine flags (flags_dev). */
+int bssn_remesh_wavelet_f64(bssn_mesh mesh, const double* const* unzip_dev,
+                            int nvars, double tol, double* scores_dev,
+                            double* ratio_dev, uint8_t* flags_dev,
+                            bssn_stream_t stream);
+/* 16 cheap features per block (floats): log10 of max |centred difference|
+ * of chi (x,y,z), of alpha (x,y,z), max |K|, max |Gt^i| (3), level, side/55,
+ * log10 min chi, log10 max |second difference of chi|, log10 max |At_ij|,
+ * log10 h. */
+int bssn_remesh_features_f64(bssn_mesh mesh, const double* const* unzip_dev,
+                             float* feats_dev, bssn_stream_t stream);
+/* The indicator network: 16 -> 64 -> 64 -> 1 with GELU, parameters
+ * W1[64][16], b1[64], W2[64][64], b2[64], W3[64], b3 (BSSN_MLP_NPARAM
+ * values) held in BF16 for compute, all accumulation in FP32.  norm_dev
+ * (optional): 16 means then 16 inverse standard deviations applied to the
+ * inputs. */
+#define BSSN_MLP_NPARAM 5313
+int bssn_remesh_mlp_fwd_bf16(const void* wq_dev, const float* norm_dev,
+                             const float* x_dev, int n, float* logits_dev,
+                             bssn_stream_t stream);
+/* floats of scratch bssn_remesh_mlp_bwd_bf16 needs for n samples */
+size_t bssn_remesh_mlp_grad_scratch(int n);
+/* Gradient of L = sum_i c_i BCE(sigmoid(z_i), y_i) / n with respect to the
+ * parameters (FP32, deterministic order); c_dev optional (1); loss_dev
+ * optional. */
+int bssn_remesh_mlp_bwd_bf16(const void* wq_dev, const float* norm_dev,
+                             const float* x_dev, const float* y_dev,
+                             const float* c_dev, int n, float* grad_dev,
+                             float* loss_dev, float* scratch_dev,
+                             bssn_stream_t stream);
+/* Adam step on FP32 master parameters, refreshing the BF16 copy (step t>=1). */
+int bssn_remesh_mlp_step_bf16(float* master_dev, void* wq_dev,
+                              const float* grad_dev, float* m_dev, float* v_dev,
+                              float lr, float beta1, float beta2, float eps,
+                              int t, bssn_stream_t stream);
+/* The learned decision: features -> network -> refine where p >= hi, keep
+ * where p <= lo, run the exact test on the uncertain blocks and on a seeded
+ * audit sample (fraction audit_frac); flags_dev gets one byte per block.
+ * stats_dev (4 ints): uncertain blocks, extra audited blocks, audited
+ * blocks the network alone would have missed, audited blocks the exact test
+ * refines.  work_dev: bssn_remesh_decide_work_bytes(mesh) bytes. */
+size_t bssn_remesh_decide_work_bytes(bssn_mesh mesh);
+int bssn_remesh_decide_f64(bssn_mesh mesh, const double* const* unzip_dev,
+                           const void* wq_dev, const float* norm_dev, float lo,
+                           float hi, double audit_frac, uint64_t seed,
+                           double tol, uint8_t* flags_dev, int* stats_dev,
+                           void* work_dev, size_t work_bytes,
+                           bssn_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
 /* One whole RK4 step as a plan over a mesh (the reference's per-step
  * sequence rkBSSN.cpp:764-860: per stage unzip -> bssnRHS -> zip -> stage
  * update).  The plan owns its scratch buffers (two padded 24-variable

@@ -912,3 +912,119 @@ void orc_physical_constraints(double** cons, const double** u, unsigned offset,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Remesh: wavelet refinement scores and block features (see the header).
+// ---------------------------------------------------------------------------
+namespace {
+// degree-5 Lagrange weights at fine patch positions 4, 6, 8 from coarse
+// positions 1, 3, 5, 7, 9, 11 (exact dyadic rationals)
+const double kWfine[3][6] = {
+    {-7.0 / 256, 105.0 / 256, 105.0 / 128, -35.0 / 128, 21.0 / 256, -3.0 / 256},
+    {3.0 / 256, -25.0 / 256, 75.0 / 128, 75.0 / 128, -25.0 / 256, 3.0 / 256},
+    {-3.0 / 256, 21.0 / 256, -35.0 / 128, 105.0 / 128, 105.0 / 256, -7.0 / 256}};
+
+// interpolation of the patch at local node (a,b,c) in [0,6]^3; p = patch
+// origin (value at patch (0,0,0)), strides 1, s, s*s
+double wavelet_interp(const double* p, int s, int a, int b, int c) {
+    int n[3], pos[3][6];
+    double w[3][6];
+    const int loc[3] = {a, b, c};
+    for (int d = 0; d < 3; d++) {
+        if (loc[d] & 1) {
+            n[d] = 6;
+            for (int t = 0; t < 6; t++) {
+                pos[d][t] = 1 + 2 * t;
+                w[d][t] = kWfine[(loc[d] - 1) / 2][t];
+            }
+        } else {
+            n[d] = 1;
+            pos[d][0] = loc[d] + 3;
+            w[d][0] = 1.0;
+        }
+    }
+    double az = 0.0;
+    for (int k = 0; k < n[2]; k++) {
+        double ay = 0.0;
+        for (int j = 0; j < n[1]; j++) {
+            double ax = 0.0;
+            for (int i = 0; i < n[0]; i++)
+                ax += w[0][i] * p[pos[0][i] + (int64_t)s * (pos[1][j] + (int64_t)s * pos[2][k])];
+            ay += w[1][j] * ax;
+        }
+        az += w[2][k] * ay;
+    }
+    return az;
+}
+}  // namespace
+
+extern "C" void orc_wavelet_scores(const double** unzip, const OrcBlock* blks, int nblk,
+                                   int nvars, double* scores) {
+    std::vector<int64_t> first(nblk + 1, 0);
+    for (int b = 0; b < nblk; b++) {
+        const int w = (blks[b].sz - 7) / 6;
+        first[b + 1] = first[b] + (int64_t)w * w * w;
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int b = 0; b < nblk; b++) {
+        const int s = blks[b].sz, w = (s - 7) / 6;
+        for (int e = 0; e < w * w * w; e++) {
+            const int ox = e % w, oy = (e / w) % w, oz = e / (w * w);
+            for (int v = 0; v < nvars; v++) {
+                const double* p = unzip[v] + blks[b].offset + 6 * ox +
+                                  (int64_t)s * (6 * oy + (int64_t)s * 6 * oz);
+                double part[32] = {0};
+                int q = 0;
+                for (int c = 0; c < 7; c++)
+                    for (int bb = 0; bb < 7; bb++)
+                        for (int a = 0; a < 7; a++) {
+                            if (!((a | bb | c) & 1)) continue;
+                            const double u = p[(a + 3) + (int64_t)s * ((bb + 3) + (int64_t)s * (c + 3))];
+                            const double wv = u - wavelet_interp(p, s, a, bb, c);
+                            part[q & 31] += wv * wv;
+                            q++;
+                        }
+                double tot = 0.0;
+                for (int l = 0; l < 32; l++) tot += part[l];
+                scores[(first[b] + e) * nvars + v] = sqrt(tot / 279.0);
+            }
+        }
+    }
+}
+
+extern "C" void orc_block_features(const double** unzip, const OrcBlock* blks, int nblk,
+                                   float* feats) {
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int b = 0; b < nblk; b++) {
+        const int s = blks[b].sz;
+        const int64_t st[3] = {1, s, (int64_t)s * s};
+        double mx[16];
+        for (int f = 0; f < 16; f++) mx[f] = 0.0;
+        double chimin = 1e300;
+        for (int k = 3; k < s - 3; k++)
+            for (int j = 3; j < s - 3; j++)
+                for (int i = 3; i < s - 3; i++) {
+                    const int64_t p = blks[b].offset + i + s * (j + (int64_t)s * k);
+                    const double* chi = unzip[U_CHI];
+                    const double* al = unzip[U_ALPHA];
+                    for (int d = 0; d < 3; d++) {
+                        mx[d] = std::max(mx[d], fabs((chi[p + st[d]] - chi[p - st[d]]) * 0.5));
+                        mx[3 + d] = std::max(mx[3 + d], fabs((al[p + st[d]] - al[p - st[d]]) * 0.5));
+                        mx[7 + d] = std::max(mx[7 + d], fabs(unzip[U_GT0 + d][p]));
+                        mx[13] = std::max(mx[13], fabs((chi[p + st[d]] - chi[p]) - (chi[p] - chi[p - st[d]])));
+                    }
+                    mx[6] = std::max(mx[6], fabs(unzip[U_K][p]));
+                    for (int c = 0; c < 6; c++) mx[14] = std::max(mx[14], fabs(unzip[U_SYMAT0 + c][p]));
+                    chimin = std::min(chimin, chi[p]);
+                }
+        const double h = (blks[b].ptmax[0] - blks[b].ptmin[0]) / (s - 1);
+        float* f = feats + (int64_t)b * 16;
+        for (int q = 0; q < 10; q++) f[q] = (float)log10(mx[q] + 1e-30);
+        f[10] = (float)blks[b].level;
+        f[11] = (float)(s / 55.0);
+        f[12] = (float)log10(chimin);
+        f[13] = (float)log10(mx[13] + 1e-30);
+        f[14] = (float)log10(mx[14] + 1e-30);
+        f[15] = (float)log10(h);
+    }
+}

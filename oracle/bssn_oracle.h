@@ -112,6 +112,24 @@ void orc_physical_constraints(double** cons, const double** u, unsigned offset,
                               const double* pmin, const double* pmax,
                               const unsigned* sz, unsigned bflag, double* ws);
 
+
+/* --- remesh (the absent dendrolib wavelet transform behind isReMeshWAMR,
+ * BSSN_GR/src/dataUtils.cpp:511-624; parity with Dendro unpinned).
+ * Element = one octant of a block (7^3 nodes), its 13^3 patch = the element
+ * plus 3 halo nodes.  Interpolating-wavelet coefficient at every element
+ * node with an odd local index along some axis: the value minus its
+ * degree-5 Lagrange interpolation from the coarse (even local index) nodes
+ * at patch positions {1,3,5,7,9,11} along each odd axis.  Score of an
+ * (element, variable) = sqrt(sum w^2 / 279), summed in the canonical order:
+ * node q (z, y, x ascending over the 279 wavelet nodes) goes to partial
+ * q mod 32, partials added in ascending order.  scores: one per element per
+ * variable, elements numbered block by block, octant x fastest. */
+void orc_wavelet_scores(const double** unzip, const OrcBlock* blks, int nblk,
+                        int nvars, double* scores);
+/* Per-block remesh features (16 floats per block, see bssn_b200.h). */
+void orc_block_features(const double** unzip, const OrcBlock* blks, int nblk,
+                        float* feats);
+
 #ifdef __cplusplus
 }
 #endif
