@@ -80,6 +80,20 @@ def _sig():
     lib.bssn_constraint_norms_f64.argtypes = [vp, vp, i, P(d), d, P(d), P(d), vp, vp]
     lib.bssn_rk4_plan_time_rhs.argtypes = [vp, i, vp, P(C.c_float)]
     lib.bssn_fp64_probe.argtypes = [vp, i, vp, P(d)]
+    lib.bssn_mesh_num_elements.argtypes = [vp]
+    lib.bssn_mesh_num_elements.restype = i64
+    lib.bssn_remesh_wavelet_f64.argtypes = [vp, vp, i, d, vp, vp, vp, vp]
+    lib.bssn_remesh_features_f64.argtypes = [vp, vp, vp, vp]
+    lib.bssn_remesh_mlp_fwd_bf16.argtypes = [vp, vp, vp, i, vp, vp]
+    lib.bssn_remesh_mlp_grad_scratch.argtypes = [i]
+    lib.bssn_remesh_mlp_grad_scratch.restype = C.c_size_t
+    lib.bssn_remesh_mlp_bwd_bf16.argtypes = [vp, vp, vp, vp, vp, i, vp, vp, vp, vp]
+    lib.bssn_remesh_mlp_step_bf16.argtypes = [vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float,
+                                              C.c_float, i, vp]
+    lib.bssn_remesh_decide_work_bytes.argtypes = [vp]
+    lib.bssn_remesh_decide_work_bytes.restype = C.c_size_t
+    lib.bssn_remesh_decide_f64.argtypes = [vp, vp, vp, vp, C.c_float, C.c_float, d, C.c_uint64, d,
+                                           vp, vp, vp, C.c_size_t, vp]
     lib.bssn_tile_count.argtypes = []
     lib.bssn_tile_info.argtypes = [i, P(i)]
 
@@ -335,3 +349,100 @@ def constraint_norms(mesh: Mesh, cons, norms, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0)
     check(lib.bssn_constraint_norms_f64(mesh.h, _cons_ptrs(cons), ncons, xm, spec.h, b, r,
                                         C.c_void_p(norms.data_ptr()), stream_ptr(stream)),
           "constraint_norms")
+
+
+# ---------------------------------------------------------------------------
+# remesh indicator
+# ---------------------------------------------------------------------------
+MLP_NPARAM = 5313
+
+
+def _vp(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def wavelet_scores(mesh: Mesh, unz, tol=1e-6, nvars=NVARS, stream=None):
+    """Exact wavelet test: (scores[num_elements, nvars], ratio[nblocks],
+    flags[nblocks]) as CUDA tensors."""
+    import torch
+    ne = lib.bssn_mesh_num_elements(mesh.h)
+    nb = mesh.spec.nblocks
+    scores = torch.empty((ne, nvars), dtype=torch.float64, device="cuda")
+    ratio = torch.empty(nb, dtype=torch.float64, device="cuda")
+    flags = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    check(lib.bssn_remesh_wavelet_f64(mesh.h, ptrs(unz), nvars, tol, _vp(scores), _vp(ratio), _vp(flags),
+                                      stream_ptr(stream)), "remesh_wavelet")
+    return scores, ratio, flags
+
+
+def block_features(mesh: Mesh, unz, stream=None):
+    import torch
+    f = torch.empty((mesh.spec.nblocks, 16), dtype=torch.float32, device="cuda")
+    check(lib.bssn_remesh_features_f64(mesh.h, ptrs(unz), _vp(f), stream_ptr(stream)), "remesh_features")
+    return f
+
+
+class RemeshMLP:
+    """The 16 -> 64 -> 64 -> 1 GELU indicator network: FP32 master
+    parameters, BF16 compute copy, Adam state, input normalisation."""
+
+    def __init__(self, seed=0):
+        import torch
+        g = torch.Generator().manual_seed(seed)
+        p = torch.zeros(MLP_NPARAM, dtype=torch.float32)
+        # He-style init of the weight blocks; biases zero
+        p[0:1024] = torch.randn(1024, generator=g) * (2.0 / 16) ** 0.5
+        p[1088:1088 + 4096] = torch.randn(4096, generator=g) * (2.0 / 64) ** 0.5
+        p[5248:5312] = torch.randn(64, generator=g) * (1.0 / 64) ** 0.5
+        self.master = p.cuda()
+        self.wq = self.master.to(torch.bfloat16)
+        self.m = torch.zeros_like(self.master)
+        self.v = torch.zeros_like(self.master)
+        self.norm = torch.cat([torch.zeros(16), torch.ones(16)]).cuda()
+        self.t = 0
+        self.lo, self.hi = 0.02, 0.98
+
+    def set_norm(self, X):
+        mu = X.mean(0)
+        sd = X.std(0).clamp_min(1e-3)
+        import torch
+        self.norm = torch.cat([mu, 1.0 / sd]).float().contiguous()
+
+    def logits(self, X, stream=None):
+        import torch
+        out = torch.empty(X.shape[0], dtype=torch.float32, device="cuda")
+        check(lib.bssn_remesh_mlp_fwd_bf16(_vp(self.wq), _vp(self.norm), _vp(X), X.shape[0], _vp(out),
+                                           stream_ptr(stream)), "mlp_fwd")
+        return out
+
+    def grad(self, X, Y, Cw=None, stream=None):
+        import torch
+        n = X.shape[0]
+        scratch = torch.empty(lib.bssn_remesh_mlp_grad_scratch(n), dtype=torch.float32, device="cuda")
+        g = torch.empty(MLP_NPARAM, dtype=torch.float32, device="cuda")
+        loss = torch.empty(1, dtype=torch.float32, device="cuda")
+        check(lib.bssn_remesh_mlp_bwd_bf16(_vp(self.wq), _vp(self.norm), _vp(X), _vp(Y), _vp(Cw), n,
+                                           _vp(g), _vp(loss), _vp(scratch), stream_ptr(stream)), "mlp_bwd")
+        return g, loss
+
+    def step(self, g, lr=3e-3, b1=0.9, b2=0.999, eps=1e-8, stream=None):
+        self.t += 1
+        check(lib.bssn_remesh_mlp_step_bf16(_vp(self.master), _vp(self.wq), _vp(g), _vp(self.m), _vp(self.v),
+                                            lr, b1, b2, eps, self.t, stream_ptr(stream)), "mlp_step")
+
+
+def remesh_decide(mesh: Mesh, unz, net: RemeshMLP, tol=1e-6, audit_frac=0.05, seed=7, work=None,
+                  stream=None):
+    """Learned remesh flags with the exact-test fallback and audit; returns
+    (flags uint8[nblocks], stats int32[4])."""
+    import torch
+    nb = mesh.spec.nblocks
+    wb = lib.bssn_remesh_decide_work_bytes(mesh.h)
+    if work is None or work.numel() < wb:
+        work = torch.empty(wb, dtype=torch.uint8, device="cuda")
+    flags = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    stats = torch.zeros(4, dtype=torch.int32, device="cuda")
+    check(lib.bssn_remesh_decide_f64(mesh.h, ptrs(unz), _vp(net.wq), _vp(net.norm), net.lo, net.hi, audit_frac,
+                                     seed, tol, _vp(flags), _vp(stats), _vp(work), wb, stream_ptr(stream)),
+          "remesh_decide")
+    return flags, stats

@@ -1,0 +1,172 @@
+"""GPU tests of the remesh indicator: the exact wavelet test and the block
+features against the CPU oracle, the BF16 MLP forward / backward / Adam
+kernels against a float64 numpy restatement (same BF16-rounded weights), and
+the learned decision against the exact test."""
+import ctypes as C
+import time
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def B():
+    import bssn_b200
+    return bssn_b200
+
+
+@pytest.fixture(scope="module")
+def state(B):
+    """A mixed mesh, evolved a few steps so the fields have structure."""
+    spec = B.generate_mesh(1, (2, 1, 1), seed=1, xmin=-8.25)
+    m = B.Mesh(spec)
+    U = torch.zeros((24, spec.n_nodes), dtype=torch.float64, device="cuda")
+    B.initial_data(U, spec, bh=(0.6, -4.1, -4.2, -0.6, -4.1, -4.2))
+    plan = B.RK4Plan(m, B.default_params())
+    for _ in range(3):
+        plan.step(U, 0.25 * spec.h)
+    Pz = torch.zeros((24, m.n_unzip), dtype=torch.float64, device="cuda")
+    m.unzip(Pz, U)
+    torch.cuda.synchronize()
+    return spec, m, Pz
+
+
+def test_wavelet_scores_vs_oracle(B, state):
+    spec, m, Pz = state
+    scores, ratio, flags = B.wavelet_scores(m, Pz, tol=1e-6)
+    torch.cuda.synchronize()
+    U = Pz.cpu().numpy()
+    ne = B.lib.bssn_mesh_num_elements(m.h)
+    ref = np.zeros(ne * 24)
+    O = ol.oracle()
+    O.lib.orc_wavelet_scores(ol.rows(U), spec.blocks, spec.nblocks, 24, ref.ctypes.data_as(ol._dp))
+    got = scores.cpu().numpy().ravel()
+    # identical per-node coefficients; partial-sum order identical too
+    assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))
+    # per-block flags: any element / variable above tol
+    first = np.cumsum([0] + [((int(s) - 7) // 6) ** 3 for s in spec.sides])
+    rmax = np.array([ref.reshape(ne, 24)[first[b]:first[b + 1]].max() for b in range(spec.nblocks)])
+    assert np.array_equal(flags.cpu().numpy(), (rmax / 1e-6 > 1.0).astype(np.uint8))
+
+
+def test_block_features_vs_oracle(B, state):
+    spec, m, Pz = state
+    f = B.block_features(m, Pz).cpu().numpy()
+    U = Pz.cpu().numpy()
+    ref = np.zeros((spec.nblocks, 16), dtype=np.float32)
+    ol.oracle().lib.orc_block_features(ol.rows(U), spec.blocks, spec.nblocks, ref.ctypes.data_as(C.c_void_p))
+    assert np.allclose(f, ref, rtol=1e-6, atol=1e-6)
+
+
+# ---- float64 numpy restatement of the network --------------------------------
+def _split(p):
+    return (p[0:1024].reshape(64, 16), p[1024:1088], p[1088:5184].reshape(64, 64), p[5184:5248],
+            p[5248:5312], p[5312])
+
+
+def _gelu(a):
+    from scipy.special import erf
+    return 0.5 * a * (1.0 + erf(a / np.sqrt(2.0)))
+
+
+def _gelu_grad(a):
+    from scipy.special import erf
+    return 0.5 * (1.0 + erf(a / np.sqrt(2.0))) + a * np.exp(-0.5 * a * a) / np.sqrt(2 * np.pi)
+
+
+def _np_forward_backward(p, norm, X, Y, Cw):
+    W1, b1, W2, b2, W3, b3 = _split(p)
+    x = (X - norm[:16]) * norm[16:]
+    a1 = x @ W1.T + b1
+    h1 = _gelu(a1)
+    a2 = h1 @ W2.T + b2
+    h2 = _gelu(a2)
+    z = h2 @ W3 + b3
+    n = len(X)
+    loss = np.sum(Cw * (np.maximum(z, 0) - z * Y + np.log1p(np.exp(-np.abs(z))))) / n
+    dz = Cw * (1 / (1 + np.exp(-z)) - Y) / n
+    gW3 = h2.T @ dz
+    gb3 = dz.sum()
+    da2 = np.outer(dz, W3) * _gelu_grad(a2)
+    gW2 = da2.T @ h1
+    gb2 = da2.sum(0)
+    da1 = (da2 @ W2) * _gelu_grad(a1)
+    gW1 = da1.T @ x
+    gb1 = da1.sum(0)
+    g = np.concatenate([gW1.ravel(), gb1, gW2.ravel(), gb2, gW3, [gb3]])
+    return z, loss, g
+
+
+def test_mlp_forward_backward_vs_numpy(B):
+    net = B.RemeshMLP(seed=3)
+    rng = np.random.default_rng(0)
+    n = 1000
+    X = torch.tensor(rng.standard_normal((n, 16)) * 2 + 1, dtype=torch.float32, device="cuda")
+    Y = torch.tensor((rng.random(n) < 0.3).astype(np.float32), device="cuda")
+    Cw = torch.tensor(rng.uniform(0.5, 2.0, n).astype(np.float32), device="cuda")
+    net.set_norm(X)
+    z = net.logits(X)
+    g, loss = net.grad(X, Y, Cw)
+    torch.cuda.synchronize()
+    p = net.wq.float().cpu().numpy().astype(np.float64)  # the BF16 values the kernels use
+    norm = net.norm.cpu().numpy().astype(np.float64)
+    zr, lr, gr = _np_forward_backward(p, norm, X.cpu().numpy().astype(np.float64), Y.cpu().numpy(),
+                                      Cw.cpu().numpy())
+    assert np.allclose(z.cpu().numpy(), zr, rtol=1e-4, atol=1e-4)
+    assert abs(loss.item() - lr) <= 1e-5 * abs(lr)
+    gg = g.cpu().numpy()
+    assert np.abs(gg - gr).max() <= 1e-3 * np.abs(gr).max(), np.abs(gg - gr).max() / np.abs(gr).max()
+
+
+def test_adam_step_vs_numpy(B):
+    net = B.RemeshMLP(seed=4)
+    rng = np.random.default_rng(1)
+    g = torch.tensor(rng.standard_normal(B.MLP_NPARAM).astype(np.float32), device="cuda")
+    p0 = net.master.cpu().numpy().astype(np.float64)
+    net.step(g, lr=1e-2)
+    torch.cuda.synchronize()
+    gn = g.cpu().numpy().astype(np.float64)
+    m = 0.1 * gn
+    v = 0.001 * gn * gn
+    ref = p0 - 1e-2 * (m / 0.1) / (np.sqrt(v / 0.001) + 1e-8)
+    assert np.allclose(net.master.cpu().numpy(), ref, rtol=1e-5, atol=1e-6)
+    assert torch.equal(net.wq, net.master.to(torch.bfloat16))
+
+
+def test_learned_decision_matches_exact_where_it_defers(B, state):
+    """Blocks the network defers (uncertain or audited) get exactly the
+    exact-test flag; with lo=0, hi=1 every block defers and the learned
+    pipeline reproduces the exact test."""
+    spec, m, Pz = state
+    net = B.RemeshMLP(seed=5)
+    net.lo, net.hi = 0.0, 1.0
+    flags, stats = B.remesh_decide(m, Pz, net, tol=1e-6, audit_frac=0.05)
+    _, _, exact = B.wavelet_scores(m, Pz, tol=1e-6)
+    torch.cuda.synchronize()
+    assert torch.equal(flags, exact)
+    assert int(stats[0]) + int(stats[1]) == spec.nblocks
+
+
+def test_trained_indicator_gains_over_exact_test(B):
+    """Train on labels from small mixed-mesh runs, then compare on held-out
+    blocks and on a fresh snapshot: the learned decision defers only a
+    fraction of the blocks to the exact test, misses almost none of the
+    blocks the exact test refines, and takes less time than the exact test
+    on every block."""
+    from bssn_b200 import remesh_train as rt
+    X, Y = rt.collect(16000, dims=(4, 3, 3), log=lambda *a: None)
+    assert 0.005 < Y.mean() < 0.9
+    net = B.RemeshMLP(seed=0)
+    rt.train(net, X[:10000], Y[:10000], steps=600, batch=4096, log=lambda *a: None)
+    pv = torch.sigmoid(net.logits(torch.tensor(X[10000:13000], device="cuda"))).cpu().numpy()
+    net.lo, net.hi = rt.pick_thresholds(pv, Y[10000:13000], fn_target=2e-3)
+    ev = rt.evaluate(net, X[13000:], Y[13000:])
+    assert ev["deferred_fraction"] < 0.5, ev
+    assert ev["false_negative_rate"] <= 0.01, ev
+    tm = rt.time_decisions(net, dims=(4, 3, 3))
+    assert tm["learned_ms"] < tm["exact_ms"], tm
