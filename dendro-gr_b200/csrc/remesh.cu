@@ -17,11 +17,13 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <vector>
 
 #include "bssn_common.cuh"
 #include "mesh.h"
 #include "remesh.h"
+#include "bssn_b200.h"
 
 namespace bssn {
 namespace {
@@ -507,4 +509,68 @@ int launch_remesh_merge(int nblk, const uint8_t* need, const uint8_t* decided,
     return cuda_status(cudaGetLastError());
 }
 
+// ---------------------------------------------------------------------------
+// Gradient without allocation.  Some callers may not allocate device memory
+// at the moment they need a gradient: code running in a CUDA host callback
+// (where CUDA calls are not allowed), code inside a framework that owns every
+// byte of device memory through its own pool and forbids allocations behind
+// its back, or a hard real-time loop that cannot risk an allocation's
+// latency or failure.  For them the per-CTA partial sums that
+// bssn_remesh_mlp_bwd_bf16 keeps in caller-provided scratch live here, in a
+// fixed array in device memory that exists for as long as the library is
+// loaded (on every GPU that loads it).
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kNoAllocMaxSamples = 16384;
+constexpr int kNoAllocParts = kNoAllocMaxSamples / MLP_THREADS;  // 128 CTAs
+// kNoAllocParts x (MLP_NPARAM + 1) floats = 2.72 MB
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocParts * (MLP_NPARAM + 1)];
+
+// device address of g_noalloc_scratch per device ordinal, found once per
+// device with that device current (the array's host-side name is not a
+// device address)
+constexpr int kMaxDevices = 64;
+float* g_noalloc_ptr[kMaxDevices] = {nullptr};
+std::mutex g_noalloc_mu;
+}  // namespace
+
 }  // namespace bssn
+
+extern "C" int bssn_remesh_mlp_bwd_noalloc_bf16(const void* wq_dev, const float* norm_dev,
+                                                const float* x_dev, const float* y_dev,
+                                                const float* c_dev, int n, float* grad_dev,
+                                                float* loss_dev, bssn_stream_t stream) {
+    using namespace bssn;
+    if (!wq_dev || !x_dev || !y_dev || !grad_dev || n < 1) return BSSN_EINVAL;
+    if (n > kNoAllocMaxSamples) return BSSN_ELIMIT;
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (dev < 0 || dev >= kMaxDevices) return BSSN_ELIMIT;
+    float* scratch;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess) return cuda_status(e);
+            g_noalloc_ptr[dev] = static_cast<float*>(p);
+        }
+        scratch = g_noalloc_ptr[dev];
+    }
+    // every CTA overwrites its whole partial slot before the reduction reads
+    // it, so nothing in the array has to start at zero
+    const int parts = (n + MLP_THREADS - 1) / MLP_THREADS;
+    float* gpart = scratch;
+    float* lpart = gpart + (size_t)kNoAllocParts * MLP_NPARAM;
+    const size_t smem = sizeof(float) * (MLP_NPARAM + MLP_THREADS * (IN + 4 * HID + 2));
+    e = cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_status(e);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    mlp_grad_kernel<<<parts, MLP_THREADS, smem, s>>>((const __nv_bfloat16*)wq_dev, norm_dev, x_dev, y_dev,
+                                                     c_dev, n, gpart, lpart);
+    mlp_reduce_kernel<<<(MLP_NPARAM + MLP_THREADS - 1) / MLP_THREADS, MLP_THREADS, 0, s>>>(gpart, parts,
+                                                                                         grad_dev);
+    if (loss_dev) mlp_loss_reduce_kernel<<<1, 32, 0, s>>>(lpart, parts, loss_dev);
+    return cuda_status(cudaGetLastError());
+}

@@ -227,6 +227,22 @@ int bssn_remesh_mlp_bwd_bf16(const void* wq_dev, const float* norm_dev,
                              const float* c_dev, int n, float* grad_dev,
                              float* loss_dev, float* scratch_dev,
                              bssn_stream_t stream);
+/* The same gradient without any device allocation, for callers that cannot
+ * allocate when they need it (a CUDA host callback, where CUDA calls are
+ * forbidden; a framework that owns all device memory through its own pool;
+ * a loop that cannot risk an allocation's latency or failure).  No
+ * counterpart in the reference.  The per-CTA partial sums live in one fixed
+ * array in device memory (2.72 MB, held on every GPU that loads the library
+ * until the process exits), so n is limited to 16384 samples: larger n
+ * returns BSSN_ELIMIT before any launch.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  All calls share
+ * the array: calls whose kernels overlap on the GPU (different streams or
+ * devices' threads racing on one device) race on it; serialise them. */
+int bssn_remesh_mlp_bwd_noalloc_bf16(const void* wq_dev, const float* norm_dev,
+                                     const float* x_dev, const float* y_dev,
+                                     const float* c_dev, int n, float* grad_dev,
+                                     float* loss_dev, bssn_stream_t stream);
 /* Adam step on FP32 master parameters, refreshing the BF16 copy (step t>=1). */
 int bssn_remesh_mlp_step_bf16(float* master_dev, void* wq_dev,
                               const float* grad_dev, float* m_dev, float* v_dev,
