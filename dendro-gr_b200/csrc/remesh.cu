@@ -511,11 +511,11 @@ int launch_remesh_merge(int nblk, const uint8_t* need, const uint8_t* decided,
 
 // ---------------------------------------------------------------------------
 // Gradient without allocation.  Some callers may not allocate device memory
-// at the moment they need a gradient: code running in a CUDA host callback
-// (where CUDA calls are not allowed), code inside a framework that owns every
-// byte of device memory through its own pool and forbids allocations behind
-// its back, or a hard real-time loop that cannot risk an allocation's
-// latency or failure.  For them the per-CTA partial sums that
+// at the moment they need a gradient: an application that owns every byte of
+// device memory through its own pool under a fixed budget and forbids
+// libraries to allocate behind its back, or a time-stepping loop that must
+// not pay the implicit synchronisation and latency of cudaMalloc / cudaFree,
+// nor risk their failure, in the middle of a run.  For them the per-CTA partial sums that
 // bssn_remesh_mlp_bwd_bf16 keeps in caller-provided scratch live here, in a
 // fixed array in device memory that exists for as long as the library is
 // loaded (on every GPU that loads it).

@@ -228,17 +228,19 @@ int bssn_remesh_mlp_bwd_bf16(const void* wq_dev, const float* norm_dev,
                              float* loss_dev, float* scratch_dev,
                              bssn_stream_t stream);
 /* The same gradient without any device allocation, for callers that cannot
- * allocate when they need it (a CUDA host callback, where CUDA calls are
- * forbidden; a framework that owns all device memory through its own pool;
- * a loop that cannot risk an allocation's latency or failure).  No
+ * allocate when they need it: an application that owns all device memory
+ * through its own pool under a fixed budget and forbids libraries to
+ * allocate behind its back, or a time-stepping loop that must not pay the
+ * implicit synchronisation and latency of cudaMalloc / cudaFree, nor risk
+ * their failure, in the middle of a run.  No
  * counterpart in the reference.  The per-CTA partial sums live in one fixed
  * array in device memory (2.72 MB, held on every GPU that loads the library
  * until the process exits), so n is limited to 16384 samples: larger n
  * returns BSSN_ELIMIT before any launch.  The first call on a device looks
  * up the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  All calls share
- * the array: calls whose kernels overlap on the GPU (different streams or
- * devices' threads racing on one device) race on it; serialise them. */
+ * current; make that first call before any stream capture.  All calls on a
+ * device share the array, so calls whose kernels overlap on the GPU (for
+ * example issued on two streams) race on it; serialise them. */
 int bssn_remesh_mlp_bwd_noalloc_bf16(const void* wq_dev, const float* norm_dev,
                                      const float* x_dev, const float* y_dev,
                                      const float* c_dev, int n, float* grad_dev,

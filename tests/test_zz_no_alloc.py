@@ -1,7 +1,8 @@
 """GPU test of bssn_remesh_mlp_bwd_noalloc_bf16: the network-gradient entry
 point for callers that cannot allocate device memory when they need a
-gradient (inside a CUDA host callback, under a framework that owns all device
-memory, in a loop that cannot afford an allocation).  It must give the same
+gradient (an application that owns all device memory through its own pool,
+a time-stepping loop that must not pay cudaMalloc's synchronisation, latency
+or failure mid-run).  It must give the same
 gradient and loss as the regular entry point, which works in caller-provided
 scratch, on consecutive calls (the fixed device array it uses keeps the
 previous call's contents), and must refuse batches above its fixed limit
