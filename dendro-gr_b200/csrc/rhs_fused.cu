@@ -50,18 +50,66 @@ struct Dir3 {
     double d1, d2, ko;
 };
 
+// Interior (centred) stencils, bit-exact: the reference's left-to-right
+// order, every product and sum rounded.
+__device__ __forceinline__ double d1_in(const double* t, int st, const AxisCoef& c) {
+    double r = -t[-3 * st];
+    r = __dadd_rn(r, __dmul_rn(9.0, t[-2 * st]));
+    r = __dadd_rn(r, __dmul_rn(-45.0, t[-st]));
+    r = __dadd_rn(r, __dmul_rn(45.0, t[st]));
+    r = __dadd_rn(r, __dmul_rn(-9.0, t[2 * st]));
+    r = __dadd_rn(r, t[3 * st]);
+    return __dmul_rn(r, c.ih60);
+}
+__device__ __forceinline__ double d2_in(const double* t, int st, const AxisCoef& c) {
+    double r = __dmul_rn(2.0, t[-3 * st]);
+    r = __dadd_rn(r, __dmul_rn(-27.0, t[-2 * st]));
+    r = __dadd_rn(r, __dmul_rn(270.0, t[-st]));
+    r = __dadd_rn(r, __dmul_rn(-490.0, t[0]));
+    r = __dadd_rn(r, __dmul_rn(270.0, t[st]));
+    r = __dadd_rn(r, __dmul_rn(-27.0, t[2 * st]));
+    r = __dadd_rn(r, __dmul_rn(2.0, t[3 * st]));
+    return __dmul_rn(r, c.ih2_180);
+}
+__device__ __forceinline__ double ko_in(const double* t, int st, const AxisCoef& c) {
+    double r = -t[-3 * st];
+    r = __dadd_rn(r, __dmul_rn(6.0, t[-2 * st]));
+    r = __dadd_rn(r, __dmul_rn(-15.0, t[-st]));
+    r = __dadd_rn(r, __dmul_rn(20.0, t[0]));
+    r = __dadd_rn(r, __dmul_rn(-15.0, t[st]));
+    r = __dadd_rn(r, __dmul_rn(6.0, t[2 * st]));
+    r = __dadd_rn(r, -t[3 * st]);
+    return __dmul_rn(c.ko_pre, r);
+}
+
+// One-sided closures near a physical face, kept out of line: they run only
+// in boundary blocks, and inlining every case for every variable and axis
+// made the kernel too large for the instruction cache.
+__device__ __noinline__ Dir3 dir_closure(const double* t, int st, int a, int s, bool blo, bool bhi,
+                                         AxisCoef c, bool second) {
+    Dir3 r;
+    const double* p0 = t - a * st;
+    r.d1 = ex::d1(p0, st, a, s, blo, bhi, c);
+    r.d2 = second ? ex::d2(p0, st, a, s, blo, bhi, c) : 0.0;
+    r.ko = ex::ko(p0, st, a, s, blo, bhi, c);
+    return r;
+}
+
+__device__ __forceinline__ bool near_face(int a, int s, bool blo, bool bhi) {
+    return (blo && a <= 5) || (bhi && a >= s - 6);
+}
+
 // exact first derivative (mixed pass on the evolved variable)
 __device__ __forceinline__ double d1_exact(const double* t, int st, int a, int s,
                                            bool blo, bool bhi, const AxisCoef& c) {
-    return ex::d1(t - a * st, st, a, s, blo, bhi, c);
+    if (near_face(a, s, blo, bhi)) return dir_closure(t, st, a, s, blo, bhi, c, false).d1;
+    return d1_in(t, st, c);
 }
 
 // outer stage of a mixed derivative
 __device__ __forceinline__ double d1_fast(const double* t, int st, int a, int s,
                                           bool blo, bool bhi, const AxisCoef& c) {
-    const bool lo = blo && a <= 5;
-    const bool hi = bhi && a >= s - 6;
-    if (lo || hi) return ex::d1(t - a * st, st, a, s, blo, bhi, c);
+    if (near_face(a, s, blo, bhi)) return dir_closure(t, st, a, s, blo, bhi, c, false).d1;
     const double D1 = t[st] - t[-st], D2 = t[2 * st] - t[-2 * st],
                  D3 = t[3 * st] - t[-3 * st];
     return fma(45.0, D1, fma(-9.0, D2, D3)) * c.ih60;
@@ -71,11 +119,11 @@ __device__ __forceinline__ double d1_fast(const double* t, int st, int a, int s,
 template <bool SECOND>
 __device__ __forceinline__ Dir3 dir_all(const double* t, int st, int a, int s,
                                         bool blo, bool bhi, const AxisCoef& c) {
+    if (near_face(a, s, blo, bhi)) return dir_closure(t, st, a, s, blo, bhi, c, SECOND);
     Dir3 r;
-    const double* p0 = t - a * st;
-    r.d1 = ex::d1(p0, st, a, s, blo, bhi, c);
-    r.d2 = SECOND ? ex::d2(p0, st, a, s, blo, bhi, c) : 0.0;
-    r.ko = ex::ko(p0, st, a, s, blo, bhi, c);
+    r.d1 = d1_in(t, st, c);
+    r.d2 = SECOND ? d2_in(t, st, c) : 0.0;
+    r.ko = ko_in(t, st, c);
     return r;
 }
 
@@ -593,8 +641,8 @@ __device__ __forceinline__ void rhs_brick(const RhsArgs& A, const BssnBlockDesc&
 
 // One brick per CTA: from the task list, or (tasks == nullptr) from
 // blockIdx.x over the bricks of the single block passed by value.
-template <int BX, int BY, int BZ>
-__global__ void __launch_bounds__(Brick<BX, BY, BZ>::THREADS, 1)
+template <int BX, int BY, int BZ, int MINB>
+__global__ void __launch_bounds__(Brick<BX, BY, BZ>::THREADS, MINB)
 rhs_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
            const BrickTask* __restrict__ tasks, BssnBlockDesc single) {
     extern __shared__ __align__(16) double smem[];
@@ -627,10 +675,13 @@ struct TileEntry {
     void (*kern)(RhsArgs, const BssnBlockDesc*, const BrickTask*, BssnBlockDesc);
 };
 
-template <int BX, int BY, int BZ>
+// MINB: resident CTAs per SM the register allocation must allow
+// (1 lets a thread use 255 registers; more CTAs cap registers and trade
+// spills for latency hiding -- the autotuner measures which wins).
+template <int BX, int BY, int BZ, int MINB = 1>
 TileEntry make_entry() {
     using Bk = Brick<BX, BY, BZ>;
-    return TileEntry{BX, BY, BZ, Bk::THREADS, Bk::SMEM_BYTES, rhs_kernel<BX, BY, BZ>};
+    return TileEntry{BX, BY, BZ, Bk::THREADS, Bk::SMEM_BYTES, rhs_kernel<BX, BY, BZ, MINB>};
 }
 
 const TileEntry* tile_table(int* count) {
@@ -638,6 +689,8 @@ const TileEntry* tile_table(int* count) {
         make_entry<8, 8, 4>(),
         make_entry<7, 7, 4>(),
         make_entry<8, 4, 4>(),
+        make_entry<8, 8, 4, 2>(),
+        make_entry<8, 4, 4, 4>(),
     };
     *count = (int)(sizeof(table) / sizeof(table[0]));
     return table;
@@ -735,6 +788,8 @@ long tile_selfcheck(int tile) {
         case 0: return check_tile_shape<8, 8, 4>();
         case 1: return check_tile_shape<7, 7, 4>();
         case 2: return check_tile_shape<8, 4, 4>();
+        case 3: return check_tile_shape<8, 8, 4>();
+        case 4: return check_tile_shape<8, 4, 4>();
         default: return -1;
     }
 }
