@@ -82,17 +82,51 @@ __device__ __forceinline__ double ko_in(const double* t, int st, const AxisCoef&
     return __dmul_rn(c.ko_pre, r);
 }
 
-// One-sided closures near a physical face, kept out of line: they run only
-// in boundary blocks, and inlining every case for every variable and axis
-// made the kernel too large for the instruction cache.
-__device__ __noinline__ Dir3 dir_closure(const double* t, int st, int a, int s, bool blo, bool bhi,
-                                         AxisCoef c, bool second) {
-    Dir3 r;
-    const double* p0 = t - a * st;
-    r.d1 = ex::d1(p0, st, a, s, blo, bhi, c);
-    r.d2 = second ? ex::d2(p0, st, a, s, blo, bhi, c) : 0.0;
-    r.ko = ex::ko(p0, st, a, s, blo, bhi, c);
+// One-sided closures near a physical face (derivs.cpp), table driven: case
+// 0..2 = a = 3,4,5 at a lower face, 3..5 = a = ie-3, ie-2, ie-1 at an upper
+// face (ie = s-3); terms listed in the reference's left-to-right order as
+// (coefficient, offset from a).  A short loop over the table keeps the code
+// small: the closures run only in boundary blocks, and unrolling every case
+// for every variable and axis overflowed the instruction cache.
+__constant__ int kCloN[3][6] = {{5, 5, 4, 4, 5, 5}, {6, 6, 5, 5, 6, 6}, {4, 5, 6, 6, 5, 4}};
+__constant__ double kCloC[3][6][6] = {
+    {{-25, 48, -36, 16, -3}, {-3, -10, 18, -6, 1}, {1, -8, 8, -1},
+     {1, -8, 8, -1}, {-1, 6, -18, 10, 3}, {3, -16, 36, -48, 25}},
+    {{45, -154, 214, -156, 61, -10}, {10, -15, -4, 14, -6, 1}, {-1, 16, -30, 16, -1},
+     {-1, 16, -30, 16, -1}, {1, -6, 14, -4, -15, 10}, {-10, 61, -156, 214, -154, 45}},
+    {{1, -3, 3, -1}, {1, -6, 12, -10, 3}, {1, -6, 15, -19, 12, -3},
+     {1, -6, 15, -19, 12, -3}, {1, -6, 12, -10, 3}, {1, -3, 3, -1}}};
+__constant__ int kCloO[3][6][6] = {
+    {{0, 1, 2, 3, 4}, {-1, 0, 1, 2, 3}, {-2, -1, 1, 2},
+     {-2, -1, 1, 2}, {-3, -2, -1, 0, 1}, {-4, -3, -2, -1, 0}},
+    {{0, 1, 2, 3, 4, 5}, {-1, 0, 1, 2, 3, 4}, {-2, -1, 0, 1, 2},
+     {-2, -1, 0, 1, 2}, {-4, -3, -2, -1, 0, 1}, {-5, -4, -3, -2, -1, 0}},
+    {{3, 2, 1, 0}, {3, 2, 1, 0, -1}, {3, 2, 1, 0, -1, -2},
+     {-3, -2, -1, 0, 1, 2}, {-3, -2, -1, 0, 1}, {-3, -2, -1, 0}}};
+
+__device__ __forceinline__ double closure_fold(const double* t, int st, int kind, int c) {
+    const int n = kCloN[kind][c];
+    double r = __dmul_rn(kCloC[kind][c][0], t[kCloO[kind][c][0] * st]);
+#pragma unroll 1
+    for (int q = 1; q < n; q++) r = __dadd_rn(r, __dmul_rn(kCloC[kind][c][q], t[kCloO[kind][c][q] * st]));
     return r;
+}
+
+__device__ __forceinline__ Dir3 closure3(const double* t, int st, int a, int s, bool blo,
+                                         const AxisCoef& cf, bool second) {
+    const int c = (blo && a <= 5) ? a - 3 : a - (s - 6) + 3;
+    Dir3 r;
+    r.d1 = __dmul_rn(closure_fold(t, st, 0, c), cf.ih12);
+    r.d2 = second ? __dmul_rn(closure_fold(t, st, 1, c), cf.ih2_12) : 0.0;
+    const double smr = (c == 0 || c == 5) ? cf.smr3 : ((c == 1 || c == 4) ? cf.smr2 : cf.smr1);
+    r.ko = __ddiv_rn(closure_fold(t, st, 2, c), smr);
+    return r;
+}
+
+__device__ __forceinline__ double closure_d1(const double* t, int st, int a, int s, bool blo,
+                                             const AxisCoef& cf) {
+    const int c = (blo && a <= 5) ? a - 3 : a - (s - 6) + 3;
+    return __dmul_rn(closure_fold(t, st, 0, c), cf.ih12);
 }
 
 __device__ __forceinline__ bool near_face(int a, int s, bool blo, bool bhi) {
@@ -102,14 +136,14 @@ __device__ __forceinline__ bool near_face(int a, int s, bool blo, bool bhi) {
 // exact first derivative (mixed pass on the evolved variable)
 __device__ __forceinline__ double d1_exact(const double* t, int st, int a, int s,
                                            bool blo, bool bhi, const AxisCoef& c) {
-    if (near_face(a, s, blo, bhi)) return dir_closure(t, st, a, s, blo, bhi, c, false).d1;
+    if (near_face(a, s, blo, bhi)) return closure_d1(t, st, a, s, blo, c);
     return d1_in(t, st, c);
 }
 
 // outer stage of a mixed derivative
 __device__ __forceinline__ double d1_fast(const double* t, int st, int a, int s,
                                           bool blo, bool bhi, const AxisCoef& c) {
-    if (near_face(a, s, blo, bhi)) return dir_closure(t, st, a, s, blo, bhi, c, false).d1;
+    if (near_face(a, s, blo, bhi)) return closure_d1(t, st, a, s, blo, c);
     const double D1 = t[st] - t[-st], D2 = t[2 * st] - t[-2 * st],
                  D3 = t[3 * st] - t[-3 * st];
     return fma(45.0, D1, fma(-9.0, D2, D3)) * c.ih60;
@@ -119,7 +153,7 @@ __device__ __forceinline__ double d1_fast(const double* t, int st, int a, int s,
 template <bool SECOND>
 __device__ __forceinline__ Dir3 dir_all(const double* t, int st, int a, int s,
                                         bool blo, bool bhi, const AxisCoef& c) {
-    if (near_face(a, s, blo, bhi)) return dir_closure(t, st, a, s, blo, bhi, c, SECOND);
+    if (near_face(a, s, blo, bhi)) return closure3(t, st, a, s, blo, c, SECOND);
     Dir3 r;
     r.d1 = d1_in(t, st, c);
     r.d2 = SECOND ? d2_in(t, st, c) : 0.0;
@@ -689,8 +723,6 @@ const TileEntry* tile_table(int* count) {
         make_entry<8, 8, 4>(),
         make_entry<7, 7, 4>(),
         make_entry<8, 4, 4>(),
-        make_entry<8, 8, 4, 2>(),
-        make_entry<8, 4, 4, 4>(),
     };
     *count = (int)(sizeof(table) / sizeof(table[0]));
     return table;
@@ -788,8 +820,6 @@ long tile_selfcheck(int tile) {
         case 0: return check_tile_shape<8, 8, 4>();
         case 1: return check_tile_shape<7, 7, 4>();
         case 2: return check_tile_shape<8, 4, 4>();
-        case 3: return check_tile_shape<8, 8, 4>();
-        case 4: return check_tile_shape<8, 4, 4>();
         default: return -1;
     }
 }
