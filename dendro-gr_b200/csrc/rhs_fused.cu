@@ -114,7 +114,8 @@ __device__ __forceinline__ double closure_fold(const double* t, int st, int kind
 
 __device__ __forceinline__ Dir3 closure3(const double* t, int st, int a, int s, bool blo,
                                          const AxisCoef& cf, bool second) {
-    const int c = (blo && a <= 5) ? a - 3 : a - (s - 6) + 3;
+    int c = (blo && a <= 5) ? a - 3 : a - (s - 6) + 3;
+    c = c < 0 ? 0 : (c > 5 ? 5 : c);
     Dir3 r;
     r.d1 = __dmul_rn(closure_fold(t, st, 0, c), cf.ih12);
     r.d2 = second ? __dmul_rn(closure_fold(t, st, 1, c), cf.ih2_12) : 0.0;
@@ -125,7 +126,8 @@ __device__ __forceinline__ Dir3 closure3(const double* t, int st, int a, int s, 
 
 __device__ __forceinline__ double closure_d1(const double* t, int st, int a, int s, bool blo,
                                              const AxisCoef& cf) {
-    const int c = (blo && a <= 5) ? a - 3 : a - (s - 6) + 3;
+    int c = (blo && a <= 5) ? a - 3 : a - (s - 6) + 3;
+    c = c < 0 ? 0 : (c > 5 ? 5 : c);
     return __dmul_rn(closure_fold(t, st, 0, c), cf.ih12);
 }
 
@@ -276,13 +278,18 @@ __device__ __forceinline__ void rhs_brick(const RhsArgs& A, const BssnBlockDesc&
     };
 
     // zone of this thread
-    // threads past the brick's zone count take zone (0,0,0) so that every
-    // shared-memory read they make stays inside the tile; they store nothing
+    // Threads without a zone (past the brick's zone count, or outside a
+    // ragged brick's extent) compute on the nearest zone of the brick, so
+    // every coordinate they use lies in the block interior [3, s-3) and every
+    // shared-memory read stays inside the staged tile; they store nothing.
     const bool in_brick = tid < Bk::NZ;
-    const int tx = in_brick ? tid % BX : 0;
-    const int ty = in_brick ? (tid / BX) % BY : 0;
-    const int tz = in_brick ? tid / (BX * BY) : 0;
-    const bool active = in_brick && tx < e[0] && ty < e[1] && tz < e[2];
+    const int rx = in_brick ? tid % BX : 0;
+    const int ry = in_brick ? (tid / BX) % BY : 0;
+    const int rz = in_brick ? tid / (BX * BY) : 0;
+    const bool active = in_brick && rx < e[0] && ry < e[1] && rz < e[2];
+    const int tx = rx < e[0] ? rx : e[0] - 1;
+    const int ty = ry < e[1] ? ry : e[1] - 1;
+    const int tz = rz < e[2] ? rz : e[2] - 1;
     ZoneCtx zc;
     zc.s = s;
     zc.bflag = bflag;
@@ -305,10 +312,7 @@ __device__ __forceinline__ void rhs_brick(const RhsArgs& A, const BssnBlockDesc&
     const double* mxk_z = mxk + tx + BX * (ty + BY * (tz + PW));
     const double* myk_z = myk + tx + BX * (ty + BY * (tz + PW));
 
-    // clamp inactive threads to a valid zone so their loads stay in bounds
-    const int za0 = active ? zc.a[0] : PW + o[0];
-    const int za1 = active ? zc.a[1] : PW + o[1];
-    const int za2 = active ? zc.a[2] : PW + o[2];
+    const int za0 = zc.a[0], za1 = zc.a[1], za2 = zc.a[2];
     const int64_t pidx = off + za0 + (int64_t)s * (za1 + (int64_t)s * za2);
     auto pv = [&](int v) { return __ldg(A.u.p[v] + pidx); };
     auto store = [&](int v, double val) {
@@ -793,10 +797,12 @@ long check_tile_shape() {
                     const bool blo = (face & 2) != 0, bhi = (face & 2) != 0;
                     for (int tid = 0; tid < Bk::THREADS; tid++) {
                         const bool in_brick = tid < Bk::NZ;
-                        const int t3[3] = {in_brick ? tid % BX : 0,
+                        const int r3[3] = {in_brick ? tid % BX : 0,
                                            in_brick ? (tid / BX) % BY : 0,
                                            in_brick ? tid / (BX * BY) : 0};
-                        const bool active = in_brick && t3[0] < e[0] && t3[1] < e[1] && t3[2] < e[2];
+                        const bool active = in_brick && r3[0] < e[0] && r3[1] < e[1] && r3[2] < e[2];
+                        int t3[3];
+                        for (int d = 0; d < 3; d++) t3[d] = r3[d] < e[d] ? r3[d] : e[d] - 1;
                         for (int d = 0; d < 3; d++) {
                             const int a = o[d] + PW + t3[d];
                             int pmin, pmax;
@@ -808,6 +814,8 @@ long check_tile_shape() {
                             if (pmin - o[d] < 0 || pmax - o[d] >= T[d]) bad++;
                             if (active && pmax - o[d] >= e[d] + 2 * PW) bad++;
                             if (t3[d] >= B[d]) bad++;
+                            // the closure tables cover a in [3, s-3) only
+                            if (a < 3 || a > s - 4) bad++;
                         }
                     }
                 }
