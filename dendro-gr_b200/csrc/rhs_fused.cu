@@ -112,10 +112,19 @@ __device__ __forceinline__ double closure_fold(const double* t, int st, int kind
     return r;
 }
 
+// Closure case of padded coordinate a (callers guarantee near_face).  Chosen
+// by explicit comparisons: the arithmetic form a - (s - 6) + 3 (clamped)
+// produced the wrong case at a = s - 5 in some inlined copies of this kernel
+// built by nvcc 12.9 for sm_100a (reproducible; the compiled code was not
+// inspected), while this form is bit-exact against the oracle.
+__device__ __forceinline__ int closure_case(int a, int s, bool blo) {
+    return (blo && a == 3) ? 0 : (blo && a == 4) ? 1 : (blo && a == 5) ? 2
+         : (a == s - 6) ? 3 : (a == s - 5) ? 4 : 5;
+}
+
 __device__ __forceinline__ Dir3 closure3(const double* t, int st, int a, int s, bool blo,
                                          const AxisCoef& cf, bool second) {
-    int c = (blo && a <= 5) ? a - 3 : a - (s - 6) + 3;
-    c = c < 0 ? 0 : (c > 5 ? 5 : c);
+    const int c = closure_case(a, s, blo);
     Dir3 r;
     r.d1 = __dmul_rn(closure_fold(t, st, 0, c), cf.ih12);
     r.d2 = second ? __dmul_rn(closure_fold(t, st, 1, c), cf.ih2_12) : 0.0;
@@ -126,8 +135,7 @@ __device__ __forceinline__ Dir3 closure3(const double* t, int st, int a, int s, 
 
 __device__ __forceinline__ double closure_d1(const double* t, int st, int a, int s, bool blo,
                                              const AxisCoef& cf) {
-    int c = (blo && a <= 5) ? a - 3 : a - (s - 6) + 3;
-    c = c < 0 ? 0 : (c > 5 ? 5 : c);
+    const int c = closure_case(a, s, blo);
     return __dmul_rn(closure_fold(t, st, 0, c), cf.ih12);
 }
 
