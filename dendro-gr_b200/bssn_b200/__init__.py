@@ -274,12 +274,18 @@ class PlainRK4:
 
 
 def tiles():
+    """(bx, by, bz, threads) per tile id."""
     out = []
     info = (C.c_int * 4)()
     for t in range(lib.bssn_tile_count()):
         check(lib.bssn_tile_info(t, info), "tile_info")
         out.append(tuple(info))
     return out
+
+
+def tile_mode(t):
+    """0: fused kernel; 1: split derivative + equation passes."""
+    return lib.bssn_tile_mode(t)
 
 
 PLAN_ENFORCE_STAGES = 1

@@ -118,8 +118,10 @@ int bssn_rhs_blocks_f64(bssn_mesh mesh, double* const* rhs_dev, const double* co
     const bssn::BrickTask* tasks;
     int ntasks;
     int r = bssn::mesh_tasks(mesh->st, t, &tasks, &ntasks);
+    if (!r) r = bssn::mesh_scratch(mesh->st, bssn::split_need(mesh->st, t, 0));
     if (r) return r;
-    return bssn::launch_rhs_tasks(t, A, mesh->st->d_blocks, tasks, ntasks, S(stream));
+    return bssn::launch_rhs_tasks(t, A, mesh->st->d_blocks, tasks, ntasks, S(stream),
+                                  mesh->st->d_scratch, mesh->st->scratch_zones);
 }
 
 int bssn_unzip_f64(bssn_mesh mesh, double* const* unzip_dev, const double* const* zip_dev,
@@ -344,6 +346,8 @@ int bssn_remesh_decide_f64(bssn_mesh mesh, const double* const* unzip_dev, const
 int bssn_tile_count(void) { return bssn::tile_count(); }
 
 long bssn_tile_selfcheck(int tile) { return bssn::tile_selfcheck(tile); }
+
+int bssn_tile_mode(int tile) { return bssn::tile_mode(tile); }
 
 int bssn_tile_info(int tile, int info[4]) {
     if (!info) return BSSN_EINVAL;

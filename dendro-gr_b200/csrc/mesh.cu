@@ -130,7 +130,31 @@ void mesh_destroy(MeshState* m) {
     cudaFree(m->d_elems);
     cudaFree(m->d_elem_first);
     for (auto& t : m->tasks) cudaFree(t.second.first);
+    cudaFree(m->d_scratch);
     delete m;
+}
+
+int mesh_scratch(MeshState* m, int64_t zones) {
+    if (zones > kSplitScratchZonesMax) zones = kSplitScratchZonesMax;
+    if (zones <= m->scratch_zones) return 0;
+    cudaFree(m->d_scratch);
+    m->d_scratch = nullptr;
+    m->scratch_zones = 0;
+    if (cudaMalloc((void**)&m->d_scratch, sizeof(double) * kSplitSlots * zones) != cudaSuccess) {
+        cudaGetLastError();
+        return BSSN_ENOMEM;
+    }
+    m->scratch_zones = zones;
+    return 0;
+}
+
+int64_t split_need(MeshState* m, int tile, int side) {
+    if (tile_mode(tile) != 1) return 0;
+    const BrickTask* tk;
+    int nt = 0;
+    if (mesh_tasks_side(m, tile, side, &tk, &nt)) return 0;
+    const int64_t need = (int64_t)nt * tile_zones(tile);
+    return need < kSplitScratchZonesMax ? need : kSplitScratchZonesMax;
 }
 
 int mesh_tasks_side(MeshState* m, int tile, int side, const BrickTask** tasks, int* ntasks) {

@@ -41,6 +41,9 @@ struct MeshState {
     int64_t n_elems = 0;
     // autotuned tile per padded side (0 = not tuned)
     std::map<int, int> tuned;
+    // scratch of the split right-hand side (kSplitSlots doubles per zone)
+    double* d_scratch = nullptr;
+    int64_t scratch_zones = 0;
 };
 
 int mesh_create(const BssnBlockDesc* blocks, int nblocks, const int32_t G[3],
@@ -48,6 +51,11 @@ int mesh_create(const BssnBlockDesc* blocks, int nblocks, const int32_t G[3],
 void mesh_destroy(MeshState* m);
 int mesh_tasks(MeshState* m, int tile, const BrickTask** tasks, int* ntasks);
 int mesh_tasks_side(MeshState* m, int tile, int side, const BrickTask** tasks, int* ntasks);
+// Make the split-path scratch hold at least min(zones, kSplitScratchZonesMax)
+// zones (allocates; call outside stream capture).
+int mesh_scratch(MeshState* m, int64_t zones);
+// Scratch zones a split tile needs for the task list (tile, side), capped.
+int64_t split_need(MeshState* m, int tile, int side);
 int mesh_generate(int mode, const int32_t dims[3], const double p[4], uint64_t seed,
                   double xmin, double L, BssnBlockDesc* blocks, int* nblocks,
                   int32_t G[3], double* h);

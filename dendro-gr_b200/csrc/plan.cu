@@ -59,7 +59,9 @@ int plan_create(MeshState* m, const BssnParams& prm, int flags, Plan** out) {
     std::set<int> sides;
     for (auto& b : m->blocks) sides.insert(b.sz);
     p->sides.assign(sides.begin(), sides.end());
-    // task lists and kernel attributes must exist before any graph capture
+    // task lists, the split-path scratch and kernel attributes must exist
+    // before any graph capture
+    int64_t need = 0;
     for (int side : p->sides) {
         for (int t = 0; t < tile_count(); t++) {
             const BrickTask* tk;
@@ -69,7 +71,13 @@ int plan_create(MeshState* m, const BssnParams& prm, int flags, Plan** out) {
                 plan_destroy(p);
                 return st;
             }
+            need = std::max(need, split_need(m, t, side));
         }
+    }
+    st = mesh_scratch(m, need);
+    if (st) {
+        plan_destroy(p);
+        return st;
     }
     st = prepare_all_tiles();
     if (st) {
@@ -122,7 +130,7 @@ int plan_rhs(Plan* p, cudaStream_t s) {
         const BrickTask* tk;
         int nt;
         int st = mesh_tasks_side(m, t, side, &tk, &nt);
-        if (!st) st = launch_rhs_tasks(t, A, m->d_blocks, tk, nt, s);
+        if (!st) st = launch_rhs_tasks(t, A, m->d_blocks, tk, nt, s, m->d_scratch, m->scratch_zones);
         if (st) return st;
     }
     return 0;
@@ -226,7 +234,7 @@ int plan_autotune(Plan* p, double* const* u, int reps, cudaStream_t s, float* ti
             float tbest = 1e30f;
             for (int r = 0; r <= reps; r++) {
                 cudaEventRecord(e0, s);
-                st = launch_rhs_tasks(t, A, m->d_blocks, tk, ntask, s);
+                st = launch_rhs_tasks(t, A, m->d_blocks, tk, ntask, s, m->d_scratch, m->scratch_zones);
                 cudaEventRecord(e1, s);
                 if (st) break;
                 cudaEventSynchronize(e1);

@@ -1,0 +1,249 @@
+// Split BSSN right-hand side: a derivative pass, then a pointwise equation
+// pass, over the same brick task lists as the fused kernel.
+//
+// The fused kernel keeps every derivative of a zone in registers; its code is
+// one straight run of all 24 variables (about 1 MB of instructions) at 255
+// registers and one CTA per SM, so it stalls on instruction fetch and on
+// FP64 latency.  Here:
+//   * deriv_kernel loops over the 24 variables at run time (one copy of the
+//     staging, mixed-pass and stencil code), at a few dozen registers and
+//     several CTAs per SM, and writes each zone's gradient, second
+//     derivatives and summed KO term to a scratch array;
+//   * eq_kernel evaluates the equations per zone (rhs_equations.cuh, the same
+//     code as the fused kernel) reading those derivatives back.
+// The scratch is slot-major, [slot][task * NZ + thread], so both passes move
+// whole rows of consecutive zones.  A task list longer than the scratch is
+// processed in chunks, each a derivative launch followed by an equation
+// launch on the same stream.
+//
+// Derivatives are bit-identical to the fused kernel's (same stencils, same
+// tiles); the equations are the same code, so both paths give the same RHS.
+#include <cuda_runtime.h>
+
+#include "bssn_common.cuh"
+#include "rhs_brick.cuh"
+#include "rhs_equations.cuh"
+#include "rhs_fused.cuh"
+
+namespace bssn {
+
+namespace {
+
+// Scratch slots per zone: gradient (3) + second derivatives (6) + KO for the
+// 11 variables with second derivatives, gradient + KO for the other 13.
+constexpr int kSlotsSecond = 10;
+constexpr int kSlotsFirst = 4;
+__host__ __device__ constexpr int slot_len(int step) {
+    return stage_second(step) ? kSlotsSecond : kSlotsFirst;
+}
+__host__ __device__ constexpr int slot_base(int step) {
+    int b = 0;
+    for (int k = 0; k < step; k++) b += slot_len(k);
+    return b;
+}
+static_assert(slot_base(NVARS) == kSplitSlots, "scratch slot count");
+
+constexpr int kMinDerivCtas = 3;  // resident derivative CTAs per SM the registers must allow
+// equation pass: variables whose derivatives are in flight ahead of use, and
+// the per-thread ring of scratch slots (shared memory) they land in; one
+// variable more than the prefetch distance, so a copy never targets a row
+// read by the variable just consumed
+constexpr int kPrefetchSteps = 4;
+constexpr int kRingSlots = (kPrefetchSteps + 1) * kSlotsSecond;
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait_pending() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+template <int BX, int BY, int BZ>
+__global__ void __launch_bounds__(Brick<BX, BY, BZ>::THREADS, kMinDerivCtas)
+deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
+             const BrickTask* __restrict__ tasks, double* __restrict__ S, int64_t zs) {
+    using Bk = Brick<BX, BY, BZ>;
+    extern __shared__ __align__(16) double smem[];
+    __shared__ const double* src[NVARS];
+    double* tiles[2] = {smem, smem + Bk::TILE};
+    double* mx = smem + 2 * Bk::TILE;  // mxj | mxk | myk
+    const BrickTask tk = tasks[blockIdx.x];
+    const BssnBlockDesc blk = blocks[tk.blk];
+    const int o[3] = {tk.o[0], tk.o[1], tk.o[2]};
+    const int e[3] = {tk.e[0], tk.e[1], tk.e[2]};
+    const int tid = threadIdx.x;
+    const int s = blk.sz;
+    if (tid < NVARS) src[tid] = u.p[stage_order(tid)] + blk.offset;
+    const BrickThread<Bk> th(tid, e);
+    const BrickZone<Bk> bz(blk, o, th);
+    const StagePlan<Bk> sp(o, e, s, tid);
+    double* out = S + (int64_t)blockIdx.x * Bk::NZ + tid;
+    __syncthreads();
+
+    sp.stage(src[0], tiles[0], tid);
+    int64_t slot = 0;
+#pragma unroll 1
+    for (int step = 0; step < NVARS; step++) {
+        cp_async_wait_all();
+        __syncthreads();
+        const double* cur = tiles[step & 1];
+        if (step + 1 < NVARS) sp.stage(src[step + 1], tiles[(step + 1) & 1], tid);
+        double d1[3], d2[6], ko;
+        if (stage_second(step)) {
+            mixed_pass_fixed<Bk>(cur, mx, o, e, s, blk.bflag, bz.zc.cf, tid);
+            __syncthreads();
+            zone_derivs<true>(bz.zc, cur, mx + bz.mxj_off, mx + Bk::MXJ + bz.mxk_off,
+                              mx + Bk::MXJ + Bk::MXK + bz.mxk_off, bz.mj, bz.mk, d1, d2, ko);
+            if (th.active) {
+                double* w = out + slot * zs;
+#pragma unroll
+                for (int q = 0; q < 3; q++) w[q * zs] = d1[q];
+#pragma unroll
+                for (int q = 0; q < 6; q++) w[(3 + q) * zs] = d2[q];
+                w[9 * zs] = ko;
+            }
+            slot += kSlotsSecond;
+        } else {
+            zone_derivs<false>(bz.zc, cur, nullptr, nullptr, nullptr, 0, 0, d1, d2, ko);
+            if (th.active) {
+                double* w = out + slot * zs;
+#pragma unroll
+                for (int q = 0; q < 3; q++) w[q * zs] = d1[q];
+                w[3 * zs] = ko;
+            }
+            slot += kSlotsFirst;
+        }
+    }
+}
+
+// One thread per zone.  Each thread streams its own zone's scratch slots
+// into its own column of a shared-memory ring with cp.async, kPrefetchSteps
+// variables ahead of the equations that consume them (one commit group per
+// variable; a thread only reads what it copied itself, so no barrier).
+template <int BX, int BY, int BZ>
+__global__ void __launch_bounds__(Brick<BX, BY, BZ>::THREADS, 1)
+eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
+          const BrickTask* __restrict__ tasks, const double* __restrict__ S, int64_t zs) {
+    using Bk = Brick<BX, BY, BZ>;
+    extern __shared__ __align__(16) double ring[];  // [kRingSlots][NZ]
+    const int tid = threadIdx.x;
+    if (tid >= Bk::NZ) return;
+    const BrickTask tk = tasks[blockIdx.x];
+    const int r0 = tid % BX, r1 = (tid / BX) % BY, r2 = tid / (BX * BY);
+    if (r0 >= tk.e[0] || r1 >= tk.e[1] || r2 >= tk.e[2]) return;
+    const double* in = S + (int64_t)blockIdx.x * Bk::NZ + tid;
+    double* col = ring + tid;
+    auto issue = [&](int step) {
+        if (step < NVARS) {
+            const int b = slot_base(step), n = slot_len(step);
+#pragma unroll
+            for (int q = 0; q < kSlotsSecond; q++)
+                if (q < n) cp_async8(col + ((b + q) % kRingSlots) * Bk::NZ, in + (int64_t)(b + q) * zs);
+        }
+        cp_async_commit();  // empty groups past the last variable keep the count fixed
+    };
+#pragma unroll
+    for (int k = 0; k < kPrefetchSteps; k++) issue(k);
+    const BssnBlockDesc blk = blocks[tk.blk];
+    int step = 0;
+    auto get = [&](auto tag, double* d1, double* d2, double& ko) {
+        constexpr bool SECOND = decltype(tag)::value;
+        cp_async_wait_pending<kPrefetchSteps - 1>();
+        const int b = slot_base(step);
+        auto rd = [&](int q) { return col[((b + q) % kRingSlots) * Bk::NZ]; };
+#pragma unroll
+        for (int q = 0; q < 3; q++) d1[q] = rd(q);
+        if (SECOND) {
+#pragma unroll
+            for (int q = 0; q < 6; q++) d2[q] = rd(3 + q);
+            ko = rd(9);
+        } else {
+            ko = rd(3);
+        }
+        issue(step + kPrefetchSteps);  // rows of variables consumed before this one
+        step++;
+    };
+    zone_equations(A, blk, tk.o[0] + PW + r0, tk.o[1] + PW + r1, tk.o[2] + PW + r2, true, get);
+}
+
+struct SplitEntry {
+    int nz, threads;
+    size_t smem, eq_smem;
+    void (*deriv)(ConstVars, const BssnBlockDesc*, const BrickTask*, double*, int64_t);
+    void (*eq)(RhsArgs, const BssnBlockDesc*, const BrickTask*, const double*, int64_t);
+};
+
+template <int BX, int BY, int BZ>
+SplitEntry make_split() {
+    using Bk = Brick<BX, BY, BZ>;
+    return SplitEntry{Bk::NZ, Bk::THREADS, Bk::SMEM_BYTES,
+                      sizeof(double) * kRingSlots * Bk::NZ, deriv_kernel<BX, BY, BZ>,
+                      eq_kernel<BX, BY, BZ>};
+}
+
+// same shapes, same order as the fused tiles
+const SplitEntry* split_table(int* count) {
+    static const SplitEntry table[] = {
+        make_split<8, 8, 4>(),
+        make_split<7, 7, 4>(),
+        make_split<8, 4, 4>(),
+    };
+    *count = (int)(sizeof(table) / sizeof(table[0]));
+    return table;
+}
+
+}  // namespace
+
+int split_shape_count() {
+    int c;
+    split_table(&c);
+    return c;
+}
+
+int split_zone_count(int shape) {
+    int c;
+    const SplitEntry* t = split_table(&c);
+    return (shape < 0 || shape >= c) ? 0 : t[shape].nz;
+}
+
+int prepare_split(int shape) {
+    static bool done[8] = {false};
+    int c;
+    const SplitEntry* t = split_table(&c);
+    if (shape < 0 || shape >= c) return BSSN_EINVAL;
+    if (!done[shape]) {
+        cudaError_t e = cudaFuncSetAttribute(t[shape].deriv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)t[shape].smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(t[shape].eq, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)t[shape].eq_smem);
+        if (e != cudaSuccess) return cuda_status(e);
+        done[shape] = true;
+    }
+    return 0;
+}
+
+int launch_rhs_split(int shape, const RhsArgs& A, const BssnBlockDesc* blocks_dev,
+                     const BrickTask* tasks_dev, int ntasks, double* scratch,
+                     int64_t scratch_zones, cudaStream_t s) {
+    int c;
+    const SplitEntry* tab = split_table(&c);
+    if (shape < 0 || shape >= c) return BSSN_EINVAL;
+    if (ntasks <= 0) return 0;
+    const SplitEntry& t = tab[shape];
+    const int64_t chunk = scratch ? scratch_zones / t.nz : 0;
+    if (chunk <= 0) return BSSN_EINVAL;
+    int st = prepare_split(shape);
+    if (st) return st;
+    const int64_t zs = chunk * t.nz;  // slot stride
+    for (int64_t c0 = 0; c0 < ntasks; c0 += chunk) {
+        const int n = (int)(ntasks - c0 < chunk ? ntasks - c0 : chunk);
+        t.deriv<<<n, t.threads, t.smem, s>>>(A.u, blocks_dev, tasks_dev + c0, scratch, zs);
+        st = cuda_status(cudaGetLastError());
+        if (st) return st;
+        t.eq<<<n, t.threads, t.eq_smem, s>>>(A, blocks_dev, tasks_dev + c0, scratch, zs);
+        st = cuda_status(cudaGetLastError());
+        if (st) return st;
+    }
+    return 0;
+}
+
+}  // namespace bssn

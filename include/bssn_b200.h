@@ -320,10 +320,17 @@ int bssn_mesh_generate(int mode, const int32_t dims[3], const double p[4],
                        BssnBlockDesc* blocks, int* nblocks, int32_t G[3],
                        double* h);
 
-/* Number of compiled tile shapes and their description (bx, by, bz,
- * threads) for the fused RHS kernel. */
+/* Number of compiled tiles and their brick shape (bx, by, bz, threads).
+ * A tile runs its brick shape either fused (one kernel forms the derivatives
+ * in registers and evaluates the equations) or split (a derivative pass
+ * writes every zone's derivatives to a mesh-owned scratch of 162 doubles per
+ * zone, at most 6 Mi zones, allocated by bssn_rk4_plan_create or by the
+ * first bssn_rhs_blocks_f64 call with that tile; an equation pass reads them
+ * back).  Both give the same result. */
 int bssn_tile_count(void);
 int bssn_tile_info(int tile, int info[4]);
+/* 0 fused, 1 split, -1 unknown tile. */
+int bssn_tile_mode(int tile);
 /* Host-only replay of a tile's shared-memory indexing over every brick
  * extent, face case and thread: the number of out-of-range reads (0 when
  * every access is in bounds), or -1 for an unknown tile. */
