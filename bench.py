@@ -43,10 +43,34 @@ MIX = (0.7, 0.2, 0.08, 0.02)
 FLOP_PER_ZONE_STAGE = 6535.0  # 6,439 RHS + 96 RK axpy (per zone, per stage)
 
 
-def fused_rhs_bytes(sides):
-    """Compulsory HBM bytes of one fused-RHS pass: read the 24 padded
-    variables, write the 24 interior right-hand sides."""
-    return sum(8 * 24 * (int(s) ** 3 + (int(s) - 6) ** 3) for s in sides)
+SPLIT_SLOTS = 162  # scratch doubles per zone of the split right-hand side
+
+
+def kernel_bytes(sides, chosen, modes):
+    """Algorithmic HBM bytes of one right-hand-side pass per kernel kind,
+    given the tile chosen per block side and each tile's mode (0 fused,
+    1 split).  Fused: read the 24 padded variables, write the 24 interior
+    right-hand sides.  Derivative pass: read the 24 padded variables, write
+    162 derivative doubles per interior zone.  Equation pass: read the 162
+    derivatives and the 24 variables of each zone, write its 24 right-hand
+    sides."""
+    out = {"fused": 0, "deriv": 0, "eq": 0}
+    for s in sides:
+        s = int(s)
+        pad, inner = s ** 3, (s - 6) ** 3
+        if modes[chosen[s]] == 0:
+            out["fused"] += 8 * 24 * (pad + inner)
+        else:
+            out["deriv"] += 8 * (24 * pad + SPLIT_SLOTS * inner)
+            out["eq"] += 8 * (SPLIT_SLOTS + 24 + 24) * inner
+    return out
+
+
+# DRAM traffic / algorithmic bytes of each kernel, from the ncu capture
+# summarised in profiles/rhs_split_kernels_uniform512.md (read + write bytes
+# of one launch divided by that launch's algorithmic bytes); scales the
+# algorithmic bytes of a full pass to its expected DRAM traffic.
+TRAFFIC_RATIO = {}
 
 
 def step_bytes(sides, n_nodes):
@@ -287,9 +311,15 @@ def main():
     for _ in range(args.warmup):
         plan.step(U, dt)
     torch.cuda.synchronize()
-    # kernel roofline: the fused RHS pass timed alone (CUDA events)
+    # kernel rooflines: every right-hand-side launch timed with CUDA events
+    # on the launch stream (3 passes after a warm-up)
     rhs_ms = C.c_float(0)
     B.check(B.lib.bssn_rk4_plan_time_rhs(plan.h, 3, B.stream_ptr(), C.byref(rhs_ms)), "time_rhs")
+    kt = (C.c_double * 6)()
+    B.lib.bssn_rk4_plan_time_kernels.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_double)]
+    B.check(B.lib.bssn_rk4_plan_time_kernels(plan.h, 3, B.stream_ptr(), kt), "time_kernels")
+    B.lib.bssn_rk4_plan_launches_per_step.argtypes = [C.c_void_p]
+    launches_per_step = B.lib.bssn_rk4_plan_launches_per_step(plan.h)
     scratch = torch.zeros(1, dtype=torch.float64, device="cuda")
     fp64 = C.c_double(0)
     B.lib.bssn_fp64_probe.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_double)]
@@ -373,17 +403,34 @@ def main():
 
     peaks, peak_src = measured_peaks()
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    rb = fused_rhs_bytes(spec.sides)
-    achieved = rb / (rhs_ms.value * 1e-3) / 1e9
+    modes = [B.tile_mode(t) for t in range(len(B.tiles()))]
+    kb = kernel_bytes(spec.sides, chosen, modes)
+    names = {"fused": "bssn::rhs_kernel (fused RHS)", "deriv": "bssn::deriv_kernel (derivative pass)",
+             "eq": "bssn::eq_kernel (equation pass)"}
+    kernels = {}
+    for k, key in enumerate(("fused", "deriv", "eq")):
+        ms, n = kt[k], kt[3 + k]
+        if n <= 0:
+            continue
+        gbs = kb[key] / (ms * 1e-3) / 1e9
+        kernels[key] = {"kernel": names[key], "ms_per_pass": ms, "launches_per_pass": n,
+                        "bytes_per_pass": kb[key], "achieved_gbs": gbs, "frac": gbs / hbm_peak}
+    dom = max(kernels, key=lambda k: kernels[k]["ms_per_pass"])
+    d = kernels[dom]
+    ratio = TRAFFIC_RATIO.get(dom)
     flops_rhs = zones * FLOP_PER_ZONE_STAGE
-    roofline = {"bound": "hbm", "kernel": "fused RHS pass (bssn::rhs_kernel, all buckets)",
-                "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "peak_source": peak_src,
-                "traffic": None, "launch_ms": rhs_ms.value,
-                "bytes_per_launch": rb,
+    roofline = {"bound": "hbm", "kernel": d["kernel"],
+                "achieved": d["achieved_gbs"], "peak": hbm_peak, "unit": "GB/s",
+                "frac": d["frac"], "peak_source": peak_src,
+                "traffic": (ratio * d["bytes_per_pass"] / d["launches_per_pass"]) if ratio else None,
+                "launch_ms": d["ms_per_pass"] / d["launches_per_pass"],
+                "bytes_per_launch": d["bytes_per_pass"] / d["launches_per_pass"],
+                "kernels": kernels,
+                "rhs_pass_ms": rhs_ms.value,
                 "fp64": {"achieved_tflops": flops_rhs / (rhs_ms.value * 1e-3) / 1e12,
                          "peak_tflops": fp64.value, "peak_source": "measured FMA probe",
-                         "frac": flops_rhs / (rhs_ms.value * 1e-3) / 1e12 / fp64.value}}
+                         "frac": flops_rhs / (rhs_ms.value * 1e-3) / 1e12 / fp64.value,
+                         "scope": "whole right-hand-side pass"}}
     sb = step_bytes(spec.sides, spec.n_nodes) * 4
     out = {"metric": "BSSN RK4 zone-updates/s FP64 on 1 B200, batched vs plain; % HBM roofline",
            "value": value, "unit": "zone-updates/s", "n_gpus": world, "steps": args.steps,
@@ -400,7 +447,7 @@ def main():
                         "frac": sb / (ms_step * 1e-3) / 1e9 / hbm_peak},
            "plain": plain, "batched_vs_plain": (value / plain["value"]) if plain else None,
            "e2e": e2e, "clocks": clk,
-           "gpu_launches": args.steps * 4 * (2 + len(chosen)),
+           "gpu_launches": args.steps * launches_per_step,
            "enforce_violations": violations, "state_finite": finite,
            "autotune_ms": {str(k): v for k, v in table.items()}}
     if not args.no_cpu:

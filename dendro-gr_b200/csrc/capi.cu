@@ -206,6 +206,16 @@ int bssn_rk4_plan_time_rhs(bssn_rk4_plan plan, int reps, bssn_stream_t stream, f
     return bssn::plan_time_rhs(plan->p, reps, S(stream), ms);
 }
 
+int bssn_rk4_plan_time_kernels(bssn_rk4_plan plan, int reps, bssn_stream_t stream, double out[6]) {
+    if (!plan || reps < 1 || !out) return BSSN_EINVAL;
+    return bssn::plan_time_kernels(plan->p, reps, S(stream), out);
+}
+
+int bssn_rk4_plan_launches_per_step(bssn_rk4_plan plan) {
+    if (!plan) return BSSN_EINVAL;
+    return bssn::plan_launches_per_step(plan->p);
+}
+
 int bssn_fp64_probe(double* scratch_dev, int iters, bssn_stream_t stream, double* tflops) {
     if (!scratch_dev || iters < 1 || !tflops) return BSSN_EINVAL;
     return bssn::fp64_probe(scratch_dev, iters, S(stream), tflops);

@@ -34,14 +34,22 @@ __global__ void __launch_bounds__(CHUNK) unzip_kernel(MutVars unz, ConstVars zip
     const Chunk c = chunks[blockIdx.x];
     const BssnBlockDesc b = blocks[c.blk];
     const int s = b.sz;
-    const int64_t n = (int64_t)s * s * s;
-    const int64_t p = c.start + threadIdx.x;
-    if (p >= n || threadIdx.x >= c.count) return;
-    const int i = (int)(p % s), j = (int)((p / s) % s), k = (int)(p / ((int64_t)s * s));
+    if (threadIdx.x >= c.count) return;
+    const int p = (int)c.start + (int)threadIdx.x;  // < s^3, fits 32 bits
+    const int i = p % s, j = (p / s) % s, k = p / (s * s);
     const int64_t x = b.g0[0] + i - 3, y = b.g0[1] + j - 3, z = b.g0[2] + k - 3;
     const bool in = x >= 0 && y >= 0 && z >= 0 && x < gx && y < gy && z < gz;
     const int64_t node = in ? x + (int64_t)gx * (y + (int64_t)gy * z) : 0;
-    for (int v = 0; v < nvars; v++) unz.p[v][b.offset + p] = in ? __ldg(zip.p[v] + node) : 0.0;
+    double* const* out = unz.p;
+    if (nvars == NVARS) {  // every load in flight before the first store
+        double v[NVARS];
+#pragma unroll
+        for (int q = 0; q < NVARS; q++) v[q] = in ? __ldg(zip.p[q] + node) : 0.0;
+#pragma unroll
+        for (int q = 0; q < NVARS; q++) out[q][b.offset + p] = v[q];
+        return;
+    }
+    for (int v = 0; v < nvars; v++) out[v][b.offset + p] = in ? __ldg(zip.p[v] + node) : 0.0;
 }
 
 // Gather back.  Each interior node of a block is written only if the block
@@ -54,16 +62,23 @@ __global__ void __launch_bounds__(CHUNK) zip_kernel(MutVars zip, ConstVars unz, 
     const Chunk c = chunks[blockIdx.x];
     const BssnBlockDesc b = blocks[c.blk];
     const int s = b.sz, N = s - 6;
-    const int64_t n = (int64_t)N * N * N;
-    const int64_t q = c.start + threadIdx.x;
-    if (q >= n || threadIdx.x >= c.count) return;
-    const int i = (int)(q % N), j = (int)((q / N) % N), k = (int)(q / ((int64_t)N * N));
+    if (threadIdx.x >= c.count) return;
+    const int q = (int)c.start + (int)threadIdx.x;  // < N^3
+    const int i = q % N, j = (q / N) % N, k = q / (N * N);
     const int64_t x = b.g0[0] + i, y = b.g0[1] + j, z = b.g0[2] + k;
     const bool own = (i < N - 1 || x == gx - 1) && (j < N - 1 || y == gy - 1) &&
                      (k < N - 1 || z == gz - 1);
     if (!own) return;
     const int64_t node = x + (int64_t)gx * (y + (int64_t)gy * z);
     const int64_t p = b.offset + (i + 3) + (int64_t)s * ((j + 3) + (int64_t)s * (k + 3));
+    if (nvars == NVARS) {
+        double v[NVARS];
+#pragma unroll
+        for (int w = 0; w < NVARS; w++) v[w] = __ldg(unz.p[w] + p);
+#pragma unroll
+        for (int w = 0; w < NVARS; w++) zip.p[w][node] = v[w];
+        return;
+    }
     for (int v = 0; v < nvars; v++) zip.p[v][node] = __ldg(unz.p[v] + p);
 }
 

@@ -106,7 +106,7 @@ int plan_tile(const Plan* p, int side) {
     return it == p->mesh->tuned.end() ? 0 : it->second;
 }
 
-int plan_rhs(Plan* p, cudaStream_t s) {
+int plan_rhs(Plan* p, cudaStream_t s, KernelTimer* tm = nullptr) {
     MeshState* m = p->mesh;
     RhsArgs A;
     A.prm = p->prm;
@@ -130,7 +130,7 @@ int plan_rhs(Plan* p, cudaStream_t s) {
         const BrickTask* tk;
         int nt;
         int st = mesh_tasks_side(m, t, side, &tk, &nt);
-        if (!st) st = launch_rhs_tasks(t, A, m->d_blocks, tk, nt, s, m->d_scratch, m->scratch_zones);
+        if (!st) st = launch_rhs_tasks(t, A, m->d_blocks, tk, nt, s, m->d_scratch, m->scratch_zones, tm);
         if (st) return st;
     }
     return 0;
@@ -283,6 +283,47 @@ int plan_time_rhs(Plan* p, int reps, cudaStream_t s, float* ms) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return st ? st : cuda_status(cudaGetLastError());
+}
+
+// Per-kernel timing of the right-hand-side pass: `reps` passes after one
+// warm-up, CUDA events around every launch; out[k] = milliseconds per pass
+// spent in kernels of kind k (fused, derivative, equation), out[3 + k] =
+// launches of kind k per pass.  Blocking.
+int plan_time_kernels(Plan* p, int reps, cudaStream_t s, double out[6]) {
+    int st = plan_rhs(p, s);
+    if (st) return st;
+    double ms[KernelTimer::NKIND] = {0, 0, 0};
+    int n[KernelTimer::NKIND] = {0, 0, 0};
+    for (int r = 0; r < reps && !st; r++) {
+        KernelTimer tm;
+        st = plan_rhs(p, s, &tm);
+        const int st2 = tm.collect(ms, n);
+        if (!st) st = st2;
+    }
+    for (int k = 0; k < KernelTimer::NKIND; k++) {
+        out[k] = reps > 0 ? ms[k] / reps : 0.0;
+        out[3 + k] = reps > 0 ? (double)n[k] / reps : 0.0;
+    }
+    return st ? st : cuda_status(cudaGetLastError());
+}
+
+// Kernel launches of one RK4 step: per stage the ghost fill, the
+// right-hand-side launches of every bucket, and the zip-stage kernel.
+int plan_launches_per_step(Plan* p) {
+    MeshState* m = p->mesh;
+    int rhs = 0;
+    if (p->flags & BSSN_PLAN_PER_BLOCK) {
+        rhs = (int)m->blocks.size();
+    } else {
+        for (int side : p->sides) {
+            const int t = plan_tile(p, side);
+            const BrickTask* tk;
+            int nt = 0;
+            if (mesh_tasks_side(m, t, side, &tk, &nt)) return -1;
+            rhs += rhs_launch_count(t, nt, m->scratch_zones);
+        }
+    }
+    return 4 * (rhs + 2);
 }
 
 namespace {

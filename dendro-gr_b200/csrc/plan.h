@@ -34,6 +34,8 @@ int plan_step(Plan* p, double* const* u, double dt, cudaStream_t s);
 int plan_autotune(Plan* p, double* const* u, int reps, cudaStream_t s, float* times_out);
 int plan_tile(const Plan* p, int side);
 int plan_time_rhs(Plan* p, int reps, cudaStream_t s, float* ms);
+int plan_time_kernels(Plan* p, int reps, cudaStream_t s, double out[6]);
+int plan_launches_per_step(Plan* p);
 int fp64_probe(double* scratch, int iters, cudaStream_t s, double* tflops);
 
 }  // namespace bssn

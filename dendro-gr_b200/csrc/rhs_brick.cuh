@@ -347,6 +347,77 @@ __device__ __forceinline__ void mixed_pass_fixed(const double* tile, double* mx,
     }
 }
 
+// Interior stencils of one direction, computed for every zone whatever its
+// position (the taps of a zone of the brick always lie in the staged tile);
+// zones near a physical face then take the closure instead.  Doing the three
+// directions without branches lets their nine FP64 chains interleave.
+template <bool SECOND>
+__device__ __forceinline__ Dir3 dir_in(const double* t, int st, const AxisCoef& c) {
+    Dir3 r;
+    r.d1 = d1_in(t, st, c);
+    r.d2 = SECOND ? d2_in(t, st, c) : 0.0;
+    r.ko = ko_in(t, st, c);
+    return r;
+}
+__device__ __forceinline__ double d1_fast_in(const double* t, int st, const AxisCoef& c) {
+    const double D1 = t[st] - t[-st], D2 = t[2 * st] - t[-2 * st], D3 = t[3 * st] - t[-3 * st];
+    return fma(45.0, D1, fma(-9.0, D2, D3)) * c.ih60;
+}
+
+// Gradient, pure second derivatives and summed KO of the tile's variable at
+// the zone (interior stencils, closures as an override in boundary blocks).
+template <bool SECOND, class Bk>
+__device__ __forceinline__ void zone_dirs(const ZoneCtx& z, const double* tile, Dir3 r[3]) {
+    const double* t = tile + z.tc;
+    // compile-time strides: every tap is an immediate offset
+    r[0] = dir_in<SECOND>(t, 1, z.cf[0]);
+    r[1] = dir_in<SECOND>(t, Bk::TX, z.cf[1]);
+    r[2] = dir_in<SECOND>(t, Bk::TX * Bk::TY, z.cf[2]);
+    if (z.bflag) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const bool lo = z.bflag & (1u << (2 * d)), hi = z.bflag & (2u << (2 * d));
+            if (near_face(z.a[d], z.s, lo, hi)) r[d] = closure3(t, z.st[d], z.a[d], z.s, lo, z.cf[d], SECOND);
+        }
+    }
+}
+
+// The halo part of the mixed scratch: d/dx on the 6 halo rows in y (mxj) and
+// d/dx, d/dy on the 6 halo planes in z (mxk, myk); the brick part is written
+// by the zones themselves from their own gradient.  Halo row / plane h in
+// 0..5 sits at h (below the brick) or e + h (above it).
+template <class Bk>
+__device__ __forceinline__ void mixed_halo_pass(const double* tile, double* mx, const int o[3],
+                                                const int e[3], int s, unsigned bflag,
+                                                const AxisCoef cf[3], int tid) {
+    constexpr int BX = Bk::BX, BY = Bk::BY, BZ = Bk::BZ, TX = Bk::TX, TY = Bk::TY;
+    constexpr int HJ = BX * 2 * PW * BZ, HK = BX * BY * 2 * PW;
+    for (int idx = tid; idx < HJ + 2 * HK; idx += Bk::THREADS) {
+        if (idx < HJ) {
+            const int i = idx % BX, r = idx / BX, h = r % (2 * PW), k = r / (2 * PW);
+            const int j = h < PW ? h : e[1] + h;
+            if (i < e[0] && k < e[2]) {
+                const double* t = tile + (i + PW) + TX * (j + TY * (k + PW));
+                mx[i + BX * (j + TY * k)] = d1_exact(t, 1, o[0] + PW + i, s, bflag & 1u, bflag & 2u, cf[0]);
+            }
+            continue;
+        }
+        const bool ydir = idx >= HJ + HK;
+        const int q = idx - (ydir ? HJ + HK : HJ);
+        const int i = q % BX, r = q / BX, j = r % BY, h = r / BY;
+        const int k = h < PW ? h : e[2] + h;
+        if (i < e[0] && j < e[1]) {
+            const double* t = tile + (i + PW) + TX * ((j + PW) + TY * k);
+            const int w = i + BX * (j + BY * k);
+            if (ydir)
+                mx[Bk::MXJ + Bk::MXK + w] = d1_exact(t, TX, o[1] + PW + j, s, bflag & 4u, bflag & 8u, cf[1]);
+            else
+                mx[Bk::MXJ + w] = d1_exact(t, 1, o[0] + PW + i, s, bflag & 1u, bflag & 2u, cf[0]);
+        }
+    }
+    (void)BZ;
+}
+
 // The zone a thread works on.  Threads without a zone (past the brick's zone
 // count, or outside a ragged brick's extent) compute on the nearest zone of
 // the brick, so every coordinate they use lies in the block interior [3, s-3)

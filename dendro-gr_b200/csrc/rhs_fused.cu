@@ -280,18 +280,29 @@ void build_tasks(const BssnBlockDesc* blocks, int nblocks, int tile,
 
 int launch_rhs_tasks(int tile, const RhsArgs& A, const BssnBlockDesc* blocks_dev,
                      const BrickTask* tasks_dev, int ntasks, cudaStream_t s,
-                     double* scratch, int64_t scratch_zones) {
+                     double* scratch, int64_t scratch_zones, KernelTimer* tm) {
     int c;
     const TileEntry* tab = tile_table(&c);
     if (tile < 0 || tile >= c) return BSSN_EINVAL;
     if (ntasks <= 0) return 0;
     const TileEntry& t = tab[tile];
     if (t.mode == 1)
-        return launch_rhs_split(t.shape, A, blocks_dev, tasks_dev, ntasks, scratch, scratch_zones, s);
+        return launch_rhs_split(t.shape, A, blocks_dev, tasks_dev, ntasks, scratch, scratch_zones,
+                                s, tm);
     int st = prepare(t);
+    if (!st && tm) st = tm->start(KernelTimer::FUSED, s);
     if (st) return st;
     t.kern<<<ntasks, t.threads, t.smem, s>>>(A, blocks_dev, tasks_dev, BssnBlockDesc{});
-    return cuda_status(cudaGetLastError());
+    st = cuda_status(cudaGetLastError());
+    if (!st && tm) st = tm->stop(s);
+    return st;
+}
+
+int rhs_launch_count(int tile, int ntasks, int64_t scratch_zones) {
+    if (ntasks <= 0) return 0;
+    if (tile_mode(tile) != 1) return 1;
+    const int64_t chunk = scratch_zones / tile_zones(tile);
+    return chunk > 0 ? (int)(2 * ((ntasks + chunk - 1) / chunk)) : 0;
 }
 
 int launch_rhs_single(int tile, const RhsArgs& A, const BssnBlockDesc& blk,

@@ -5,6 +5,7 @@
 
 #include <vector>
 
+#include "bssn_b200.h"
 #include "bssn_common.cuh"
 
 namespace bssn {
@@ -37,11 +38,52 @@ int prepare_all_tiles();
 int tile_info(int tile, int info[4]);
 void build_tasks(const BssnBlockDesc* blocks, int nblocks, int tile,
                  std::vector<BrickTask>& out);
+// Optional timing of every right-hand-side launch: CUDA events recorded on
+// the launch stream around each kernel, summed per kernel kind by collect()
+// (blocking).
+struct KernelTimer {
+    enum Kind { FUSED = 0, DERIV = 1, EQ = 2, NKIND = 3 };
+    std::vector<int> kind;
+    std::vector<cudaEvent_t> ev;  // start, stop per launch
+    int start(int k, cudaStream_t s) {
+        cudaEvent_t a, b;
+        if (cudaEventCreate(&a) != cudaSuccess) return BSSN_ENOMEM;
+        if (cudaEventCreate(&b) != cudaSuccess) {
+            cudaEventDestroy(a);
+            return BSSN_ENOMEM;
+        }
+        kind.push_back(k);
+        ev.push_back(a);
+        ev.push_back(b);
+        return cuda_status(cudaEventRecord(a, s));
+    }
+    int stop(cudaStream_t s) { return cuda_status(cudaEventRecord(ev.back(), s)); }
+    // adds each kind's summed milliseconds to ms[NKIND] and its launch count
+    // to n[NKIND]; releases the events
+    int collect(double ms[NKIND], int n[NKIND]) {
+        int st = 0;
+        for (size_t i = 0; i < kind.size(); i++) {
+            float t = 0;
+            cudaError_t e = cudaEventSynchronize(ev[2 * i + 1]);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]);
+            if (e != cudaSuccess && !st) st = cuda_status(e);
+            ms[kind[i]] += t;
+            n[kind[i]] += 1;
+        }
+        for (auto e : ev) cudaEventDestroy(e);
+        kind.clear();
+        ev.clear();
+        return st;
+    }
+};
+
 // scratch / scratch_zones: the split path's scratch (kSplitSlots * zones
-// doubles); ignored by fused tiles.
+// doubles); ignored by fused tiles.  tm (optional): time each launch.
 int launch_rhs_tasks(int tile, const RhsArgs& A, const BssnBlockDesc* blocks_dev,
                      const BrickTask* tasks_dev, int ntasks, cudaStream_t s,
-                     double* scratch, int64_t scratch_zones);
+                     double* scratch, int64_t scratch_zones, KernelTimer* tm = nullptr);
+// kernel launches launch_rhs_tasks makes for a task list of ntasks bricks
+int rhs_launch_count(int tile, int ntasks, int64_t scratch_zones);
 // one block; a split tile runs its shape fused
 int launch_rhs_single(int tile, const RhsArgs& A, const BssnBlockDesc& blk,
                       cudaStream_t s);
@@ -52,6 +94,6 @@ int split_zone_count(int shape);
 int prepare_split(int shape);
 int launch_rhs_split(int shape, const RhsArgs& A, const BssnBlockDesc* blocks_dev,
                      const BrickTask* tasks_dev, int ntasks, double* scratch,
-                     int64_t scratch_zones, cudaStream_t s);
+                     int64_t scratch_zones, cudaStream_t s, KernelTimer* tm = nullptr);
 
 }  // namespace bssn

@@ -48,8 +48,9 @@ constexpr int kMinDerivCtas = 3;  // resident derivative CTAs per SM the registe
 // the per-thread ring of scratch slots (shared memory) they land in; one
 // variable more than the prefetch distance, so a copy never targets a row
 // read by the variable just consumed
-constexpr int kPrefetchSteps = 4;
+constexpr int kPrefetchSteps = 6;
 constexpr int kRingSlots = (kPrefetchSteps + 1) * kSlotsSecond;
+constexpr int kEqThreads = 128;
 
 template <int N>
 __device__ __forceinline__ void cp_async_wait_pending() {
@@ -75,68 +76,90 @@ deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
     const BrickThread<Bk> th(tid, e);
     const BrickZone<Bk> bz(blk, o, th);
     const StagePlan<Bk> sp(o, e, s, tid);
-    double* out = S + (int64_t)blockIdx.x * Bk::NZ + tid;
+    // next scratch slot of this zone (active threads only advance it)
+    double* w = S + (int64_t)blockIdx.x * Bk::NZ + tid;
     __syncthreads();
 
     sp.stage(src[0], tiles[0], tid);
-    int64_t slot = 0;
 #pragma unroll 1
     for (int step = 0; step < NVARS; step++) {
         cp_async_wait_all();
         __syncthreads();
         const double* cur = tiles[step & 1];
         if (step + 1 < NVARS) sp.stage(src[step + 1], tiles[(step + 1) & 1], tid);
-        double d1[3], d2[6], ko;
         if (stage_second(step)) {
-            mixed_pass_fixed<Bk>(cur, mx, o, e, s, blk.bflag, bz.zc.cf, tid);
+            Dir3 r[3];
+            zone_dirs<true, Bk>(bz.zc, cur, r);
+            // the brick part of the mixed scratch from the zones' own gradient
+            if (th.active) {
+                mx[bz.mxj_off] = r[0].d1;  // the offsets include the halo
+                mx[Bk::MXJ + bz.mxk_off] = r[0].d1;
+                mx[Bk::MXJ + Bk::MXK + bz.mxk_off] = r[1].d1;
+            }
+            mixed_halo_pass<Bk>(cur, mx, o, e, s, blk.bflag, bz.zc.cf, tid);
             __syncthreads();
-            zone_derivs<true>(bz.zc, cur, mx + bz.mxj_off, mx + Bk::MXJ + bz.mxk_off,
-                              mx + Bk::MXJ + Bk::MXK + bz.mxk_off, bz.mj, bz.mk, d1, d2, ko);
-            if (th.active) {
-                double* w = out + slot * zs;
-#pragma unroll
-                for (int q = 0; q < 3; q++) w[q * zs] = d1[q];
-#pragma unroll
-                for (int q = 0; q < 6; q++) w[(3 + q) * zs] = d2[q];
-                w[9 * zs] = ko;
+            const double* mxj = mx + bz.mxj_off;
+            const double* mxk = mx + Bk::MXJ + bz.mxk_off;
+            const double* myk = mx + Bk::MXJ + Bk::MXK + bz.mxk_off;
+            const ZoneCtx& z = bz.zc;
+            double xy = d1_fast_in(mxj, Bk::BX, z.cf[1]);
+            double xz = d1_fast_in(mxk, Bk::BX * Bk::BY, z.cf[2]);
+            double yz = d1_fast_in(myk, Bk::BX * Bk::BY, z.cf[2]);
+            if (z.bflag) {
+                if (near_face(z.a[1], s, z.bflag & 4u, z.bflag & 8u))
+                    xy = closure_d1(mxj, bz.mj, z.a[1], s, z.bflag & 4u, z.cf[1]);
+                if (near_face(z.a[2], s, z.bflag & 16u, z.bflag & 32u)) {
+                    xz = closure_d1(mxk, bz.mk, z.a[2], s, z.bflag & 16u, z.cf[2]);
+                    yz = closure_d1(myk, bz.mk, z.a[2], s, z.bflag & 16u, z.cf[2]);
+                }
             }
-            slot += kSlotsSecond;
+            if (th.active) {
+                const double v[kSlotsSecond] = {r[0].d1, r[1].d1, r[2].d1, r[0].d2, xy, xz,
+                                                r[1].d2, yz, r[2].d2, r[0].ko + r[1].ko + r[2].ko};
+#pragma unroll
+                for (int q = 0; q < kSlotsSecond; q++, w += zs) *w = v[q];
+            }
         } else {
-            zone_derivs<false>(bz.zc, cur, nullptr, nullptr, nullptr, 0, 0, d1, d2, ko);
+            Dir3 r[3];
+            zone_dirs<false, Bk>(bz.zc, cur, r);
             if (th.active) {
-                double* w = out + slot * zs;
+                const double v[kSlotsFirst] = {r[0].d1, r[1].d1, r[2].d1,
+                                               r[0].ko + r[1].ko + r[2].ko};
 #pragma unroll
-                for (int q = 0; q < 3; q++) w[q * zs] = d1[q];
-                w[3 * zs] = ko;
+                for (int q = 0; q < kSlotsFirst; q++, w += zs) *w = v[q];
             }
-            slot += kSlotsFirst;
         }
     }
 }
 
-// One thread per zone.  Each thread streams its own zone's scratch slots
-// into its own column of a shared-memory ring with cp.async, kPrefetchSteps
-// variables ahead of the equations that consume them (one commit group per
-// variable; a thread only reads what it copied itself, so no barrier).
+// One thread per zone, kEqThreads zones of a brick per CTA (a brick of NZ
+// zones takes ceil(NZ / kEqThreads) CTAs), so two CTAs share an SM at 254
+// registers.  Each thread streams its own zone's scratch slots into its own
+// column of a shared-memory ring with cp.async, kPrefetchSteps variables
+// ahead of the equations that consume them (one commit group per variable;
+// a thread only reads what it copied itself, so no barrier).
 template <int BX, int BY, int BZ>
-__global__ void __launch_bounds__(Brick<BX, BY, BZ>::THREADS, 1)
+__global__ void __launch_bounds__(kEqThreads, 2)
 eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
           const BrickTask* __restrict__ tasks, const double* __restrict__ S, int64_t zs) {
     using Bk = Brick<BX, BY, BZ>;
-    extern __shared__ __align__(16) double ring[];  // [kRingSlots][NZ]
+    constexpr int PARTS = (Bk::NZ + kEqThreads - 1) / kEqThreads;
+    extern __shared__ __align__(16) double ring[];  // [kRingSlots][kEqThreads]
     const int tid = threadIdx.x;
-    if (tid >= Bk::NZ) return;
-    const BrickTask tk = tasks[blockIdx.x];
-    const int r0 = tid % BX, r1 = (tid / BX) % BY, r2 = tid / (BX * BY);
+    const int task = blockIdx.x / PARTS;
+    const int l = (blockIdx.x % PARTS) * kEqThreads + tid;  // zone index in the brick
+    if (l >= Bk::NZ) return;
+    const BrickTask tk = tasks[task];
+    const int r0 = l % BX, r1 = (l / BX) % BY, r2 = l / (BX * BY);
     if (r0 >= tk.e[0] || r1 >= tk.e[1] || r2 >= tk.e[2]) return;
-    const double* in = S + (int64_t)blockIdx.x * Bk::NZ + tid;
+    const double* in = S + (int64_t)task * Bk::NZ + l;
     double* col = ring + tid;
     auto issue = [&](int step) {
         if (step < NVARS) {
             const int b = slot_base(step), n = slot_len(step);
 #pragma unroll
             for (int q = 0; q < kSlotsSecond; q++)
-                if (q < n) cp_async8(col + ((b + q) % kRingSlots) * Bk::NZ, in + (int64_t)(b + q) * zs);
+                if (q < n) cp_async8(col + ((b + q) % kRingSlots) * kEqThreads, in + (int64_t)(b + q) * zs);
         }
         cp_async_commit();  // empty groups past the last variable keep the count fixed
     };
@@ -148,7 +171,7 @@ eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
         constexpr bool SECOND = decltype(tag)::value;
         cp_async_wait_pending<kPrefetchSteps - 1>();
         const int b = slot_base(step);
-        auto rd = [&](int q) { return col[((b + q) % kRingSlots) * Bk::NZ]; };
+        auto rd = [&](int q) { return col[((b + q) % kRingSlots) * kEqThreads]; };
 #pragma unroll
         for (int q = 0; q < 3; q++) d1[q] = rd(q);
         if (SECOND) {
@@ -175,7 +198,7 @@ template <int BX, int BY, int BZ>
 SplitEntry make_split() {
     using Bk = Brick<BX, BY, BZ>;
     return SplitEntry{Bk::NZ, Bk::THREADS, Bk::SMEM_BYTES,
-                      sizeof(double) * kRingSlots * Bk::NZ, deriv_kernel<BX, BY, BZ>,
+                      sizeof(double) * kRingSlots * kEqThreads, deriv_kernel<BX, BY, BZ>,
                       eq_kernel<BX, BY, BZ>};
 }
 
@@ -223,7 +246,7 @@ int prepare_split(int shape) {
 
 int launch_rhs_split(int shape, const RhsArgs& A, const BssnBlockDesc* blocks_dev,
                      const BrickTask* tasks_dev, int ntasks, double* scratch,
-                     int64_t scratch_zones, cudaStream_t s) {
+                     int64_t scratch_zones, cudaStream_t s, KernelTimer* tm) {
     int c;
     const SplitEntry* tab = split_table(&c);
     if (shape < 0 || shape >= c) return BSSN_EINVAL;
@@ -236,11 +259,16 @@ int launch_rhs_split(int shape, const RhsArgs& A, const BssnBlockDesc* blocks_de
     const int64_t zs = chunk * t.nz;  // slot stride
     for (int64_t c0 = 0; c0 < ntasks; c0 += chunk) {
         const int n = (int)(ntasks - c0 < chunk ? ntasks - c0 : chunk);
+        if (tm && (st = tm->start(KernelTimer::DERIV, s))) return st;
         t.deriv<<<n, t.threads, t.smem, s>>>(A.u, blocks_dev, tasks_dev + c0, scratch, zs);
         st = cuda_status(cudaGetLastError());
+        if (!st && tm) st = tm->stop(s);
         if (st) return st;
-        t.eq<<<n, t.threads, t.eq_smem, s>>>(A, blocks_dev, tasks_dev + c0, scratch, zs);
+        if (tm && (st = tm->start(KernelTimer::EQ, s))) return st;
+        const int parts = (t.nz + kEqThreads - 1) / kEqThreads;
+        t.eq<<<n * parts, kEqThreads, t.eq_smem, s>>>(A, blocks_dev, tasks_dev + c0, scratch, zs);
         st = cuda_status(cudaGetLastError());
+        if (!st && tm) st = tm->stop(s);
         if (st) return st;
     }
     return 0;

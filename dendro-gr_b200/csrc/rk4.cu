@@ -179,8 +179,8 @@ __global__ void __launch_bounds__(256) zip_stage_kernel(int stage, MutVars im, M
     const int s = b.sz, N = s - 6;
     int bad = 0;
     for (int r = threadIdx.x; r < c.count; r += blockDim.x) {
-        const int64_t q = c.start + r;
-        const int i = (int)(q % N), j = (int)((q / N) % N), k = (int)(q / ((int64_t)N * N));
+        const int q = (int)c.start + r;  // < N^3, fits 32 bits
+        const int i = q % N, j = (q / N) % N, k = q / (N * N);
         const int64_t x = b.g0[0] + i, y = b.g0[1] + j, z = b.g0[2] + k;
         const bool own = (i < N - 1 || x == gx - 1) && (j < N - 1 || y == gy - 1) &&
                          (k < N - 1 || z == gz - 1);
@@ -191,13 +191,18 @@ __global__ void __launch_bounds__(256) zip_stage_kernel(int stage, MutVars im, M
             if (stage < 3) {
                 const double cu = M_(kRK4_U[stage + 1], dt);
                 const double cc = M_(kRK4_C[stage], dt);
+                // all loads before the first store (the pointer arrays may alias)
+                double kk[NVARS], a0[NVARS];
 #pragma unroll
                 for (int q2 = 0; q2 < NVARS; q2++) {
-                    const double kk = __ldg(R.p[q2] + p);
-                    const double u0 = u.p[q2][node];
-                    const double a0 = stage == 0 ? u0 : acc.p[q2][node];
-                    acc.p[q2][node] = A_(a0, M_(cc, kk));
-                    v[q2] = A_(u0, M_(cu, kk));
+                    kk[q2] = __ldg(R.p[q2] + p);
+                    v[q2] = u.p[q2][node];
+                    a0[q2] = stage == 0 ? v[q2] : acc.p[q2][node];
+                }
+#pragma unroll
+                for (int q2 = 0; q2 < NVARS; q2++) {
+                    acc.p[q2][node] = A_(a0[q2], M_(cc, kk[q2]));
+                    v[q2] = A_(v[q2], M_(cu, kk[q2]));
                 }
                 if (enforce) bad += enforce_regs(v, chi_floor);
 #pragma unroll

@@ -294,11 +294,19 @@ int bssn_rk4_plan_tile(bssn_rk4_plan plan, int side);
 /* Enforcement violations accumulated since creation (blocking read). */
 int bssn_rk4_plan_violations(bssn_rk4_plan plan, int* count);
 int bssn_rk4_plan_destroy(bssn_rk4_plan plan);
-/* Average milliseconds of one fused right-hand-side pass over all blocks on
- * the plan's current stage state (CUDA events, after one warm-up).
- * Blocking.  Used for the kernel's roofline. */
+/* Average milliseconds of one right-hand-side pass over all blocks (every
+ * bucket with its tile) on the plan's current stage state (CUDA events,
+ * after one warm-up).  Blocking. */
 int bssn_rk4_plan_time_rhs(bssn_rk4_plan plan, int reps, bssn_stream_t stream,
                            float* ms);
+/* Per-kernel timing of the right-hand-side pass (CUDA events around every
+ * launch, `reps` passes after one warm-up): out[0..2] = milliseconds per pass
+ * in fused, derivative and equation kernels; out[3..5] = their launches per
+ * pass.  Blocking.  Used for the kernels' rooflines. */
+int bssn_rk4_plan_time_kernels(bssn_rk4_plan plan, int reps, bssn_stream_t stream,
+                               double out[6]);
+/* Kernel launches one bssn_rk4_plan_step makes with the current tiles. */
+int bssn_rk4_plan_launches_per_step(bssn_rk4_plan plan);
 /* Measured FP64 fused-multiply-add throughput of this device in TFLOP/s
  * (2 flops per FMA, all SMs, independent chains); scratch_dev: 1 double. */
 int bssn_fp64_probe(double* scratch_dev, int iters, bssn_stream_t stream,
