@@ -103,21 +103,29 @@ struct TileEntry {
 };
 
 template <int BX, int BY, int BZ>
-TileEntry make_entry(int mode, int shape, int fused) {
+TileEntry make_fused(int id) {
     using Bk = Brick<BX, BY, BZ>;
-    return TileEntry{BX, BY, BZ, Bk::THREADS, Bk::SMEM_BYTES,
-                     mode == 0 ? rhs_kernel<BX, BY, BZ, 1> : nullptr, mode, shape, fused};
+    return TileEntry{BX, BY, BZ, Bk::THREADS, Bk::SMEM_BYTES, rhs_kernel<BX, BY, BZ, 1>, 0, -1, id};
+}
+template <int BX, int BY, int BZ>
+TileEntry make_split_tile(int shape, int fused) {
+    using Bk = Brick<BX, BY, BZ>;
+    return TileEntry{BX, BY, BZ, Bk::THREADS, Bk::SMEM_BYTES, nullptr, 1, shape, fused};
 }
 
-// tiles 0..2: fused; 3..5: the same shapes split (rhs_split.cu, same order)
+// tiles 0..2: fused; 3..5: the same shapes split; 6..7: split-only shapes
+// (rhs_split.cu's shape order).  `fused` is the tile a single-block launch
+// of the shape runs (the nearest fused shape for split-only ones).
 const TileEntry* tile_table(int* count) {
     static const TileEntry table[] = {
-        make_entry<8, 8, 4>(0, -1, 0),
-        make_entry<7, 7, 4>(0, -1, 1),
-        make_entry<8, 4, 4>(0, -1, 2),
-        make_entry<8, 8, 4>(1, 0, 0),
-        make_entry<7, 7, 4>(1, 1, 1),
-        make_entry<8, 4, 4>(1, 2, 2),
+        make_fused<8, 8, 4>(0),
+        make_fused<7, 7, 4>(1),
+        make_fused<8, 4, 4>(2),
+        make_split_tile<8, 8, 4>(0, 0),
+        make_split_tile<7, 7, 4>(1, 1),
+        make_split_tile<8, 4, 4>(2, 2),
+        make_split_tile<7, 7, 7>(3, 1),
+        make_split_tile<8, 8, 8>(4, 0),
     };
     *count = (int)(sizeof(table) / sizeof(table[0]));
     return table;
@@ -231,12 +239,15 @@ long tile_selfcheck(int tile) {
     int c;
     const TileEntry* tab = tile_table(&c);
     if (tile < 0 || tile >= c) return -1;
-    switch (tab[tile].fused) {  // split tiles stage and read their tiles the same way
-        case 0: return check_tile_shape<8, 8, 4>();
-        case 1: return check_tile_shape<7, 7, 4>();
-        case 2: return check_tile_shape<8, 4, 4>();
-        default: return -1;
-    }
+    // split tiles stage and read their tiles as fused tiles of the shape do
+    const int b[3] = {tab[tile].bx, tab[tile].by, tab[tile].bz};
+    auto is = [&](int x, int y, int z) { return b[0] == x && b[1] == y && b[2] == z; };
+    if (is(8, 8, 4)) return check_tile_shape<8, 8, 4>();
+    if (is(7, 7, 4)) return check_tile_shape<7, 7, 4>();
+    if (is(8, 4, 4)) return check_tile_shape<8, 4, 4>();
+    if (is(7, 7, 7)) return check_tile_shape<7, 7, 7>();
+    if (is(8, 8, 8)) return check_tile_shape<8, 8, 8>();
+    return -1;
 }
 
 int tile_count() {

@@ -43,7 +43,11 @@ __host__ __device__ constexpr int slot_base(int step) {
 }
 static_assert(slot_base(NVARS) == kSplitSlots, "scratch slot count");
 
-constexpr int kMinDerivCtas = 3;  // resident derivative CTAs per SM the registers must allow
+// resident derivative CTAs per SM the register allocation must allow: 3 for
+// bricks of up to 256 zones (80 registers), fewer for larger bricks
+__host__ __device__ constexpr int deriv_min_ctas(int threads) {
+    return threads <= 256 ? 3 : (threads <= 384 ? 2 : 1);
+}
 // equation pass: variables whose derivatives are in flight ahead of use, and
 // the per-thread ring of scratch slots (shared memory) they land in; one
 // variable more than the prefetch distance, so a copy never targets a row
@@ -58,7 +62,8 @@ __device__ __forceinline__ void cp_async_wait_pending() {
 }
 
 template <int BX, int BY, int BZ>
-__global__ void __launch_bounds__(Brick<BX, BY, BZ>::THREADS, kMinDerivCtas)
+__global__ void __launch_bounds__(Brick<BX, BY, BZ>::THREADS,
+                                   deriv_min_ctas(Brick<BX, BY, BZ>::THREADS))
 deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
              const BrickTask* __restrict__ tasks, double* __restrict__ S, int64_t zs) {
     using Bk = Brick<BX, BY, BZ>;
@@ -202,12 +207,15 @@ SplitEntry make_split() {
                       eq_kernel<BX, BY, BZ>};
 }
 
-// same shapes, same order as the fused tiles
+// the fused tiles' shapes in their order, then split-only shapes (bricks too
+// large for the fused kernel's 255 registers per zone)
 const SplitEntry* split_table(int* count) {
     static const SplitEntry table[] = {
         make_split<8, 8, 4>(),
         make_split<7, 7, 4>(),
         make_split<8, 4, 4>(),
+        make_split<7, 7, 7>(),
+        make_split<8, 8, 8>(),
     };
     *count = (int)(sizeof(table) / sizeof(table[0]));
     return table;
