@@ -46,15 +46,20 @@ FLOP_PER_ZONE_STAGE = 6535.0  # 6,439 RHS + 96 RK axpy (per zone, per stage)
 SPLIT_SLOTS = 162  # scratch doubles per zone of the split right-hand side
 
 
-def kernel_bytes(sides, chosen, modes):
-    """Algorithmic HBM bytes of one right-hand-side pass per kernel kind,
-    given the tile chosen per block side and each tile's mode (0 fused,
-    1 split).  Fused: read the 24 padded variables, write the 24 interior
-    right-hand sides.  Derivative pass: read the 24 padded variables, write
-    162 derivative doubles per interior zone.  Equation pass: read the 162
-    derivatives and the 24 variables of each zone, write its 24 right-hand
-    sides."""
+def kernel_bytes(sides, chosen, modes, n_nodes, direct):
+    """Algorithmic HBM bytes of one right-hand-side pass per kernel kind.
+    Direct plans (split tiles on the zipped grid): the derivative pass reads
+    the 24 zipped variables once and writes 162 derivative doubles per node;
+    the equation pass reads them and the node's 24 variables and writes its
+    24 right-hand sides.  Padded plans, per block by the tile chosen for its
+    side (mode 0 fused, 1 split): fused reads the 24 padded variables and
+    writes the 24 interior right-hand sides; split writes / reads the 162
+    derivative doubles of every interior zone in between."""
     out = {"fused": 0, "deriv": 0, "eq": 0}
+    if direct:
+        out["deriv"] = 8 * (24 + SPLIT_SLOTS) * int(n_nodes)
+        out["eq"] = 8 * (SPLIT_SLOTS + 24 + 24) * int(n_nodes)
+        return out
     for s in sides:
         s = int(s)
         pad, inner = s ** 3, (s - 6) ** 3
@@ -74,9 +79,10 @@ TRAFFIC_RATIO = {}
 
 
 def step_bytes(sides, n_nodes):
-    """Compulsory bytes of one RK stage of this implementation: ghost fill
-    (read zipped, write padded), fused RHS (read padded, write interior),
-    zip + update (read RHS, u, acc; write stage state and acc)."""
+    """Compulsory HBM bytes of one RK stage of the padded plan: ghost fill
+    (read zipped, write padded), right-hand side (read padded, write
+    interior), zip + update (read RHS, u, acc; write stage state and acc).
+    The split right-hand side's derivative round trip is not included."""
     pad = sum(int(s) ** 3 for s in sides)
     inner = sum((int(s) - 6) ** 3 for s in sides)
     n_nodes = int(n_nodes)
@@ -404,7 +410,7 @@ def main():
     peaks, peak_src = measured_peaks()
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     modes = [B.tile_mode(t) for t in range(len(B.tiles()))]
-    kb = kernel_bytes(spec.sides, chosen, modes)
+    kb = kernel_bytes(spec.sides, chosen, modes, spec.n_nodes, direct=False)
     names = {"fused": "bssn::rhs_kernel (fused RHS)", "deriv": "bssn::deriv_kernel (derivative pass)",
              "eq": "bssn::eq_kernel (equation pass)"}
     kernels = {}

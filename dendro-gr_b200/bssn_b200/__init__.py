@@ -291,6 +291,7 @@ def tile_mode(t):
 PLAN_ENFORCE_STAGES = 1
 PLAN_GRAPH = 2
 PLAN_PER_BLOCK = 4
+PLAN_DIRECT = 8
 
 
 class RK4Plan:

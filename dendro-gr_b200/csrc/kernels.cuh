@@ -24,5 +24,9 @@ int launch_zip(const MeshState* m, double* const* zip, const double* const* unz,
 int launch_zip_stage(const MeshState* m, int stage, double* const* im, double* const* acc,
                      double* const* u, const double* const* R, double dt, int enforce,
                      double chi_floor, int* status, cudaStream_t s);
+// the zip-stage algebra with R already on the zipped grid (n nodes)
+int launch_node_stage(int stage, double* const* im, double* const* acc, double* const* u,
+                      const double* const* R, int64_t n, double dt, int enforce,
+                      double chi_floor, int* status, cudaStream_t s);
 
 }  // namespace bssn

@@ -172,6 +172,19 @@ int64_t split_need(MeshState* m, int tile, int side) {
     return need < kSplitScratchZonesMax ? need : kSplitScratchZonesMax;
 }
 
+namespace {
+// Z-order (Morton) key of a block's first interior node in octant units
+// (6 nodes per octant), 21 bits per axis: for the leaves of an octree this is
+// the space-filling-curve order, so consecutive blocks are neighbours.
+uint64_t morton_key(const BssnBlockDesc& b) {
+    uint64_t k = 0;
+    const uint64_t c[3] = {(uint64_t)(b.g0[0] / 6), (uint64_t)(b.g0[1] / 6), (uint64_t)(b.g0[2] / 6)};
+    for (int bit = 20; bit >= 0; bit--)
+        for (int d = 2; d >= 0; d--) k = (k << 1) | ((c[d] >> bit) & 1u);
+    return k;
+}
+}  // namespace
+
 int mesh_tasks_side(MeshState* m, int tile, int side, const BrickTask** tasks, int* ntasks) {
     const auto key = std::make_pair(tile, side);
     auto it = m->tasks.find(key);
@@ -179,7 +192,12 @@ int mesh_tasks_side(MeshState* m, int tile, int side, const BrickTask** tasks, i
         std::vector<BrickTask> all, h;
         build_tasks(m->blocks.data(), (int)m->blocks.size(), tile, all);
         for (auto& t : all)
-            if (side == 0 || m->blocks[t.blk].sz == side) h.push_back(t);
+            if (side <= 0 || m->blocks[t.blk].sz == side) h.push_back(t);
+        if (side < 0) {  // all blocks, Z-order of their origins (bricks of a block stay together)
+            std::stable_sort(h.begin(), h.end(), [&](const BrickTask& a, const BrickTask& b) {
+                return morton_key(m->blocks[a.blk]) < morton_key(m->blocks[b.blk]);
+            });
+        }
         BrickTask* d = nullptr;
         int st = upload(h, &d);
         if (st) return st;

@@ -50,6 +50,10 @@ int mesh_create(const BssnBlockDesc* blocks, int nblocks, const int32_t G[3],
                 MeshState** out);
 void mesh_destroy(MeshState* m);
 int mesh_tasks(MeshState* m, int tile, const BrickTask** tasks, int* ntasks);
+// Brick tasks of one tile for the blocks of padded side `side` (in block
+// order), for all blocks (side 0, block order) or for all blocks in the
+// Z-order of their origins (side kAllZOrder).
+constexpr int kAllZOrder = -1;
 int mesh_tasks_side(MeshState* m, int tile, int side, const BrickTask** tasks, int* ntasks);
 // Make the split-path scratch hold at least min(zones, kSplitScratchZonesMax)
 // zones (allocates; call outside stream capture).

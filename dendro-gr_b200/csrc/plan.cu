@@ -43,15 +43,25 @@ int plan_create(MeshState* m, const BssnParams& prm, int flags, Plan** out) {
     const int64_t nu = m->unzip_size;
     const int64_t nn = (int64_t)m->G[0] * m->G[1] * m->G[2];
     p->n_nodes = nn;
-    int st = alloc(&p->P, (size_t)NVARS * nu);
-    if (!st) st = alloc(&p->R, (size_t)NVARS * nu);
+    // node indices of the direct path are 32-bit
+    p->direct = (flags & BSSN_PLAN_DIRECT) && !(flags & BSSN_PLAN_PER_BLOCK) &&
+                nn < (int64_t(1) << 31);
+    int st = 0;
+    if (p->direct) {
+        st = alloc(&p->Rz, (size_t)NVARS * nn);
+        if (!st) st = cuda_status(cudaMemset(p->Rz, 0, sizeof(double) * NVARS * nn));
+    } else {
+        st = alloc(&p->P, (size_t)NVARS * nu);
+        if (!st) st = alloc(&p->R, (size_t)NVARS * nu);
+        // padded buffers start at zero so never-written points stay finite
+        if (!st) st = cuda_status(cudaMemset(p->P, 0, sizeof(double) * NVARS * nu));
+        if (!st) st = cuda_status(cudaMemset(p->R, 0, sizeof(double) * NVARS * nu));
+    }
     if (!st) st = alloc(&p->im, (size_t)NVARS * nn);
     if (!st) st = alloc(&p->acc, (size_t)NVARS * nn);
+    if (!st) st = cuda_status(cudaMemset(p->im, 0, sizeof(double) * NVARS * nn));
     if (!st && cudaMalloc((void**)&p->status, sizeof(int)) != cudaSuccess) st = BSSN_ENOMEM;
     if (!st) st = cuda_status(cudaMemset(p->status, 0, sizeof(int)));
-    // padded buffers start at zero so never-written points stay finite
-    if (!st) st = cuda_status(cudaMemset(p->P, 0, sizeof(double) * NVARS * nu));
-    if (!st) st = cuda_status(cudaMemset(p->R, 0, sizeof(double) * NVARS * nu));
     if (st) {
         plan_destroy(p);
         return st;
@@ -62,16 +72,20 @@ int plan_create(MeshState* m, const BssnParams& prm, int flags, Plan** out) {
     // task lists, the split-path scratch and kernel attributes must exist
     // before any graph capture
     int64_t need = 0;
-    for (int side : p->sides) {
+    // direct plans: one Z-ordered list over all blocks per split tile;
+    // padded plans: one list per block-size bucket and tile
+    std::vector<int> keys = p->direct ? std::vector<int>{kAllZOrder} : p->sides;
+    for (int key : keys) {
         for (int t = 0; t < tile_count(); t++) {
+            if (p->direct && tile_mode(t) != 1) continue;
             const BrickTask* tk;
             int nt;
-            st = mesh_tasks_side(m, t, side, &tk, &nt);
+            st = mesh_tasks_side(m, t, key, &tk, &nt);
             if (st) {
                 plan_destroy(p);
                 return st;
             }
-            need = std::max(need, split_need(m, t, side));
+            need = std::max(need, split_need(m, t, key));
         }
     }
     st = mesh_scratch(m, need);
@@ -93,6 +107,7 @@ void plan_destroy(Plan* p) {
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
     if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
+    cudaFree(p->Rz);
     cudaFree(p->P);
     cudaFree(p->R);
     cudaFree(p->im);
@@ -101,15 +116,39 @@ void plan_destroy(Plan* p) {
     delete p;
 }
 
+// The tile a plan runs for blocks of side `side`: direct plans run one split
+// tile over all blocks (tuned under the key kAllZOrder), padded plans the
+// tile tuned for the side.
 int plan_tile(const Plan* p, int side) {
-    auto it = p->mesh->tuned.find(side);
-    return it == p->mesh->tuned.end() ? 0 : it->second;
+    auto it = p->mesh->tuned.find(p->direct ? kAllZOrder : side);
+    const int t = it == p->mesh->tuned.end() ? -1 : it->second;
+    if (p->direct) return (t >= 0 && tile_mode(t) == 1) ? t : default_split_tile();
+    return t >= 0 ? t : 0;
 }
 
-int plan_rhs(Plan* p, cudaStream_t s, KernelTimer* tm = nullptr) {
+// One right-hand-side pass over every bucket.  Direct plans read the zipped
+// stage state `src` and write Rz; the others read the padded P (filled by
+// the ghost fill) and write R.
+int plan_rhs(Plan* p, cudaStream_t s, KernelTimer* tm, const double* const* src) {
     MeshState* m = p->mesh;
     RhsArgs A;
     A.prm = p->prm;
+    if (p->direct) {
+        double* Rz[NVARS];
+        set_ptrs(p->Rz, p->n_nodes, Rz);
+        for (int v = 0; v < NVARS; v++) {
+            A.u.p[v] = src[v];
+            A.rhs.p[v] = Rz[v];
+        }
+        const int t = plan_tile(p, kAllZOrder);
+        const BrickTask* tk;
+        int nt;
+        int st = mesh_tasks_side(m, t, kAllZOrder, &tk, &nt);
+        if (!st)
+            st = launch_rhs_tasks(t, A, m->d_blocks, tk, nt, s, m->d_scratch, m->scratch_zones, tm,
+                                  m->G);
+        return st;
+    }
     double* Pp[NVARS];
     double* Rp[NVARS];
     set_ptrs(p->P, m->unzip_size, Pp);
@@ -147,10 +186,22 @@ int plan_enqueue(Plan* p, double* const* u, double dt, cudaStream_t s) {
     set_ptrs(p->im, p->n_nodes, Ip);
     set_ptrs(p->acc, p->n_nodes, Ap);
     const int enf = (p->flags & BSSN_PLAN_ENFORCE_STAGES) ? 1 : 0;
+    if (p->direct) {
+        double* Rz[NVARS];
+        set_ptrs(p->Rz, p->n_nodes, Rz);
+        for (int stage = 0; stage < 4; stage++) {
+            const double* const* src = stage == 0 ? (const double* const*)u : (const double* const*)Ip;
+            int st = plan_rhs(p, s, nullptr, src);
+            if (!st) st = launch_node_stage(stage, Ip, Ap, u, Rz, p->n_nodes, dt, enf,
+                                            p->prm.chi_floor, p->status, s);
+            if (st) return st;
+        }
+        return 0;
+    }
     for (int stage = 0; stage < 4; stage++) {
         const double* const* src = stage == 0 ? (const double* const*)u : (const double* const*)Ip;
         int st = launch_unzip(m, Pp, src, NVARS, s);
-        if (!st) st = plan_rhs(p, s);
+        if (!st) st = plan_rhs(p, s, nullptr, nullptr);
         if (!st) st = launch_zip_stage(m, stage, Ip, Ap, u, Rp, dt, enf, p->prm.chi_floor,
                                        p->status, s);
         if (st) return st;
@@ -206,32 +257,84 @@ int plan_step(Plan* p, double* const* u, double dt, cudaStream_t s) {
 // and keep the fastest.  Blocking.
 int plan_autotune(Plan* p, double* const* u, int reps, cudaStream_t s, float* times_out) {
     MeshState* m = p->mesh;
-    double* Pp[NVARS];
-    set_ptrs(p->P, m->unzip_size, Pp);
-    int st = launch_unzip(m, Pp, (const double* const*)u, NVARS, s);
-    if (st) return st;
     RhsArgs A;
     A.prm = p->prm;
-    double* Rp[NVARS];
-    set_ptrs(p->R, m->unzip_size, Rp);
-    for (int v = 0; v < NVARS; v++) {
-        A.u.p[v] = Pp[v];
-        A.rhs.p[v] = Rp[v];
+    int st = 0;
+    if (p->direct) {  // split tiles on the zipped state u
+        double* Rz[NVARS];
+        set_ptrs(p->Rz, p->n_nodes, Rz);
+        for (int v = 0; v < NVARS; v++) {
+            A.u.p[v] = u[v];
+            A.rhs.p[v] = Rz[v];
+        }
+    } else {
+        double* Pp[NVARS];
+        set_ptrs(p->P, m->unzip_size, Pp);
+        st = launch_unzip(m, Pp, (const double* const*)u, NVARS, s);
+        if (st) return st;
+        double* Rp[NVARS];
+        set_ptrs(p->R, m->unzip_size, Rp);
+        for (int v = 0; v < NVARS; v++) {
+            A.u.p[v] = Pp[v];
+            A.rhs.p[v] = Rp[v];
+        }
     }
+    const int32_t* zg = p->direct ? m->G : nullptr;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     const int nt = tile_count();
+    if (p->direct) {
+        // every split tile over the whole Z-ordered list; each bucket row of
+        // `times` gets the same figures
+        float best = 1e30f;
+        int best_t = default_split_tile();
+        std::vector<float> tt(nt, 1e30f);
+        for (int t = 0; t < nt && !st; t++) {
+            if (tile_mode(t) != 1) continue;
+            const BrickTask* tk;
+            int ntask;
+            st = mesh_tasks_side(m, t, kAllZOrder, &tk, &ntask);
+            for (int r = 0; r <= reps && !st; r++) {
+                cudaEventRecord(e0, s);
+                st = launch_rhs_tasks(t, A, m->d_blocks, tk, ntask, s, m->d_scratch,
+                                      m->scratch_zones, nullptr, zg);
+                cudaEventRecord(e1, s);
+                if (st) break;
+                cudaEventSynchronize(e1);
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (r > 0) tt[t] = std::min(tt[t], ms);
+            }
+            if (!st && tt[t] < best) {
+                best = tt[t];
+                best_t = t;
+            }
+        }
+        if (!st) m->tuned[kAllZOrder] = best_t;
+        if (times_out)
+            for (size_t i = 0; i < p->sides.size(); i++)
+                for (int t = 0; t < nt; t++) times_out[i * nt + t] = tt[t];
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (p->exec) {  // tile choice changed: recapture on the next step
+            cudaGraphExecDestroy(p->exec);
+            cudaGraphDestroy(p->graph);
+            p->exec = nullptr;
+            p->graph = nullptr;
+        }
+        return st;
+    }
     int idx = 0;
     for (int side : p->sides) {
         float best = 1e30f;
         int best_t = 0;
         for (int t = 0; t < nt; t++) {
+            float tbest = 1e30f;
             const BrickTask* tk;
             int ntask;
             st = mesh_tasks_side(m, t, side, &tk, &ntask);
             if (st) break;
-            float tbest = 1e30f;
             for (int r = 0; r <= reps; r++) {
                 cudaEventRecord(e0, s);
                 st = launch_rhs_tasks(t, A, m->d_blocks, tk, ntask, s, m->d_scratch, m->scratch_zones);
@@ -267,14 +370,24 @@ int plan_autotune(Plan* p, double* const* u, int reps, cudaStream_t s, float* ti
 // Average duration of one full fused-RHS pass (all buckets) on the plan's
 // current padded state, CUDA events on `s` around `reps` back-to-back passes
 // after one warm-up pass.  Blocking.
+// The stage state the timing functions run the right-hand side on: the
+// padded P of the last ghost fill, or (direct) the zipped intermediate state.
+const double* const* timing_src(Plan* p, double* buf[NVARS]) {
+    if (!p->direct) return nullptr;
+    set_ptrs(p->im, p->n_nodes, buf);
+    return (const double* const*)buf;
+}
+
 int plan_time_rhs(Plan* p, int reps, cudaStream_t s, float* ms) {
-    int st = plan_rhs(p, s);
+    double* buf[NVARS];
+    const double* const* src = timing_src(p, buf);
+    int st = plan_rhs(p, s, nullptr, src);
     if (st) return st;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s);
-    for (int r = 0; r < reps && !st; r++) st = plan_rhs(p, s);
+    for (int r = 0; r < reps && !st; r++) st = plan_rhs(p, s, nullptr, src);
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
     float t = 0;
@@ -290,13 +403,15 @@ int plan_time_rhs(Plan* p, int reps, cudaStream_t s, float* ms) {
 // spent in kernels of kind k (fused, derivative, equation), out[3 + k] =
 // launches of kind k per pass.  Blocking.
 int plan_time_kernels(Plan* p, int reps, cudaStream_t s, double out[6]) {
-    int st = plan_rhs(p, s);
+    double* buf[NVARS];
+    const double* const* src = timing_src(p, buf);
+    int st = plan_rhs(p, s, nullptr, src);
     if (st) return st;
     double ms[KernelTimer::NKIND] = {0, 0, 0};
     int n[KernelTimer::NKIND] = {0, 0, 0};
     for (int r = 0; r < reps && !st; r++) {
         KernelTimer tm;
-        st = plan_rhs(p, s, &tm);
+        st = plan_rhs(p, s, &tm, src);
         const int st2 = tm.collect(ms, n);
         if (!st) st = st2;
     }
@@ -314,6 +429,12 @@ int plan_launches_per_step(Plan* p) {
     int rhs = 0;
     if (p->flags & BSSN_PLAN_PER_BLOCK) {
         rhs = (int)m->blocks.size();
+    } else if (p->direct) {
+        const int t = plan_tile(p, kAllZOrder);
+        const BrickTask* tk;
+        int nt = 0;
+        if (mesh_tasks_side(m, t, kAllZOrder, &tk, &nt)) return -1;
+        rhs = rhs_launch_count(t, nt, m->scratch_zones);
     } else {
         for (int side : p->sides) {
             const int t = plan_tile(p, side);
@@ -323,7 +444,7 @@ int plan_launches_per_step(Plan* p) {
             rhs += rhs_launch_count(t, nt, m->scratch_zones);
         }
     }
-    return 4 * (rhs + 2);
+    return 4 * (rhs + (p->direct ? 1 : 2));
 }
 
 namespace {

@@ -15,6 +15,11 @@ struct Plan {
     BssnParams prm;
     int flags = 0;
     int64_t n_nodes = 0;
+    // direct: the right-hand side reads the zipped stage state and writes a
+    // zipped right-hand side (no ghost fill, no padded arrays); otherwise the
+    // ghost fill -> padded right-hand side -> zip-stage sequence
+    bool direct = false;
+    double* Rz = nullptr;   // zipped right-hand side (direct)
     double* P = nullptr;    // padded stage state (24 x unzip size)
     double* R = nullptr;    // padded right-hand side
     double* im = nullptr;   // zipped intermediate stage state

@@ -167,7 +167,9 @@ struct ZoneCtx {
     int a[3];        // padded block coordinates of the zone
     int s;           // padded side
     unsigned bflag;
-    AxisCoef cf[3];
+    // per-axis stencil factors: the same for every zone of a block, so they
+    // live in shared memory (three AxisCoef in registers would take 48)
+    const AxisCoef* cf;
     int tc;          // tile index of the zone
     int st[3];       // tile strides
 };
@@ -297,24 +299,46 @@ __device__ __forceinline__ void mixed_pass(const double* tile, double* mxj, doub
 // tile points idx = tid + k*THREADS (k < ITER) of every variable, so it keeps
 // their offsets from the block's first point (-1: outside the staged region
 // [o, o+e+6)^3 of a ragged brick) in registers.
-template <class Bk>
+//
+// Source of the tile: the padded block (offsets from its first point), or,
+// for blocks of a single-level mesh, the zipped node grid directly (gx > 0:
+// offsets are node indices, points outside the grid are zero -- exactly the
+// values the ghost fill writes there -- marked -2).
+struct ZipGrid {
+    int gx, gy, gz;  // gx == 0: padded input
+};
+
+template <class Bk, bool ZIP>
 struct StagePlan {
     static constexpr int ITER = (Bk::TILE + Bk::THREADS - 1) / Bk::THREADS;
     int goff[ITER];
-    __device__ __forceinline__ StagePlan(const int o[3], const int e[3], int s, int tid) {
+    __device__ __forceinline__ StagePlan(const int o[3], const int e[3], int s, int tid,
+                                         const ZipGrid& g, const int32_t g0[3]) {
 #pragma unroll
         for (int k = 0; k < ITER; k++) {
             const int idx = tid + k * Bk::THREADS;
             const int ti = idx % Bk::TX, r = idx / Bk::TX, tj = r % Bk::TY, tk = r / Bk::TY;
             const bool in = idx < Bk::TILE && ti < e[0] + 2 * PW && tj < e[1] + 2 * PW &&
                             tk < e[2] + 2 * PW;
-            goff[k] = in ? (o[0] + ti) + s * ((o[1] + tj) + s * (o[2] + tk)) : -1;
+            if (!ZIP) {
+                goff[k] = in ? (o[0] + ti) + s * ((o[1] + tj) + s * (o[2] + tk)) : -1;
+            } else {
+                // padded coordinate o + t is node g0 + o + t - 3
+                const int x = g0[0] + o[0] + ti - PW, y = g0[1] + o[1] + tj - PW,
+                          z = g0[2] + o[2] + tk - PW;
+                const bool grid = x >= 0 && y >= 0 && z >= 0 && x < g.gx && y < g.gy && z < g.gz;
+                goff[k] = !in ? -1 : (grid ? x + g.gx * (y + g.gy * z) : -2);
+            }
         }
     }
     __device__ __forceinline__ void stage(const double* src, double* dst, int tid) const {
 #pragma unroll
-        for (int k = 0; k < ITER; k++)
-            if (goff[k] >= 0) cp_async8(dst + tid + k * Bk::THREADS, src + goff[k]);
+        for (int k = 0; k < ITER; k++) {
+            if (goff[k] >= 0)
+                cp_async8(dst + tid + k * Bk::THREADS, src + goff[k]);
+            else if (ZIP && goff[k] == -2)
+                dst[tid + k * Bk::THREADS] = 0.0;
+        }
         cp_async_commit();
     }
 };
@@ -439,6 +463,12 @@ struct BrickThread {
     }
 };
 
+// The block's per-axis stencil factors, written by threads 0..2 into shared
+// memory (visible after the caller's next barrier).
+__device__ __forceinline__ void fill_axis_coefs(AxisCoef* cf, const BssnBlockDesc& blk, int tid) {
+    if (tid < 3) cf[tid] = axis_coef((blk.ptmax[tid] - blk.ptmin[tid]) / (blk.sz - 1));
+}
+
 // Stencil context of a thread's zone in a brick (tile strides, padded
 // coordinates, per-axis coefficients) and its positions in the mixed scratch.
 template <class Bk>
@@ -446,16 +476,15 @@ struct BrickZone {
     ZoneCtx zc;
     int mj, mk;
     int mxj_off, mxk_off;  // offsets of the zone in mxj and in mxk / myk
+    // cf: the block's three AxisCoef in shared memory (fill_axis_coefs)
     __device__ __forceinline__ BrickZone(const BssnBlockDesc& blk, const int o[3],
-                                         const BrickThread<Bk>& th) {
+                                         const BrickThread<Bk>& th, const AxisCoef* cf) {
         const int s = blk.sz;
         zc.s = s;
         zc.bflag = blk.bflag;
+        zc.cf = cf;
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            zc.cf[d] = axis_coef((blk.ptmax[d] - blk.ptmin[d]) / (s - 1));
-            zc.a[d] = o[d] + PW + th.t[d];
-        }
+        for (int d = 0; d < 3; d++) zc.a[d] = o[d] + PW + th.t[d];
         zc.st[0] = 1;
         zc.st[1] = Bk::TX;
         zc.st[2] = Bk::TX * Bk::TY;

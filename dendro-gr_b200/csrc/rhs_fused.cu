@@ -35,8 +35,10 @@ __device__ __forceinline__ void rhs_brick(const RhsArgs& A, const BssnBlockDesc&
     const int tid = threadIdx.x;
     const int s = blk.sz;
     const int64_t off = blk.offset;
+    __shared__ AxisCoef cfs[3];
+    fill_axis_coefs(cfs, blk, tid);  // visible after the first get()'s barrier
     const BrickThread<Bk> th(tid, e);
-    const BrickZone<Bk> bz(blk, o, th);
+    const BrickZone<Bk> bz(blk, o, th, cfs);
 
     int step = 0;
     stage_var<Bk>(A.u.p[stage_order(0)] + off, tiles[0], o, e, s, tid);
@@ -58,7 +60,8 @@ __device__ __forceinline__ void rhs_brick(const RhsArgs& A, const BssnBlockDesc&
         zone_derivs<SECOND>(bz.zc, cur, mxj + bz.mxj_off, mxk + bz.mxk_off, myk + bz.mxk_off,
                             bz.mj, bz.mk, d1, d2, ko);
     };
-    zone_equations(A, blk, bz.zc.a[0], bz.zc.a[1], bz.zc.a[2], th.active, get);
+    const int64_t pidx = off + bz.zc.a[0] + (int64_t)s * (bz.zc.a[1] + (int64_t)s * bz.zc.a[2]);
+    zone_equations(A, blk, bz.zc.a[0], bz.zc.a[1], bz.zc.a[2], pidx, pidx, th.active, get);
 }
 
 }  // namespace
@@ -160,6 +163,18 @@ int tile_mode(int tile) {
     int c;
     const TileEntry* tab = tile_table(&c);
     return (tile < 0 || tile >= c) ? -1 : tab[tile].mode;
+}
+
+int default_split_tile() {
+    int c;
+    const TileEntry* tab = tile_table(&c);
+    int first = -1;
+    for (int t = 0; t < c; t++) {
+        if (tab[t].mode != 1) continue;
+        if (first < 0) first = t;
+        if (tab[t].bx == 7 && tab[t].by == 7 && tab[t].bz == 7) return t;
+    }
+    return first;
 }
 
 int tile_zones(int tile) {
@@ -291,7 +306,8 @@ void build_tasks(const BssnBlockDesc* blocks, int nblocks, int tile,
 
 int launch_rhs_tasks(int tile, const RhsArgs& A, const BssnBlockDesc* blocks_dev,
                      const BrickTask* tasks_dev, int ntasks, cudaStream_t s,
-                     double* scratch, int64_t scratch_zones, KernelTimer* tm) {
+                     double* scratch, int64_t scratch_zones, KernelTimer* tm,
+                     const int32_t* zip_grid) {
     int c;
     const TileEntry* tab = tile_table(&c);
     if (tile < 0 || tile >= c) return BSSN_EINVAL;
@@ -299,7 +315,8 @@ int launch_rhs_tasks(int tile, const RhsArgs& A, const BssnBlockDesc* blocks_dev
     const TileEntry& t = tab[tile];
     if (t.mode == 1)
         return launch_rhs_split(t.shape, A, blocks_dev, tasks_dev, ntasks, scratch, scratch_zones,
-                                s, tm);
+                                s, tm, zip_grid);
+    if (zip_grid) return BSSN_EINVAL;  // the fused kernel reads padded blocks only
     int st = prepare(t);
     if (!st && tm) st = tm->start(KernelTimer::FUSED, s);
     if (st) return st;

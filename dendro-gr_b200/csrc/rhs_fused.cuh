@@ -32,6 +32,7 @@ constexpr int64_t kSplitScratchZonesMax = int64_t(6) << 20;
 
 int tile_count();
 int tile_mode(int tile);   // 0 fused, 1 split, -1 unknown
+int default_split_tile();  // the split tile used before autotuning
 int tile_zones(int tile);  // zones per brick (BX*BY*BZ)
 long tile_selfcheck(int tile);
 int prepare_all_tiles();
@@ -79,9 +80,13 @@ struct KernelTimer {
 
 // scratch / scratch_zones: the split path's scratch (kSplitSlots * zones
 // doubles); ignored by fused tiles.  tm (optional): time each launch.
+// zip_grid (optional, split tiles only): the node-grid dimensions of a
+// single-level mesh; A.u then holds the zipped stage state and A.rhs the
+// zipped right-hand side, written once per node by the block owning it.
 int launch_rhs_tasks(int tile, const RhsArgs& A, const BssnBlockDesc* blocks_dev,
                      const BrickTask* tasks_dev, int ntasks, cudaStream_t s,
-                     double* scratch, int64_t scratch_zones, KernelTimer* tm = nullptr);
+                     double* scratch, int64_t scratch_zones, KernelTimer* tm = nullptr,
+                     const int32_t* zip_grid = nullptr);
 // kernel launches launch_rhs_tasks makes for a task list of ntasks bricks
 int rhs_launch_count(int tile, int ntasks, int64_t scratch_zones);
 // one block; a split tile runs its shape fused
@@ -94,6 +99,7 @@ int split_zone_count(int shape);
 int prepare_split(int shape);
 int launch_rhs_split(int shape, const RhsArgs& A, const BssnBlockDesc* blocks_dev,
                      const BrickTask* tasks_dev, int ntasks, double* scratch,
-                     int64_t scratch_zones, cudaStream_t s, KernelTimer* tm = nullptr);
+                     int64_t scratch_zones, cudaStream_t s, KernelTimer* tm = nullptr,
+                     const int32_t* zip_grid = nullptr);
 
 }  // namespace bssn

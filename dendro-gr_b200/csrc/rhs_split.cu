@@ -61,14 +61,33 @@ __device__ __forceinline__ void cp_async_wait_pending() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-template <int BX, int BY, int BZ>
+// Whether the zone at brick position t owns its node of the zipped grid: a
+// node on a block's upper face belongs to the next block unless the face
+// lies on the grid's upper boundary (the zip's owner rule).
+__device__ __forceinline__ bool owns_node(const BssnBlockDesc& blk, const int o[3], const int t[3],
+                                          const ZipGrid& g) {
+    const int n = blk.sz - 2 * PW;
+    const int gd[3] = {g.gx, g.gy, g.gz};
+    bool own = true;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const int i = o[d] + t[d];  // interior index
+        own = own && (i < n - 1 || blk.g0[d] + i == gd[d] - 1);
+    }
+    return own;
+}
+
+// ZIP: stage from the zipped node grid (g) instead of the padded blocks.
+template <int BX, int BY, int BZ, bool ZIP>
 __global__ void __launch_bounds__(Brick<BX, BY, BZ>::THREADS,
                                    deriv_min_ctas(Brick<BX, BY, BZ>::THREADS))
 deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
-             const BrickTask* __restrict__ tasks, double* __restrict__ S, int64_t zs) {
+             const BrickTask* __restrict__ tasks, double* __restrict__ S, int64_t zs,
+             ZipGrid g) {
     using Bk = Brick<BX, BY, BZ>;
     extern __shared__ __align__(16) double smem[];
     __shared__ const double* src[NVARS];
+    __shared__ AxisCoef cfs[3];
     double* tiles[2] = {smem, smem + Bk::TILE};
     double* mx = smem + 2 * Bk::TILE;  // mxj | mxk | myk
     const BrickTask tk = tasks[blockIdx.x];
@@ -77,11 +96,15 @@ deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
     const int e[3] = {tk.e[0], tk.e[1], tk.e[2]};
     const int tid = threadIdx.x;
     const int s = blk.sz;
-    if (tid < NVARS) src[tid] = u.p[stage_order(tid)] + blk.offset;
+    if (tid < NVARS) src[tid] = u.p[stage_order(tid)] + (ZIP ? 0 : blk.offset);
+    fill_axis_coefs(cfs, blk, tid);
     const BrickThread<Bk> th(tid, e);
-    const BrickZone<Bk> bz(blk, o, th);
-    const StagePlan<Bk> sp(o, e, s, tid);
-    // next scratch slot of this zone (active threads only advance it)
+    const BrickZone<Bk> bz(blk, o, th, cfs);
+    const StagePlan<Bk, ZIP> sp(o, e, s, tid, g, blk.g0);
+    // zones whose derivatives the equation pass reads: every zone of the
+    // brick, or on the zipped grid only the zones that own their node
+    const bool keep = th.active && (!ZIP || owns_node(blk, o, th.t, g));
+    // next scratch slot of this zone (kept zones only advance it)
     double* w = S + (int64_t)blockIdx.x * Bk::NZ + tid;
     __syncthreads();
 
@@ -118,7 +141,7 @@ deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
                     yz = closure_d1(myk, bz.mk, z.a[2], s, z.bflag & 16u, z.cf[2]);
                 }
             }
-            if (th.active) {
+            if (keep) {
                 const double v[kSlotsSecond] = {r[0].d1, r[1].d1, r[2].d1, r[0].d2, xy, xz,
                                                 r[1].d2, yz, r[2].d2, r[0].ko + r[1].ko + r[2].ko};
 #pragma unroll
@@ -127,7 +150,7 @@ deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
         } else {
             Dir3 r[3];
             zone_dirs<false, Bk>(bz.zc, cur, r);
-            if (th.active) {
+            if (keep) {
                 const double v[kSlotsFirst] = {r[0].d1, r[1].d1, r[2].d1,
                                                r[0].ko + r[1].ko + r[2].ko};
 #pragma unroll
@@ -146,7 +169,8 @@ deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
 template <int BX, int BY, int BZ>
 __global__ void __launch_bounds__(kEqThreads, 2)
 eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
-          const BrickTask* __restrict__ tasks, const double* __restrict__ S, int64_t zs) {
+          const BrickTask* __restrict__ tasks, const double* __restrict__ S, int64_t zs,
+          ZipGrid g) {
     using Bk = Brick<BX, BY, BZ>;
     constexpr int PARTS = (Bk::NZ + kEqThreads - 1) / kEqThreads;
     extern __shared__ __align__(16) double ring[];  // [kRingSlots][kEqThreads]
@@ -157,6 +181,20 @@ eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
     const BrickTask tk = tasks[task];
     const int r0 = l % BX, r1 = (l / BX) % BY, r2 = l / (BX * BY);
     if (r0 >= tk.e[0] || r1 >= tk.e[1] || r2 >= tk.e[2]) return;
+    const BssnBlockDesc blk = blocks[tk.blk];
+    const int o[3] = {tk.o[0], tk.o[1], tk.o[2]};
+    const int rt[3] = {r0, r1, r2};
+    // padded coordinates of the zone; its variables and right-hand sides at
+    // the padded index, or at its node of the zipped grid (owners only)
+    const int za0 = o[0] + PW + r0, za1 = o[1] + PW + r1, za2 = o[2] + PW + r2;
+    int64_t idx;
+    if (g.gx == 0) {
+        idx = blk.offset + za0 + (int64_t)blk.sz * (za1 + (int64_t)blk.sz * za2);
+    } else {
+        if (!owns_node(blk, o, rt, g)) return;
+        idx = (blk.g0[0] + za0 - PW) +
+              (int64_t)g.gx * ((blk.g0[1] + za1 - PW) + (int64_t)g.gy * (blk.g0[2] + za2 - PW));
+    }
     const double* in = S + (int64_t)task * Bk::NZ + l;
     double* col = ring + tid;
     auto issue = [&](int step) {
@@ -170,7 +208,6 @@ eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
     };
 #pragma unroll
     for (int k = 0; k < kPrefetchSteps; k++) issue(k);
-    const BssnBlockDesc blk = blocks[tk.blk];
     int step = 0;
     auto get = [&](auto tag, double* d1, double* d2, double& ko) {
         constexpr bool SECOND = decltype(tag)::value;
@@ -189,22 +226,23 @@ eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
         issue(step + kPrefetchSteps);  // rows of variables consumed before this one
         step++;
     };
-    zone_equations(A, blk, tk.o[0] + PW + r0, tk.o[1] + PW + r1, tk.o[2] + PW + r2, true, get);
+    zone_equations(A, blk, za0, za1, za2, idx, idx, true, get);
 }
 
 struct SplitEntry {
     int nz, threads;
     size_t smem, eq_smem;
-    void (*deriv)(ConstVars, const BssnBlockDesc*, const BrickTask*, double*, int64_t);
-    void (*eq)(RhsArgs, const BssnBlockDesc*, const BrickTask*, const double*, int64_t);
+    void (*deriv)(ConstVars, const BssnBlockDesc*, const BrickTask*, double*, int64_t, ZipGrid);
+    void (*deriv_zip)(ConstVars, const BssnBlockDesc*, const BrickTask*, double*, int64_t, ZipGrid);
+    void (*eq)(RhsArgs, const BssnBlockDesc*, const BrickTask*, const double*, int64_t, ZipGrid);
 };
 
 template <int BX, int BY, int BZ>
 SplitEntry make_split() {
     using Bk = Brick<BX, BY, BZ>;
     return SplitEntry{Bk::NZ, Bk::THREADS, Bk::SMEM_BYTES,
-                      sizeof(double) * kRingSlots * kEqThreads, deriv_kernel<BX, BY, BZ>,
-                      eq_kernel<BX, BY, BZ>};
+                      sizeof(double) * kRingSlots * kEqThreads, deriv_kernel<BX, BY, BZ, false>,
+                      deriv_kernel<BX, BY, BZ, true>, eq_kernel<BX, BY, BZ>};
 }
 
 // the fused tiles' shapes in their order, then split-only shapes (bricks too
@@ -244,6 +282,9 @@ int prepare_split(int shape) {
         cudaError_t e = cudaFuncSetAttribute(t[shape].deriv, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)t[shape].smem);
         if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(t[shape].deriv_zip, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)t[shape].smem);
+        if (e == cudaSuccess)
             e = cudaFuncSetAttribute(t[shape].eq, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)t[shape].eq_smem);
         if (e != cudaSuccess) return cuda_status(e);
@@ -254,7 +295,8 @@ int prepare_split(int shape) {
 
 int launch_rhs_split(int shape, const RhsArgs& A, const BssnBlockDesc* blocks_dev,
                      const BrickTask* tasks_dev, int ntasks, double* scratch,
-                     int64_t scratch_zones, cudaStream_t s, KernelTimer* tm) {
+                     int64_t scratch_zones, cudaStream_t s, KernelTimer* tm,
+                     const int32_t* zip_grid) {
     int c;
     const SplitEntry* tab = split_table(&c);
     if (shape < 0 || shape >= c) return BSSN_EINVAL;
@@ -264,17 +306,19 @@ int launch_rhs_split(int shape, const RhsArgs& A, const BssnBlockDesc* blocks_de
     if (chunk <= 0) return BSSN_EINVAL;
     int st = prepare_split(shape);
     if (st) return st;
+    const ZipGrid g = zip_grid ? ZipGrid{zip_grid[0], zip_grid[1], zip_grid[2]} : ZipGrid{0, 0, 0};
     const int64_t zs = chunk * t.nz;  // slot stride
     for (int64_t c0 = 0; c0 < ntasks; c0 += chunk) {
         const int n = (int)(ntasks - c0 < chunk ? ntasks - c0 : chunk);
         if (tm && (st = tm->start(KernelTimer::DERIV, s))) return st;
-        t.deriv<<<n, t.threads, t.smem, s>>>(A.u, blocks_dev, tasks_dev + c0, scratch, zs);
+        (g.gx ? t.deriv_zip : t.deriv)<<<n, t.threads, t.smem, s>>>(A.u, blocks_dev, tasks_dev + c0,
+                                                                    scratch, zs, g);
         st = cuda_status(cudaGetLastError());
         if (!st && tm) st = tm->stop(s);
         if (st) return st;
         if (tm && (st = tm->start(KernelTimer::EQ, s))) return st;
         const int parts = (t.nz + kEqThreads - 1) / kEqThreads;
-        t.eq<<<n * parts, kEqThreads, t.eq_smem, s>>>(A, blocks_dev, tasks_dev + c0, scratch, zs);
+        t.eq<<<n * parts, kEqThreads, t.eq_smem, s>>>(A, blocks_dev, tasks_dev + c0, scratch, zs, g);
         st = cuda_status(cudaGetLastError());
         if (!st && tm) st = tm->stop(s);
         if (st) return st;

@@ -221,6 +221,46 @@ __global__ void __launch_bounds__(256) zip_stage_kernel(int stage, MutVars im, M
     if (status && bad) atomicAdd(status, bad);
 }
 
+// The same stage algebra on the zipped node grid, with the right-hand side
+// already zipped (written once per node by the block owning it): one thread
+// per node, every access coalesced.
+__global__ void __launch_bounds__(256) node_stage_kernel(int stage, MutVars im, MutVars acc, MutVars u,
+                                  ConstVars R, int64_t n, double dt, int enforce,
+                                  double chi_floor, int* status) {
+    int bad = 0;
+    for (int64_t node = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; node < n;
+         node += (int64_t)gridDim.x * blockDim.x) {
+        double v[NVARS];
+        if (stage < 3) {
+            const double cu = M_(kRK4_U[stage + 1], dt);
+            const double cc = M_(kRK4_C[stage], dt);
+            double kk[NVARS], a0[NVARS];
+#pragma unroll
+            for (int q = 0; q < NVARS; q++) {
+                kk[q] = __ldg(R.p[q] + node);
+                v[q] = u.p[q][node];
+                a0[q] = stage == 0 ? v[q] : acc.p[q][node];
+            }
+#pragma unroll
+            for (int q = 0; q < NVARS; q++) {
+                acc.p[q][node] = A_(a0[q], M_(cc, kk[q]));
+                v[q] = A_(v[q], M_(cu, kk[q]));
+            }
+            if (enforce) bad += enforce_regs(v, chi_floor);
+#pragma unroll
+            for (int q = 0; q < NVARS; q++) im.p[q][node] = v[q];
+        } else {
+            const double cc = M_(kRK4_C[3], dt);
+#pragma unroll
+            for (int q = 0; q < NVARS; q++) v[q] = A_(acc.p[q][node], M_(cc, __ldg(R.p[q] + node)));
+            bad += enforce_regs(v, chi_floor);
+#pragma unroll
+            for (int q = 0; q < NVARS; q++) u.p[q][node] = v[q];
+        }
+    }
+    if (status && bad) atomicAdd(status, bad);
+}
+
 int grid_for(int64_t n, int threads) {
     int64_t b = (n + threads - 1) / threads;
     if (b > 148 * 64) b = 148 * 64;
@@ -280,6 +320,23 @@ int launch_zip_stage(const MeshState* m, int stage, double* const* im, double* c
     zip_stage_kernel<<<m->n_int_chunks, 256, 0, s>>>(stage, I, Ac, U, Rr, m->d_blocks,
                                                       m->d_int_chunks, m->G[0], m->G[1],
                                                       m->G[2], dt, enforce, chi_floor, status);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_node_stage(int stage, double* const* im, double* const* acc, double* const* u,
+                      const double* const* R, int64_t n, double dt, int enforce,
+                      double chi_floor, int* status, cudaStream_t s) {
+    MutVars I, Ac, U;
+    ConstVars Rr;
+    for (int q = 0; q < NVARS; q++) {
+        I.p[q] = im[q];
+        Ac.p[q] = acc[q];
+        U.p[q] = u[q];
+        Rr.p[q] = R[q];
+    }
+    if (n <= 0) return 0;
+    node_stage_kernel<<<grid_for(n, 256), 256, 0, s>>>(stage, I, Ac, U, Rr, n, dt, enforce,
+                                                       chi_floor, status);
     return cuda_status(cudaGetLastError());
 }
 

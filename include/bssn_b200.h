@@ -267,29 +267,41 @@ int bssn_remesh_decide_f64(bssn_mesh mesh, const double* const* unzip_dev,
 /* ---------------------------------------------------------------------- */
 /* One whole RK4 step as a plan over a mesh (the reference's per-step
  * sequence rkBSSN.cpp:764-860: per stage unzip -> bssnRHS -> zip -> stage
- * update).  The plan owns its scratch buffers (two padded 24-variable
- * arrays of bssn_mesh_unzip_size doubles and two zipped 24-variable arrays),
- * allocated at creation.  Per stage it runs the ghost fill, the fused
- * right-hand side (one launch per block-size bucket with that bucket's tile,
- * or one launch per block with BSSN_PLAN_PER_BLOCK), and the zip fused with
- * the stage algebra; with BSSN_PLAN_GRAPH the 4-stage sequence is captured
- * once as a CUDA graph and replayed (recaptured when u_dev or dt change).
- * u_dev (24 zipped arrays of G[0]*G[1]*G[2] doubles) is advanced in place. */
+ * update), same result.  The plan owns its scratch buffers, allocated at
+ * creation.  Default form: per stage the ghost fill into padded blocks, the
+ * right-hand side on them (one launch sequence per block-size bucket with
+ * that bucket's tile, or one launch per block with BSSN_PLAN_PER_BLOCK) and
+ * the zip fused with the stage algebra; scratch: two padded 24-variable
+ * arrays of bssn_mesh_unzip_size doubles and two zipped ones.
+ * BSSN_PLAN_DIRECT (split tiles; meshes of fewer than 2^31 nodes): every
+ * block of the single-level mesh is a box of the node grid, so the right-hand
+ * side reads the zipped stage state directly (points outside the grid read
+ * as zero, as the ghost fill writes them), writes each node's right-hand
+ * side once from the block owning it (the zip's owner rule), and a node-wise
+ * kernel applies the stage algebra; scratch: three zipped 24-variable arrays
+ * (no padded ones).  Same result; on B200 the padded form is faster (the
+ * derivative pass stages contiguous padded rows), the direct form needs far
+ * less memory.  With BSSN_PLAN_GRAPH the 4-stage sequence is captured once as
+ * a CUDA graph and replayed (recaptured when u_dev or dt change).  u_dev (24
+ * zipped arrays of G[0]*G[1]*G[2] doubles) is advanced in place. */
 #define BSSN_PLAN_ENFORCE_STAGES 1 /* enforce constraints on stage states */
 #define BSSN_PLAN_GRAPH 2          /* capture / replay as a CUDA graph */
 #define BSSN_PLAN_PER_BLOCK 4      /* one RHS launch per block (plain path) */
+#define BSSN_PLAN_DIRECT 8         /* right-hand side on the zipped grid */
 typedef struct bssn_rk4_plan_s* bssn_rk4_plan;
 int bssn_rk4_plan_create(bssn_mesh mesh, const BssnParams* params, int flags,
                          bssn_rk4_plan* out);
 int bssn_rk4_plan_step(bssn_rk4_plan plan, double* const* u_dev, double dt,
                        bssn_stream_t stream);
-/* Autotuner: times every tile shape on every block-size bucket of the mesh
- * with the state u_dev (best of reps) and keeps the fastest per bucket in the
- * mesh handle.  Blocking.  times (optional): nbuckets x bssn_tile_count()
- * milliseconds, buckets in increasing side order. */
+/* Autotuner: times every tile the plan can run (direct plans: split tiles
+ * only) on every block-size bucket of the mesh with the state u_dev (best of
+ * reps) and keeps the fastest per bucket in the mesh handle.  Blocking.
+ * times (optional): nbuckets x bssn_tile_count() milliseconds, buckets in
+ * increasing side order, 1e30 for tiles not timed. */
 int bssn_rk4_plan_autotune(bssn_rk4_plan plan, double* const* u_dev, int reps,
                            bssn_stream_t stream, float* times);
-/* The tile chosen for block side `side` (after autotuning; 0 before). */
+/* The tile the plan runs for block side `side` (the autotuned one; before
+ * tuning 0, or for direct plans the default split tile). */
 int bssn_rk4_plan_tile(bssn_rk4_plan plan, int side);
 /* Enforcement violations accumulated since creation (blocking read). */
 int bssn_rk4_plan_violations(bssn_rk4_plan plan, int* count);

@@ -147,12 +147,14 @@ def test_initial_data_config1(B, O):
     assert err0.max() <= 1e-14, err0.max()
 
 
-@pytest.mark.parametrize("path", ["python", "batched", "graph", "per_block"])
+@pytest.mark.parametrize("path", ["python", "batched", "graph", "per_block", "direct"])
 @pytest.mark.parametrize("mesh", ["uniform", "mix"])
 def test_rk4_step_vs_oracle(B, O, path, mesh):
     """One RK4 step from the same state on the GPU paths and on the CPU
     oracle (rkBSSN.cpp:764-860 restated); states compared per variable
-    relative to the variable's largest magnitude."""
+    relative to the variable's largest magnitude.  batched / graph: ghost
+    fill, padded blocks and zip; direct: right-hand side on the zipped grid;
+    per_block: one launch per block."""
     spec = B.generate_mesh(0, (4, 4, 4)) if mesh == "uniform" else B.generate_mesh(1, (2, 1, 1), seed=1, xmin=-8.25)
     mo = ol.MeshOracle(spec, O)
     Z0 = mo.initial_data(eps=1e-8)
@@ -167,7 +169,8 @@ def test_rk4_step_vs_oracle(B, O, path, mesh):
         B.PlainRK4(m, prm).step(dZ, dt)
     else:
         flags = B.PLAN_ENFORCE_STAGES | {"batched": 0, "graph": B.PLAN_GRAPH,
-                                         "per_block": B.PLAN_PER_BLOCK}[path]
+                                         "per_block": B.PLAN_PER_BLOCK,
+                                         "direct": B.PLAN_DIRECT}[path]
         plan = B.RK4Plan(m, prm, flags)
         plan.step(dZ, dt)
         torch.cuda.synchronize()
