@@ -46,7 +46,7 @@ static_assert(slot_base(NVARS) == kSplitSlots, "scratch slot count");
 // resident derivative CTAs per SM the register allocation must allow: 3 for
 // bricks of up to 256 zones (80 registers), fewer for larger bricks
 __host__ __device__ constexpr int deriv_min_ctas(int threads) {
-    return threads <= 256 ? 3 : (threads <= 384 ? 2 : 1);
+    return threads <= 384 ? 3 : 1;
 }
 // equation pass: variables whose derivatives are in flight ahead of use, and
 // the per-thread ring of scratch slots (shared memory) they land in; one
