@@ -270,6 +270,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tile", type=int, default=-1,
+                    help="pin this tile on every bucket instead of autotuning (profiling runs)")
     args = ap.parse_args()
     wl = args.workload
     if args.impl == "reference":
@@ -313,7 +315,10 @@ def main():
 
     # ---- batched, graph-captured plan
     plan = B.RK4Plan(mesh, prm, B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
-    chosen, table = plan.autotune(U, reps=2)
+    if args.tile >= 0:
+        chosen, table = plan.set_tile(args.tile), {}
+    else:
+        chosen, table = plan.autotune(U, reps=2)
     for _ in range(args.warmup):
         plan.step(U, dt)
     torch.cuda.synchronize()

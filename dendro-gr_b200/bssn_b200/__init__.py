@@ -74,6 +74,10 @@ def _sig():
     lib.bssn_rk4_plan_step.argtypes = [vp, vp, d, vp]
     lib.bssn_rk4_plan_autotune.argtypes = [vp, vp, i, vp, P(C.c_float)]
     lib.bssn_rk4_plan_tile.argtypes = [vp, i]
+    lib.bssn_rk4_plan_set_tile.argtypes = [vp, i, i]
+    lib.bssn_rk4_plan_time_kernels.argtypes = [vp, i, vp, P(d)]
+    lib.bssn_rk4_plan_launches_per_step.argtypes = [vp]
+    lib.bssn_tile_mode.argtypes = [i]
     lib.bssn_rk4_plan_violations.argtypes = [vp, P(i)]
     lib.bssn_rk4_plan_destroy.argtypes = [vp]
     lib.bssn_constraints_f64.argtypes = [vp, vp, vp, vp]
@@ -316,6 +320,12 @@ class RK4Plan:
         table = {side: [times[i * nt + t] for t in range(nt)] for i, side in enumerate(sides)}
         chosen = {side: lib.bssn_rk4_plan_tile(self.h, side) for side in sides}
         return chosen, table
+
+    def set_tile(self, tile, side=0):
+        """Pin a tile (for every side when side is 0) instead of autotuning."""
+        check(lib.bssn_rk4_plan_set_tile(self.h, side, tile), "set_tile")
+        sides = sorted(set(self.mesh.spec.sides.tolist()))
+        return {sd: lib.bssn_rk4_plan_tile(self.h, sd) for sd in sides}
 
     def violations(self):
         c = C.c_int(0)

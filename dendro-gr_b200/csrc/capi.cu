@@ -191,6 +191,11 @@ int bssn_rk4_plan_autotune(bssn_rk4_plan plan, double* const* u_dev, int reps,
     return bssn::plan_autotune(plan->p, u_dev, reps, S(stream), times);
 }
 
+int bssn_rk4_plan_set_tile(bssn_rk4_plan plan, int side, int tile) {
+    if (!plan) return BSSN_EINVAL;
+    return bssn::plan_set_tile(plan->p, side, tile);
+}
+
 int bssn_rk4_plan_tile(bssn_rk4_plan plan, int side) {
     if (!plan) return -BSSN_EINVAL;
     return bssn::plan_tile(plan->p, side);

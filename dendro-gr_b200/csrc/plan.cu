@@ -126,6 +126,25 @@ int plan_tile(const Plan* p, int side) {
     return t >= 0 ? t : 0;
 }
 
+int plan_set_tile(Plan* p, int side, int tile) {
+    if (tile < 0 || tile >= tile_count()) return BSSN_EINVAL;
+    if (p->direct) {
+        if (tile_mode(tile) != 1) return BSSN_EINVAL;
+        p->mesh->tuned[kAllZOrder] = tile;
+    } else if (side == 0) {
+        for (int sd : p->sides) p->mesh->tuned[sd] = tile;
+    } else {
+        p->mesh->tuned[side] = tile;
+    }
+    if (p->exec) {  // recapture with the new tile on the next step
+        cudaGraphExecDestroy(p->exec);
+        cudaGraphDestroy(p->graph);
+        p->exec = nullptr;
+        p->graph = nullptr;
+    }
+    return 0;
+}
+
 // One right-hand-side pass over every bucket.  Direct plans read the zipped
 // stage state `src` and write Rz; the others read the padded P (filled by
 // the ghost fill) and write R.

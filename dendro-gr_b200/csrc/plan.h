@@ -38,6 +38,7 @@ void plan_destroy(Plan* p);
 int plan_step(Plan* p, double* const* u, double dt, cudaStream_t s);
 int plan_autotune(Plan* p, double* const* u, int reps, cudaStream_t s, float* times_out);
 int plan_tile(const Plan* p, int side);
+int plan_set_tile(Plan* p, int side, int tile);
 int plan_time_rhs(Plan* p, int reps, cudaStream_t s, float* ms);
 int plan_time_kernels(Plan* p, int reps, cudaStream_t s, double out[6]);
 int plan_launches_per_step(Plan* p);

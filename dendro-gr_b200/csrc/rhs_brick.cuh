@@ -465,8 +465,14 @@ struct BrickThread {
 
 // The block's per-axis stencil factors, written by threads 0..2 into shared
 // memory (visible after the caller's next barrier).
+// (Selects, not blk.ptmax[tid]: a run-time index into the descriptor would
+// put the whole descriptor in local memory for the rest of the kernel.)
 __device__ __forceinline__ void fill_axis_coefs(AxisCoef* cf, const BssnBlockDesc& blk, int tid) {
-    if (tid < 3) cf[tid] = axis_coef((blk.ptmax[tid] - blk.ptmin[tid]) / (blk.sz - 1));
+    if (tid < 3) {
+        const double lo = tid == 0 ? blk.ptmin[0] : (tid == 1 ? blk.ptmin[1] : blk.ptmin[2]);
+        const double hi = tid == 0 ? blk.ptmax[0] : (tid == 1 ? blk.ptmax[1] : blk.ptmax[2]);
+        cf[tid] = axis_coef((hi - lo) / (blk.sz - 1));
+    }
 }
 
 // Stencil context of a thread's zone in a brick (tile strides, padded

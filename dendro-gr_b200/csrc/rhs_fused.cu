@@ -61,7 +61,8 @@ __device__ __forceinline__ void rhs_brick(const RhsArgs& A, const BssnBlockDesc&
                             bz.mj, bz.mk, d1, d2, ko);
     };
     const int64_t pidx = off + bz.zc.a[0] + (int64_t)s * (bz.zc.a[1] + (int64_t)s * bz.zc.a[2]);
-    zone_equations(A, blk, bz.zc.a[0], bz.zc.a[1], bz.zc.a[2], pidx, pidx, th.active, get);
+    auto pv = [&](int v) { return __ldg(A.u.p[v] + pidx); };
+    zone_equations(A, blk, bz.zc.a[0], bz.zc.a[1], bz.zc.a[2], pidx, th.active, get, pv);
 }
 
 }  // namespace

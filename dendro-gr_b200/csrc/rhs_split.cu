@@ -197,6 +197,11 @@ eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
     }
     const double* in = S + (int64_t)task * Bk::NZ + l;
     double* col = ring + tid;
+    double* vals = ring + kRingSlots * kEqThreads + tid;  // [NVARS][kEqThreads]
+    // the zone's 24 variables first, as their own commit group
+#pragma unroll
+    for (int v = 0; v < NVARS; v++) cp_async8(vals + v * kEqThreads, A.u.p[v] + idx);
+    cp_async_commit();
     auto issue = [&](int step) {
         if (step < NVARS) {
             const int b = slot_base(step), n = slot_len(step);
@@ -208,6 +213,8 @@ eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
     };
 #pragma unroll
     for (int k = 0; k < kPrefetchSteps; k++) issue(k);
+    cp_async_wait_pending<kPrefetchSteps>();  // the variables' group
+    auto pv = [&](int v) { return vals[v * kEqThreads]; };
     int step = 0;
     auto get = [&](auto tag, double* d1, double* d2, double& ko) {
         constexpr bool SECOND = decltype(tag)::value;
@@ -226,7 +233,7 @@ eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
         issue(step + kPrefetchSteps);  // rows of variables consumed before this one
         step++;
     };
-    zone_equations(A, blk, za0, za1, za2, idx, idx, true, get);
+    zone_equations(A, blk, za0, za1, za2, idx, true, get, pv);
 }
 
 struct SplitEntry {
@@ -241,7 +248,7 @@ template <int BX, int BY, int BZ>
 SplitEntry make_split() {
     using Bk = Brick<BX, BY, BZ>;
     return SplitEntry{Bk::NZ, Bk::THREADS, Bk::SMEM_BYTES,
-                      sizeof(double) * kRingSlots * kEqThreads, deriv_kernel<BX, BY, BZ, false>,
+                      sizeof(double) * (kRingSlots + NVARS) * kEqThreads, deriv_kernel<BX, BY, BZ, false>,
                       deriv_kernel<BX, BY, BZ, true>, eq_kernel<BX, BY, BZ>};
 }
 

@@ -303,6 +303,10 @@ int bssn_rk4_plan_autotune(bssn_rk4_plan plan, double* const* u_dev, int reps,
 /* The tile the plan runs for block side `side` (the autotuned one; before
  * tuning 0, or for direct plans the default split tile). */
 int bssn_rk4_plan_tile(bssn_rk4_plan plan, int side);
+/* Pin the tile for block side `side` (0: every side; direct plans take one
+ * split tile for all sides), as the autotuner would; the next step
+ * recaptures its graph.  BSSN_EINVAL for a tile the plan cannot run. */
+int bssn_rk4_plan_set_tile(bssn_rk4_plan plan, int side, int tile);
 /* Enforcement violations accumulated since creation (blocking read). */
 int bssn_rk4_plan_violations(bssn_rk4_plan plan, int* count);
 int bssn_rk4_plan_destroy(bssn_rk4_plan plan);
