@@ -71,11 +71,11 @@ def kernel_bytes(sides, chosen, modes, n_nodes, direct):
     return out
 
 
-# DRAM traffic / algorithmic bytes of each kernel, from the ncu capture
-# summarised in profiles/rhs_split_kernels_uniform512.md (read + write bytes
-# of one launch divided by that launch's algorithmic bytes); scales the
-# algorithmic bytes of a full pass to its expected DRAM traffic.
-TRAFFIC_RATIO = {}
+# DRAM traffic / algorithmic bytes of each kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum of one launch over that launch's algorithmic bytes),
+# from ncu captures of the 7x7x7 split tile on the uniform 512-block workload
+# (13^3 blocks); scales a full pass's algorithmic bytes to its DRAM traffic.
+TRAFFIC_RATIO = {"deriv": 0.92, "eq": 1.21}
 
 
 def step_bytes(sides, n_nodes):

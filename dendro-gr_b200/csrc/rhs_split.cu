@@ -55,6 +55,12 @@ __host__ __device__ constexpr int deriv_min_ctas(int threads) {
 constexpr int kPrefetchSteps = 6;
 constexpr int kRingSlots = (kPrefetchSteps + 1) * kSlotsSecond;
 constexpr int kEqThreads = 128;
+// derivative pass: shared-memory tiles (variables staged kDerivBuffers - 1 ahead)
+constexpr int kDerivBuffers = 2;
+template <class Bk>
+constexpr size_t deriv_smem_bytes() {
+    return sizeof(double) * (kDerivBuffers * Bk::TILE + Bk::MXJ + 2 * Bk::MXK);
+}
 
 template <int N>
 __device__ __forceinline__ void cp_async_wait_pending() {
@@ -88,8 +94,8 @@ deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
     extern __shared__ __align__(16) double smem[];
     __shared__ const double* src[NVARS];
     __shared__ AxisCoef cfs[3];
-    double* tiles[2] = {smem, smem + Bk::TILE};
-    double* mx = smem + 2 * Bk::TILE;  // mxj | mxk | myk
+    double* tiles = smem;                         // kDerivBuffers tiles
+    double* mx = smem + kDerivBuffers * Bk::TILE;  // mxj | mxk | myk
     const BrickTask tk = tasks[blockIdx.x];
     const BssnBlockDesc blk = blocks[tk.blk];
     const int o[3] = {tk.o[0], tk.o[1], tk.o[2]};
@@ -108,13 +114,20 @@ deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
     double* w = S + (int64_t)blockIdx.x * Bk::NZ + tid;
     __syncthreads();
 
-    sp.stage(src[0], tiles[0], tid);
+    // variables in flight kDerivBuffers - 1 ahead; one commit group per
+    // variable (empty past the last one, so the pending count stays fixed)
+#pragma unroll
+    for (int k = 0; k < kDerivBuffers - 1; k++) sp.stage(src[k], tiles + k * Bk::TILE, tid);
 #pragma unroll 1
     for (int step = 0; step < NVARS; step++) {
-        cp_async_wait_all();
-        __syncthreads();
-        const double* cur = tiles[step & 1];
-        if (step + 1 < NVARS) sp.stage(src[step + 1], tiles[(step + 1) & 1], tid);
+        cp_async_wait_pending<kDerivBuffers - 2>();
+        __syncthreads();  // the tile of `step` is complete; the buffer below was last read at step - 1
+        const double* cur = tiles + (step % kDerivBuffers) * Bk::TILE;
+        const int nxt = step + kDerivBuffers - 1;
+        if (nxt < NVARS)
+            sp.stage(src[nxt], tiles + (nxt % kDerivBuffers) * Bk::TILE, tid);
+        else
+            cp_async_commit();
         if (stage_second(step)) {
             Dir3 r[3];
             zone_dirs<true, Bk>(bz.zc, cur, r);
@@ -247,7 +260,7 @@ struct SplitEntry {
 template <int BX, int BY, int BZ>
 SplitEntry make_split() {
     using Bk = Brick<BX, BY, BZ>;
-    return SplitEntry{Bk::NZ, Bk::THREADS, Bk::SMEM_BYTES,
+    return SplitEntry{Bk::NZ, Bk::THREADS, deriv_smem_bytes<Bk>(),
                       sizeof(double) * (kRingSlots + NVARS) * kEqThreads, deriv_kernel<BX, BY, BZ, false>,
                       deriv_kernel<BX, BY, BZ, true>, eq_kernel<BX, BY, BZ>};
 }

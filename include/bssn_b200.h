@@ -115,8 +115,8 @@ int64_t bssn_mesh_unzip_size(bssn_mesh mesh);
 /* All blocks of a mesh in one launch.  Replaces bssnRHS(unzipVarsRHS,
  * uZipVars, blkList, numBlocks, t, uZipConstVars) (rhs.cpp:10-73) and the
  * GPU comparator device::bssnrhs3 (cuda/include/bssn_kernels.cuh:1526-1538).
- * tile: -1 = the autotuned choice per block size (the default tile before
- * tuning); otherwise a tile id in [0, bssn_tile_count()). */
+ * tile: -1 = the split 7x7x7 tile; otherwise a tile id in
+ * [0, bssn_tile_count()). */
 int bssn_rhs_blocks_f64(bssn_mesh mesh, double* const* rhs_dev,
                         const double* const* u_dev, const BssnParams* params,
                         int tile, bssn_stream_t stream);
