@@ -47,18 +47,27 @@ SPLIT_SLOTS = 162  # scratch doubles per zone of the split right-hand side
 
 
 def kernel_bytes(sides, chosen, modes, n_nodes, direct):
-    """Algorithmic HBM bytes of one right-hand-side pass per kernel kind.
-    Direct plans (split tiles on the zipped grid): the derivative pass reads
-    the 24 zipped variables once and writes 162 derivative doubles per node;
-    the equation pass reads them and the node's 24 variables and writes its
-    24 right-hand sides.  Padded plans, per block by the tile chosen for its
-    side (mode 0 fused, 1 split): fused reads the 24 padded variables and
-    writes the 24 interior right-hand sides; split writes / reads the 162
-    derivative doubles of every interior zone in between."""
+    """Algorithmic HBM bytes of one right-hand-side pass per kernel kind, as
+    the plan's timing call runs it.
+    Direct form: the derivative pass reads the 24 zipped variables once and
+    writes 162 derivative doubles per node; the equation pass reads them and
+    the node's 24 variables and writes its 24 right-hand sides.
+    Every bucket split (zipped right-hand side): the derivative pass reads
+    the 24 padded variables once (192 B per padded point) and writes 162
+    doubles per node, from the zone owning it; the equation pass reads those
+    and the node's 24 variables and writes its 24 right-hand sides.
+    Otherwise, per block by the tile chosen for its side: fused reads the 24
+    padded variables and writes the 24 interior right-hand sides; split
+    writes / reads 162 derivative doubles per interior zone in between."""
     out = {"fused": 0, "deriv": 0, "eq": 0}
+    n_nodes = int(n_nodes)
     if direct:
-        out["deriv"] = 8 * (24 + SPLIT_SLOTS) * int(n_nodes)
-        out["eq"] = 8 * (SPLIT_SLOTS + 24 + 24) * int(n_nodes)
+        out["deriv"] = 8 * (24 + SPLIT_SLOTS) * n_nodes
+        out["eq"] = 8 * (SPLIT_SLOTS + 24 + 24) * n_nodes
+        return out
+    if all(modes[chosen[int(s)]] == 1 for s in sides):
+        out["deriv"] = 8 * (24 * sum(int(s) ** 3 for s in sides) + SPLIT_SLOTS * n_nodes)
+        out["eq"] = 8 * (SPLIT_SLOTS + 24 + 24) * n_nodes
         return out
     for s in sides:
         s = int(s)

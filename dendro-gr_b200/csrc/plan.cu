@@ -53,6 +53,8 @@ int plan_create(MeshState* m, const BssnParams& prm, int flags, Plan** out) {
     } else {
         st = alloc(&p->P, (size_t)NVARS * nu);
         if (!st) st = alloc(&p->R, (size_t)NVARS * nu);
+        // zipped right-hand side of the split passes (32-bit node indices)
+        if (!st && nn < (int64_t(1) << 31)) st = alloc(&p->Rz, (size_t)NVARS * nn);
         // padded buffers start at zero so never-written points stay finite
         if (!st) st = cuda_status(cudaMemset(p->P, 0, sizeof(double) * NVARS * nu));
         if (!st) st = cuda_status(cudaMemset(p->R, 0, sizeof(double) * NVARS * nu));
@@ -60,6 +62,7 @@ int plan_create(MeshState* m, const BssnParams& prm, int flags, Plan** out) {
     if (!st) st = alloc(&p->im, (size_t)NVARS * nn);
     if (!st) st = alloc(&p->acc, (size_t)NVARS * nn);
     if (!st) st = cuda_status(cudaMemset(p->im, 0, sizeof(double) * NVARS * nn));
+    if (!st) st = cuda_status(cudaMemset(p->acc, 0, sizeof(double) * NVARS * nn));
     if (!st && cudaMalloc((void**)&p->status, sizeof(int)) != cudaSuccess) st = BSSN_ENOMEM;
     if (!st) st = cuda_status(cudaMemset(p->status, 0, sizeof(int)));
     if (st) {
@@ -145,9 +148,19 @@ int plan_set_tile(Plan* p, int side, int tile) {
     return 0;
 }
 
+// Whether a padded plan writes its right-hand side zipped (every bucket on a
+// split tile): the split passes then write each node once, from the block
+// owning it, and a node-wise kernel applies the stage (no zip gather).
+bool plan_zipped_rhs(const Plan* p) {
+    if (p->direct || !p->Rz || (p->flags & BSSN_PLAN_PER_BLOCK)) return false;
+    for (int side : p->sides)
+        if (tile_mode(plan_tile(p, side)) != 1) return false;
+    return true;
+}
+
 // One right-hand-side pass over every bucket.  Direct plans read the zipped
 // stage state `src` and write Rz; the others read the padded P (filled by
-// the ghost fill) and write R.
+// the ghost fill) and write R, or Rz when plan_zipped_rhs.
 int plan_rhs(Plan* p, cudaStream_t s, KernelTimer* tm, const double* const* src) {
     MeshState* m = p->mesh;
     RhsArgs A;
@@ -170,8 +183,12 @@ int plan_rhs(Plan* p, cudaStream_t s, KernelTimer* tm, const double* const* src)
     }
     double* Pp[NVARS];
     double* Rp[NVARS];
+    const bool zrhs = plan_zipped_rhs(p);
     set_ptrs(p->P, m->unzip_size, Pp);
-    set_ptrs(p->R, m->unzip_size, Rp);
+    if (zrhs)
+        set_ptrs(p->Rz, p->n_nodes, Rp);
+    else
+        set_ptrs(p->R, m->unzip_size, Rp);
     for (int v = 0; v < NVARS; v++) {
         A.u.p[v] = Pp[v];
         A.rhs.p[v] = Rp[v];
@@ -188,7 +205,9 @@ int plan_rhs(Plan* p, cudaStream_t s, KernelTimer* tm, const double* const* src)
         const BrickTask* tk;
         int nt;
         int st = mesh_tasks_side(m, t, side, &tk, &nt);
-        if (!st) st = launch_rhs_tasks(t, A, m->d_blocks, tk, nt, s, m->d_scratch, m->scratch_zones, tm);
+        if (!st)
+            st = launch_rhs_tasks(t, A, m->d_blocks, tk, nt, s, m->d_scratch, m->scratch_zones, tm,
+                                  zrhs ? m->G : nullptr, false);
         if (st) return st;
     }
     return 0;
@@ -211,6 +230,19 @@ int plan_enqueue(Plan* p, double* const* u, double dt, cudaStream_t s) {
         for (int stage = 0; stage < 4; stage++) {
             const double* const* src = stage == 0 ? (const double* const*)u : (const double* const*)Ip;
             int st = plan_rhs(p, s, nullptr, src);
+            if (!st) st = launch_node_stage(stage, Ip, Ap, u, Rz, p->n_nodes, dt, enf,
+                                            p->prm.chi_floor, p->status, s);
+            if (st) return st;
+        }
+        return 0;
+    }
+    if (plan_zipped_rhs(p)) {
+        double* Rz[NVARS];
+        set_ptrs(p->Rz, p->n_nodes, Rz);
+        for (int stage = 0; stage < 4; stage++) {
+            const double* const* src = stage == 0 ? (const double* const*)u : (const double* const*)Ip;
+            int st = launch_unzip(m, Pp, src, NVARS, s);
+            if (!st) st = plan_rhs(p, s, nullptr, nullptr);
             if (!st) st = launch_node_stage(stage, Ip, Ap, u, Rz, p->n_nodes, dt, enf,
                                             p->prm.chi_floor, p->status, s);
             if (st) return st;

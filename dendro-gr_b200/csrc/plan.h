@@ -19,7 +19,7 @@ struct Plan {
     // zipped right-hand side (no ghost fill, no padded arrays); otherwise the
     // ghost fill -> padded right-hand side -> zip-stage sequence
     bool direct = false;
-    double* Rz = nullptr;   // zipped right-hand side (direct)
+    double* Rz = nullptr;   // zipped right-hand side (direct form, or split buckets)
     double* P = nullptr;    // padded stage state (24 x unzip size)
     double* R = nullptr;    // padded right-hand side
     double* im = nullptr;   // zipped intermediate stage state

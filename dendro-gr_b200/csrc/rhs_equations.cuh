@@ -18,21 +18,18 @@ namespace {
 // get(BoolTag<SECOND>{}, d1, d2, ko) must deliver, on its n-th call, the
 // derivatives of variable stage_order(n): gradient d1[3], (if SECOND) the
 // second derivatives d2[6] (xx,xy,xz,yy,yz,zz) and the summed KO term;
-// pv(v) the zone's value of variable v.  za are the zone's padded block
-// coordinates; if `active`, its right-hand sides are written to
-// A.rhs.p[v][out_idx] (padded block index, or node index on the zipped grid).
-template <class Get, class PV>
+// pv(v) the zone's value of variable v; store(v, r) receives the zone's
+// right-hand side of variable v (each v once).  za are the zone's padded
+// block coordinates.
+template <class Get, class PV, class Store>
 __device__ __forceinline__ void zone_equations(const RhsArgs& A, const BssnBlockDesc& blk,
-                                               int za0, int za1, int za2, int64_t out_idx,
-                                               bool active, Get&& get, PV&& pv) {
+                                               int za0, int za1, int za2, Get&& get, PV&& pv,
+                                               Store&& store) {
     const int s = blk.sz;
     const unsigned bflag = blk.bflag;
     double hh[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) hh[d] = (blk.ptmax[d] - blk.ptmin[d]) / (s - 1);
-    auto store = [&](int v, double val) {
-        if (active) A.rhs.p[v][out_idx] = val;
-    };
 
     // coordinates and radius rounded exactly as the reference computes them
     // (pmin + i*h, no contraction), so a face point at the origin gives the

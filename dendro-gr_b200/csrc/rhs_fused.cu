@@ -62,7 +62,11 @@ __device__ __forceinline__ void rhs_brick(const RhsArgs& A, const BssnBlockDesc&
     };
     const int64_t pidx = off + bz.zc.a[0] + (int64_t)s * (bz.zc.a[1] + (int64_t)s * bz.zc.a[2]);
     auto pv = [&](int v) { return __ldg(A.u.p[v] + pidx); };
-    zone_equations(A, blk, bz.zc.a[0], bz.zc.a[1], bz.zc.a[2], pidx, th.active, get, pv);
+    const bool active = th.active;
+    auto store = [&](int v, double r) {
+        if (active) A.rhs.p[v][pidx] = r;
+    };
+    zone_equations(A, blk, bz.zc.a[0], bz.zc.a[1], bz.zc.a[2], get, pv, store);
 }
 
 }  // namespace
@@ -308,7 +312,7 @@ void build_tasks(const BssnBlockDesc* blocks, int nblocks, int tile,
 int launch_rhs_tasks(int tile, const RhsArgs& A, const BssnBlockDesc* blocks_dev,
                      const BrickTask* tasks_dev, int ntasks, cudaStream_t s,
                      double* scratch, int64_t scratch_zones, KernelTimer* tm,
-                     const int32_t* zip_grid) {
+                     const int32_t* zip_grid, bool zip_in) {
     int c;
     const TileEntry* tab = tile_table(&c);
     if (tile < 0 || tile >= c) return BSSN_EINVAL;
@@ -316,8 +320,8 @@ int launch_rhs_tasks(int tile, const RhsArgs& A, const BssnBlockDesc* blocks_dev
     const TileEntry& t = tab[tile];
     if (t.mode == 1)
         return launch_rhs_split(t.shape, A, blocks_dev, tasks_dev, ntasks, scratch, scratch_zones,
-                                s, tm, zip_grid);
-    if (zip_grid) return BSSN_EINVAL;  // the fused kernel reads padded blocks only
+                                s, tm, zip_grid, zip_in);
+    if (zip_grid) return BSSN_EINVAL;  // the fused kernel writes padded right-hand sides only
     int st = prepare(t);
     if (!st && tm) st = tm->start(KernelTimer::FUSED, s);
     if (st) return st;

@@ -81,12 +81,14 @@ struct KernelTimer {
 // scratch / scratch_zones: the split path's scratch (kSplitSlots * zones
 // doubles); ignored by fused tiles.  tm (optional): time each launch.
 // zip_grid (optional, split tiles only): the node-grid dimensions of a
-// single-level mesh; A.u then holds the zipped stage state and A.rhs the
-// zipped right-hand side, written once per node by the block owning it.
+// single-level mesh; A.rhs then holds zipped right-hand sides, written once
+// per node by the block owning it (zones that do not own their node are
+// skipped), and A.u the zipped stage state (zip_in, direct form) or the
+// padded one.
 int launch_rhs_tasks(int tile, const RhsArgs& A, const BssnBlockDesc* blocks_dev,
                      const BrickTask* tasks_dev, int ntasks, cudaStream_t s,
                      double* scratch, int64_t scratch_zones, KernelTimer* tm = nullptr,
-                     const int32_t* zip_grid = nullptr);
+                     const int32_t* zip_grid = nullptr, bool zip_in = true);
 // kernel launches launch_rhs_tasks makes for a task list of ntasks bricks
 int rhs_launch_count(int tile, int ntasks, int64_t scratch_zones);
 // one block; a split tile runs its shape fused
@@ -100,6 +102,6 @@ int prepare_split(int shape);
 int launch_rhs_split(int shape, const RhsArgs& A, const BssnBlockDesc* blocks_dev,
                      const BrickTask* tasks_dev, int ntasks, double* scratch,
                      int64_t scratch_zones, cudaStream_t s, KernelTimer* tm = nullptr,
-                     const int32_t* zip_grid = nullptr);
+                     const int32_t* zip_grid = nullptr, bool zip_in = true);
 
 }  // namespace bssn

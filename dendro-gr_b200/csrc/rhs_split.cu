@@ -108,8 +108,9 @@ deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
     const BrickZone<Bk> bz(blk, o, th, cfs);
     const StagePlan<Bk, ZIP> sp(o, e, s, tid, g, blk.g0);
     // zones whose derivatives the equation pass reads: every zone of the
-    // brick, or on the zipped grid only the zones that own their node
-    const bool keep = th.active && (!ZIP || owns_node(blk, o, th.t, g));
+    // brick, or (node grid given: direct form or stage mode) only the zones
+    // that own their node
+    const bool keep = th.active && (g.gx == 0 || owns_node(blk, o, th.t, g));
     // next scratch slot of this zone (kept zones only advance it)
     double* w = S + (int64_t)blockIdx.x * Bk::NZ + tid;
     __syncthreads();
@@ -175,18 +176,23 @@ deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
 
 // One thread per zone, kEqThreads zones of a brick per CTA (a brick of NZ
 // zones takes ceil(NZ / kEqThreads) CTAs), so two CTAs share an SM at 254
-// registers.  Each thread streams its own zone's scratch slots into its own
-// column of a shared-memory ring with cp.async, kPrefetchSteps variables
-// ahead of the equations that consume them (one commit group per variable;
-// a thread only reads what it copied itself, so no barrier).
+// registers.  Each thread streams its own zone's 24 variables and scratch
+// slots into its own columns of shared memory with cp.async, the slots
+// kPrefetchSteps variables ahead of the equations that consume them (one
+// commit group per variable; a thread only reads what it copied itself, so
+// no barrier).
+// g.gx == 0: variables and right-hand sides at the zone's padded index.
+// g.gx > 0: only zones owning their node run and write the right-hand side
+// at the node index of the zipped grid; the variables are read there too
+// (zip_in, direct form) or at the padded index.
 template <int BX, int BY, int BZ>
 __global__ void __launch_bounds__(kEqThreads, 2)
 eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
           const BrickTask* __restrict__ tasks, const double* __restrict__ S, int64_t zs,
-          ZipGrid g) {
+          ZipGrid g, int zip_in) {
     using Bk = Brick<BX, BY, BZ>;
     constexpr int PARTS = (Bk::NZ + kEqThreads - 1) / kEqThreads;
-    extern __shared__ __align__(16) double ring[];  // [kRingSlots][kEqThreads]
+    extern __shared__ __align__(16) double ring[];  // [kRingSlots][T] | vals [NVARS][T]
     const int tid = threadIdx.x;
     const int task = blockIdx.x / PARTS;
     const int l = (blockIdx.x % PARTS) * kEqThreads + tid;  // zone index in the brick
@@ -197,23 +203,21 @@ eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
     const BssnBlockDesc blk = blocks[tk.blk];
     const int o[3] = {tk.o[0], tk.o[1], tk.o[2]};
     const int rt[3] = {r0, r1, r2};
-    // padded coordinates of the zone; its variables and right-hand sides at
-    // the padded index, or at its node of the zipped grid (owners only)
     const int za0 = o[0] + PW + r0, za1 = o[1] + PW + r1, za2 = o[2] + PW + r2;
-    int64_t idx;
-    if (g.gx == 0) {
-        idx = blk.offset + za0 + (int64_t)blk.sz * (za1 + (int64_t)blk.sz * za2);
-    } else {
+    const int64_t pidx = blk.offset + za0 + (int64_t)blk.sz * (za1 + (int64_t)blk.sz * za2);
+    int64_t node = pidx;
+    if (g.gx) {
         if (!owns_node(blk, o, rt, g)) return;
-        idx = (blk.g0[0] + za0 - PW) +
-              (int64_t)g.gx * ((blk.g0[1] + za1 - PW) + (int64_t)g.gy * (blk.g0[2] + za2 - PW));
+        node = (blk.g0[0] + za0 - PW) +
+               (int64_t)g.gx * ((blk.g0[1] + za1 - PW) + (int64_t)g.gy * (blk.g0[2] + za2 - PW));
     }
+    const int64_t in_idx = zip_in ? node : pidx;
     const double* in = S + (int64_t)task * Bk::NZ + l;
     double* col = ring + tid;
     double* vals = ring + kRingSlots * kEqThreads + tid;  // [NVARS][kEqThreads]
     // the zone's 24 variables first, as their own commit group
 #pragma unroll
-    for (int v = 0; v < NVARS; v++) cp_async8(vals + v * kEqThreads, A.u.p[v] + idx);
+    for (int v = 0; v < NVARS; v++) cp_async8(vals + v * kEqThreads, A.u.p[v] + in_idx);
     cp_async_commit();
     auto issue = [&](int step) {
         if (step < NVARS) {
@@ -246,23 +250,26 @@ eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
         issue(step + kPrefetchSteps);  // rows of variables consumed before this one
         step++;
     };
-    zone_equations(A, blk, za0, za1, za2, idx, true, get, pv);
+    auto store = [&](int v, double r) { A.rhs.p[v][node] = r; };
+    zone_equations(A, blk, za0, za1, za2, get, pv, store);
 }
+
+constexpr size_t eq_smem_bytes() { return sizeof(double) * kEqThreads * (kRingSlots + NVARS); }
 
 struct SplitEntry {
     int nz, threads;
-    size_t smem, eq_smem;
+    size_t smem;
     void (*deriv)(ConstVars, const BssnBlockDesc*, const BrickTask*, double*, int64_t, ZipGrid);
     void (*deriv_zip)(ConstVars, const BssnBlockDesc*, const BrickTask*, double*, int64_t, ZipGrid);
-    void (*eq)(RhsArgs, const BssnBlockDesc*, const BrickTask*, const double*, int64_t, ZipGrid);
+    void (*eq)(RhsArgs, const BssnBlockDesc*, const BrickTask*, const double*, int64_t, ZipGrid, int);
 };
 
 template <int BX, int BY, int BZ>
 SplitEntry make_split() {
     using Bk = Brick<BX, BY, BZ>;
     return SplitEntry{Bk::NZ, Bk::THREADS, deriv_smem_bytes<Bk>(),
-                      sizeof(double) * (kRingSlots + NVARS) * kEqThreads, deriv_kernel<BX, BY, BZ, false>,
-                      deriv_kernel<BX, BY, BZ, true>, eq_kernel<BX, BY, BZ>};
+                      deriv_kernel<BX, BY, BZ, false>, deriv_kernel<BX, BY, BZ, true>,
+                      eq_kernel<BX, BY, BZ>};
 }
 
 // the fused tiles' shapes in their order, then split-only shapes (bricks too
@@ -306,7 +313,7 @@ int prepare_split(int shape) {
                                      (int)t[shape].smem);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(t[shape].eq, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)t[shape].eq_smem);
+                                     (int)eq_smem_bytes());
         if (e != cudaSuccess) return cuda_status(e);
         done[shape] = true;
     }
@@ -316,7 +323,7 @@ int prepare_split(int shape) {
 int launch_rhs_split(int shape, const RhsArgs& A, const BssnBlockDesc* blocks_dev,
                      const BrickTask* tasks_dev, int ntasks, double* scratch,
                      int64_t scratch_zones, cudaStream_t s, KernelTimer* tm,
-                     const int32_t* zip_grid) {
+                     const int32_t* zip_grid, bool zip_in) {
     int c;
     const SplitEntry* tab = split_table(&c);
     if (shape < 0 || shape >= c) return BSSN_EINVAL;
@@ -327,18 +334,20 @@ int launch_rhs_split(int shape, const RhsArgs& A, const BssnBlockDesc* blocks_de
     int st = prepare_split(shape);
     if (st) return st;
     const ZipGrid g = zip_grid ? ZipGrid{zip_grid[0], zip_grid[1], zip_grid[2]} : ZipGrid{0, 0, 0};
+    zip_in = zip_in && zip_grid;
     const int64_t zs = chunk * t.nz;  // slot stride
     for (int64_t c0 = 0; c0 < ntasks; c0 += chunk) {
         const int n = (int)(ntasks - c0 < chunk ? ntasks - c0 : chunk);
         if (tm && (st = tm->start(KernelTimer::DERIV, s))) return st;
-        (g.gx ? t.deriv_zip : t.deriv)<<<n, t.threads, t.smem, s>>>(A.u, blocks_dev, tasks_dev + c0,
-                                                                    scratch, zs, g);
+        (zip_in ? t.deriv_zip : t.deriv)<<<n, t.threads, t.smem, s>>>(A.u, blocks_dev, tasks_dev + c0,
+                                                                      scratch, zs, g);
         st = cuda_status(cudaGetLastError());
         if (!st && tm) st = tm->stop(s);
         if (st) return st;
         if (tm && (st = tm->start(KernelTimer::EQ, s))) return st;
         const int parts = (t.nz + kEqThreads - 1) / kEqThreads;
-        t.eq<<<n * parts, kEqThreads, t.eq_smem, s>>>(A, blocks_dev, tasks_dev + c0, scratch, zs, g);
+        t.eq<<<n * parts, kEqThreads, eq_smem_bytes(), s>>>(A, blocks_dev, tasks_dev + c0, scratch,
+                                                             zs, g, zip_in ? 1 : 0);
         st = cuda_status(cudaGetLastError());
         if (!st && tm) st = tm->stop(s);
         if (st) return st;
