@@ -201,6 +201,11 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
     const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(src));
 }
+// 16-byte copy, both addresses 16-byte aligned; bypasses L1 (streamed data)
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(src));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
 

@@ -11,8 +11,9 @@
 //     derivatives and summed KO term to a scratch array;
 //   * eq_kernel evaluates the equations per zone (rhs_equations.cuh, the same
 //     code as the fused kernel) reading those derivatives back.
-// The scratch is slot-major, [slot][task * NZ + thread], so both passes move
-// whole rows of consecutive zones.  A task list longer than the scratch is
+// The scratch holds slot pairs, [slot / 2][task * NZ + thread][slot % 2]
+// (every variable has an even number of slots), so both passes move 16-byte
+// pairs in whole rows of consecutive zones.  A task list longer than the scratch is
 // processed in chunks, each a derivative launch followed by an equation
 // launch on the same stream.
 //
@@ -54,6 +55,7 @@ __host__ __device__ constexpr int deriv_min_ctas(int threads) {
 // read by the variable just consumed
 constexpr int kPrefetchSteps = 6;
 constexpr int kRingSlots = (kPrefetchSteps + 1) * kSlotsSecond;
+constexpr int kRingPairs = kRingSlots / 2;
 constexpr int kEqThreads = 128;
 // derivative pass: shared-memory tiles (variables staged kDerivBuffers - 1 ahead)
 constexpr int kDerivBuffers = 2;
@@ -111,8 +113,8 @@ deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
     // brick, or (node grid given: direct form or stage mode) only the zones
     // that own their node
     const bool keep = th.active && (g.gx == 0 || owns_node(blk, o, th.t, g));
-    // next scratch slot of this zone (kept zones only advance it)
-    double* w = S + (int64_t)blockIdx.x * Bk::NZ + tid;
+    // next scratch slot pair of this zone (kept zones only advance it)
+    double2* w = reinterpret_cast<double2*>(S) + (int64_t)blockIdx.x * Bk::NZ + tid;
     __syncthreads();
 
     // variables in flight kDerivBuffers - 1 ahead; one commit group per
@@ -159,7 +161,7 @@ deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
                 const double v[kSlotsSecond] = {r[0].d1, r[1].d1, r[2].d1, r[0].d2, xy, xz,
                                                 r[1].d2, yz, r[2].d2, r[0].ko + r[1].ko + r[2].ko};
 #pragma unroll
-                for (int q = 0; q < kSlotsSecond; q++, w += zs) *w = v[q];
+                for (int q = 0; q < kSlotsSecond; q += 2, w += zs) *w = make_double2(v[q], v[q + 1]);
             }
         } else {
             Dir3 r[3];
@@ -168,7 +170,7 @@ deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
                 const double v[kSlotsFirst] = {r[0].d1, r[1].d1, r[2].d1,
                                                r[0].ko + r[1].ko + r[2].ko};
 #pragma unroll
-                for (int q = 0; q < kSlotsFirst; q++, w += zs) *w = v[q];
+                for (int q = 0; q < kSlotsFirst; q += 2, w += zs) *w = make_double2(v[q], v[q + 1]);
             }
         }
     }
@@ -192,7 +194,7 @@ eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
           ZipGrid g, int zip_in) {
     using Bk = Brick<BX, BY, BZ>;
     constexpr int PARTS = (Bk::NZ + kEqThreads - 1) / kEqThreads;
-    extern __shared__ __align__(16) double ring[];  // [kRingSlots][T] | vals [NVARS][T]
+    extern __shared__ __align__(16) double ring[];  // [kRingPairs][T][2] | vals [NVARS][T]
     const int tid = threadIdx.x;
     const int task = blockIdx.x / PARTS;
     const int l = (blockIdx.x % PARTS) * kEqThreads + tid;  // zone index in the brick
@@ -212,19 +214,21 @@ eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
                (int64_t)g.gx * ((blk.g0[1] + za1 - PW) + (int64_t)g.gy * (blk.g0[2] + za2 - PW));
     }
     const int64_t in_idx = zip_in ? node : pidx;
-    const double* in = S + (int64_t)task * Bk::NZ + l;
-    double* col = ring + tid;
+    const double2* in = reinterpret_cast<const double2*>(S) + (int64_t)task * Bk::NZ + l;
+    double2* col = reinterpret_cast<double2*>(ring) + tid;   // this thread's ring column
     double* vals = ring + kRingSlots * kEqThreads + tid;  // [NVARS][kEqThreads]
     // the zone's 24 variables first, as their own commit group
 #pragma unroll
     for (int v = 0; v < NVARS; v++) cp_async8(vals + v * kEqThreads, A.u.p[v] + in_idx);
     cp_async_commit();
+    // slot pair P of the zone lives in ring row P % kRingPairs (slot bases
+    // and counts are even, so a variable's slots are whole pairs)
     auto issue = [&](int step) {
         if (step < NVARS) {
-            const int b = slot_base(step), n = slot_len(step);
+            const int b = slot_base(step) / 2, n = slot_len(step) / 2;
 #pragma unroll
-            for (int q = 0; q < kSlotsSecond; q++)
-                if (q < n) cp_async8(col + ((b + q) % kRingSlots) * kEqThreads, in + (int64_t)(b + q) * zs);
+            for (int q = 0; q < kSlotsSecond / 2; q++)
+                if (q < n) cp_async16(col + ((b + q) % kRingPairs) * kEqThreads, in + (int64_t)(b + q) * zs);
         }
         cp_async_commit();  // empty groups past the last variable keep the count fixed
     };
@@ -237,7 +241,10 @@ eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
         constexpr bool SECOND = decltype(tag)::value;
         cp_async_wait_pending<kPrefetchSteps - 1>();
         const int b = slot_base(step);
-        auto rd = [&](int q) { return col[((b + q) % kRingSlots) * kEqThreads]; };
+        auto rd = [&](int q) {
+            const double2 p = col[(((b + q) / 2) % kRingPairs) * kEqThreads];
+            return ((b + q) & 1) ? p.y : p.x;
+        };
 #pragma unroll
         for (int q = 0; q < 3; q++) d1[q] = rd(q);
         if (SECOND) {

@@ -167,32 +167,22 @@ __global__ void __launch_bounds__(256) node_stage_kernel(int stage, MutVars im, 
     int bad = 0;
     for (int64_t node = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; node < n;
          node += (int64_t)gridDim.x * blockDim.x) {
-        double v[NVARS];
-        if (stage < 3) {
-            const double cu = M_(kRK4_U[stage + 1], dt);
-            const double cc = M_(kRK4_C[stage], dt);
-            double kk[NVARS], a0[NVARS];
+        double k[NVARS], v[NVARS], a[NVARS];
 #pragma unroll
-            for (int q = 0; q < NVARS; q++) {
-                kk[q] = __ldg(R.p[q] + node);
-                v[q] = u.p[q][node];
-                a0[q] = stage == 0 ? v[q] : acc.p[q][node];
+        for (int q = 0; q < NVARS; q++) {  // every load before the first store
+            k[q] = __ldg(R.p[q] + node);
+            v[q] = stage < 3 ? u.p[q][node] : 0.0;
+            a[q] = stage > 0 ? acc.p[q][node] : 0.0;
+        }
+        bad += stage_node(stage, dt, k, v, a, enforce, chi_floor);
+#pragma unroll
+        for (int q = 0; q < NVARS; q++) {
+            if (stage < 3) {
+                acc.p[q][node] = a[q];
+                im.p[q][node] = v[q];
+            } else {
+                u.p[q][node] = v[q];
             }
-#pragma unroll
-            for (int q = 0; q < NVARS; q++) {
-                acc.p[q][node] = A_(a0[q], M_(cc, kk[q]));
-                v[q] = A_(v[q], M_(cu, kk[q]));
-            }
-            if (enforce) bad += enforce_regs(v, chi_floor);
-#pragma unroll
-            for (int q = 0; q < NVARS; q++) im.p[q][node] = v[q];
-        } else {
-            const double cc = M_(kRK4_C[3], dt);
-#pragma unroll
-            for (int q = 0; q < NVARS; q++) v[q] = A_(acc.p[q][node], M_(cc, __ldg(R.p[q] + node)));
-            bad += enforce_regs(v, chi_floor);
-#pragma unroll
-            for (int q = 0; q < NVARS; q++) u.p[q][node] = v[q];
         }
     }
     if (status && bad) atomicAdd(status, bad);
