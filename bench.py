@@ -159,6 +159,17 @@ def _plain(o):
         return str(o)
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -170,7 +181,7 @@ def measured_peaks():
 # ---------------------------------------------------------------------------
 # reference arm: the reference's own CPU bssnrhs on the host cores
 # ---------------------------------------------------------------------------
-def cpu_reference_rate(sides_all, seconds=15.0, threads=0):
+def cpu_reference_rate(sides_all, seconds=15.0, threads=0, target=2.5e6):
     """Time the reference CPU right-hand side (oracle/_ref, compiled from the
     reference sources; else the repository's CPU restatement) on a bounded,
     size-stratified sample of the workload's blocks with all host threads.
@@ -190,7 +201,6 @@ def cpu_reference_rate(sides_all, seconds=15.0, threads=0):
     sides_all = np.asarray(sides_all)
     uniq, counts = np.unique(sides_all, return_counts=True)
     zones_all = float(((sides_all - 6.0) ** 3).sum())
-    target = 2.5e6
     frac = min(1.0, target / zones_all)
     sample = []
     for s, c in zip(uniq, counts):
@@ -472,7 +482,10 @@ def main():
            "autotune_ms": {str(k): v for k, v in table.items()}}
     if not args.no_cpu:
         rate, info = cpu_reference_rate(spec.sides, seconds=15.0)
-        out["cpu_baseline"] = dict(info, value=rate, unit="zone-updates/s")
+        rate1, info1 = cpu_reference_rate(spec.sides, seconds=5.0, threads=1, target=2.5e5)
+        out["cpu_baseline"] = dict(info, value=rate, unit="zone-updates/s", cpu_model=cpu_model(),
+                                   nproc=os.cpu_count(),
+                                   one_thread={"value": rate1, "sample": info1["sample"]})
     print(json.dumps(out, default=_plain))
     if dist is not None:
         dist.destroy_process_group()
