@@ -78,6 +78,11 @@ def _sig():
     lib.bssn_rk4_plan_time_kernels.argtypes = [vp, i, vp, P(d)]
     lib.bssn_rk4_plan_launches_per_step.argtypes = [vp]
     lib.bssn_tile_mode.argtypes = [i]
+    lib.bssn_mesh_partition.argtypes = [P(BssnBlockDesc), i, i, P(C.c_int32)]
+    lib.bssn_rk4_plan_stage.argtypes = [vp, vp, d, i, vp]
+    lib.bssn_rk4_plan_stage_state.argtypes = [vp, vp]
+    lib.bssn_halo_pack_f64.argtypes = [vp, vp, vp, i64, vp]
+    lib.bssn_halo_unpack_f64.argtypes = [vp, vp, vp, i64, vp]
     lib.bssn_rk4_plan_violations.argtypes = [vp, P(i)]
     lib.bssn_rk4_plan_destroy.argtypes = [vp]
     lib.bssn_constraints_f64.argtypes = [vp, vp, vp, vp]
@@ -142,6 +147,13 @@ class MeshSpec:
     h: float
     xmin: float
     sides: np.ndarray = field(default=None)
+    # coordinate of node (0,0,0) per axis when it differs between axes (the
+    # box of one rank of a partitioned mesh); None: xmin on every axis
+    origin: tuple = None
+
+    @property
+    def origin3(self):
+        return tuple(self.origin) if self.origin is not None else (self.xmin,) * 3
 
     @property
     def n_nodes(self):
@@ -221,7 +233,7 @@ def deriv(kind, D, u, h, sz, bflag, stream=None):
 def initial_data(U, spec: MeshSpec, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0), m1=0.5, m2=0.5,
                  chi_floor=1e-4, eps=1e-8, seed=20261203, stream=None):
     G = (C.c_int32 * 3)(*spec.G)
-    xm = (C.c_double * 3)(spec.xmin, spec.xmin, spec.xmin)
+    xm = (C.c_double * 3)(*spec.origin3)
     b = (C.c_double * 6)(*bh)
     check(lib.bssn_initial_data_f64(ptrs(U), G, xm, spec.h, b, m1, m2, chi_floor, eps, seed, stream_ptr(stream)), "initial_data")
 

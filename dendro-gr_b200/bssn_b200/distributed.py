@@ -1,0 +1,244 @@
+"""Multi-GPU evolution: block partition with a halo exchange before every
+RK4 stage (one process per GPU).
+
+The blocks are split along their Z-order into ranges of about equal zone
+counts (bssn_mesh_partition; the reference partitions its octree along a
+space-filling curve).  Rank r evolves its own blocks as a mesh of their own
+on the bounding box of the blocks' padded regions in the node grid, so the
+library's ghost fill, right-hand side, owner rule and stage kernels run
+unchanged on the box.  Every node of the box that r's blocks read but a block
+of another rank owns (the zip's owner rule: a node on a block's upper face
+belongs to the next block) is received from its owner before each stage, and
+r sends the nodes it owns that other ranks read -- the reference's
+ghostExchangeStart / ghostExchangeRecvSync around its unzip
+(BSSN_GR/src/rkBSSN.cpp:620-641).  Lists are in increasing global node
+order on both sides, so a send matches its receive element by element.
+
+Transport: torch.distributed point-to-point (NCCL between GPUs; with the
+gloo backend the buffers go through host memory).  Packing and unpacking run
+on the GPU (bssn_halo_pack_f64 / bssn_halo_unpack_f64), or, for host arrays,
+as numpy gathers (the same lists).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import (NVARS, BssnBlockDesc, Mesh, MeshSpec, RK4Plan, PLAN_ENFORCE_STAGES, PLAN_GRAPH,
+               check, default_params, lib, ptrs, stream_ptr)
+
+OCT = 6  # nodes per octant edge
+
+
+def partition(spec: MeshSpec, nparts: int) -> np.ndarray:
+    """Rank of every block (int32): nparts Z-order ranges, balanced by zones."""
+    part = np.zeros(spec.nblocks, dtype=np.int32)
+    check(lib.bssn_mesh_partition(spec.blocks, spec.nblocks, nparts,
+                                  part.ctypes.data_as(C.POINTER(C.c_int32))), "mesh_partition")
+    return part
+
+
+def _owner_blocks(spec: MeshSpec) -> np.ndarray:
+    """Block owning each node of the grid, as an array [z, y, x]: the block
+    whose octants contain the node's octant (the last octant on an axis for
+    the grid's upper boundary nodes)."""
+    G = np.asarray(spec.G, dtype=np.int64)
+    M = (G - 1) // OCT
+    omap = np.full((M[2], M[1], M[0]), -1, dtype=np.int32)
+    for b in range(spec.nblocks):
+        blk = spec.blocks[b]
+        o = np.array(blk.g0[:], dtype=np.int64) // OCT
+        w = (int(blk.sz) - 7) // OCT
+        omap[o[2]:o[2] + w, o[1]:o[1] + w, o[0]:o[0] + w] = b
+    assert (omap >= 0).all(), "blocks must tile the grid"
+    ox = np.minimum(np.arange(G[0]) // OCT, M[0] - 1)
+    oy = np.minimum(np.arange(G[1]) // OCT, M[1] - 1)
+    oz = np.minimum(np.arange(G[2]) // OCT, M[2] - 1)
+    return omap[oz[:, None, None], oy[None, :, None], ox[None, None, :]]
+
+
+def _needed_mask(spec: MeshSpec, mine) -> np.ndarray:
+    """Nodes read by the ghost fill of the given blocks: their padded boxes
+    (3 nodes around the interior) clipped to the grid, as a mask [z, y, x]."""
+    G = spec.G
+    mask = np.zeros((G[2], G[1], G[0]), dtype=bool)
+    for b in mine:
+        blk = spec.blocks[int(b)]
+        lo = [max(int(blk.g0[d]) - 3, 0) for d in range(3)]
+        hi = [min(int(blk.g0[d]) + int(blk.sz) - 3, G[d]) for d in range(3)]
+        mask[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]] = True
+    return mask
+
+
+@dataclass
+class Subdomain:
+    """Rank `rank`'s part of a partitioned mesh."""
+    spec: MeshSpec           # the rank's own mesh on its box
+    lo: tuple                # global node of local node (0, 0, 0)
+    blocks: np.ndarray       # global ids of the rank's blocks, in local order
+    send: dict               # peer -> local node indices sent to it (int64)
+    recv: dict               # peer -> local node indices received from it
+    owned: np.ndarray        # local indices of the nodes this rank owns
+    owned_global: np.ndarray  # their global node indices
+
+    @property
+    def n_nodes(self):
+        return self.spec.n_nodes
+
+
+def subdomain(spec: MeshSpec, part: np.ndarray, rank: int) -> Subdomain:
+    """Build rank `rank`'s box mesh and halo lists (host, from the global
+    mesh; every rank computes the same lists for its peers)."""
+    world = int(part.max()) + 1
+    G = np.asarray(spec.G, dtype=np.int64)
+    owner = part[_owner_blocks(spec)]                      # rank owning each node
+    needed = [_needed_mask(spec, np.nonzero(part == r)[0]) for r in range(world)]
+    mine = np.nonzero(part == rank)[0]
+    # box: the union of the padded boxes (clipped to the grid), widened to
+    # whole octants so the box is a grid of its own (6M+1 nodes per axis,
+    # block origins on octant corners)
+    z, y, x = np.nonzero(needed[rank])
+    lo = np.array([x.min(), y.min(), z.min()], dtype=np.int64) // OCT * OCT
+    hi = np.array([x.max(), y.max(), z.max()], dtype=np.int64)
+    hi = np.minimum(lo + (hi - lo + OCT - 1) // OCT * OCT, G - 1)
+    L = hi - lo + 1
+
+    def to_local(gidx):
+        gx = gidx % G[0]
+        gy = (gidx // G[0]) % G[1]
+        gz = gidx // (G[0] * G[1])
+        return (gx - lo[0]) + L[0] * ((gy - lo[1]) + L[1] * (gz - lo[2]))
+
+    flat_owner = owner.ravel()
+    send, recv = {}, {}
+    for q in range(world):
+        if q == rank:
+            continue
+        r_ids = np.nonzero(needed[rank].ravel() & (flat_owner == q))[0]
+        s_ids = np.nonzero(needed[q].ravel() & (flat_owner == rank))[0]
+        if len(r_ids):
+            recv[q] = to_local(r_ids).astype(np.int64)
+        if len(s_ids):
+            send[q] = to_local(s_ids).astype(np.int64)
+    own_ids = np.nonzero(flat_owner == rank)[0]
+    # the rank's blocks, origins shifted into the box, offsets renumbered
+    blocks = (BssnBlockDesc * len(mine))()
+    off = 0
+    for i, b in enumerate(mine):
+        src = spec.blocks[int(b)]
+        C.memmove(C.byref(blocks[i]), C.byref(src), C.sizeof(BssnBlockDesc))
+        for d in range(3):
+            blocks[i].g0[d] = int(src.g0[d]) - int(lo[d])
+        blocks[i].offset = off
+        n = int(src.sz) ** 3
+        off += (n + 1) // 2 * 2
+    origin = tuple(spec.origin3[d] + float(lo[d]) * spec.h for d in range(3))
+    local = MeshSpec(blocks, len(mine), tuple(int(v) for v in L), spec.h, spec.xmin,
+                     np.array([int(spec.blocks[int(b)].sz) for b in mine], dtype=np.int32), origin)
+    return Subdomain(local, tuple(int(v) for v in lo), mine, send, recv,
+                     to_local(own_ids).astype(np.int64), own_ids.astype(np.int64))
+
+
+class HaloExchange:
+    """Per-stage exchange of a rank's halo nodes with torch.distributed
+    point-to-point operations (every rank posts all its sends and receives
+    in increasing peer order)."""
+
+    def __init__(self, sub: Subdomain, device, group=None):
+        import torch
+        import torch.distributed as dist
+        self.sub = sub
+        self.device = device
+        self.group = group
+        self.peers = sorted(set(sub.send) | set(sub.recv))
+        gpu = device.type == "cuda"
+        # gloo moves host tensors only: device buffers then go through pinned
+        # host copies
+        self.via_host = gpu and dist.get_backend(group) == "gloo"
+        self.idx = {}
+        self.sbuf, self.rbuf, self.hbuf = {}, {}, {}
+        for q in self.peers:
+            for kind, lists, bufs in (("s", sub.send, self.sbuf), ("r", sub.recv, self.rbuf)):
+                if q in lists:
+                    ix = torch.from_numpy(lists[q])
+                    self.idx[(kind, q)] = ix.to(device) if gpu else ix
+                    bufs[q] = torch.empty(NVARS * len(lists[q]), dtype=torch.float64, device=device)
+                    if self.via_host:
+                        self.hbuf[(kind, q)] = torch.empty(NVARS * len(lists[q]), dtype=torch.float64,
+                                                           pin_memory=True)
+
+    def run(self, fields):
+        """fields: 24 device pointers (GPU) or a (24, n) float64 CPU tensor."""
+        import torch
+        import torch.distributed as dist
+        gpu = self.device.type == "cuda"
+        for q, buf in self.sbuf.items():
+            ix = self.idx[("s", q)]
+            if gpu:
+                check(lib.bssn_halo_pack_f64(C.c_void_p(buf.data_ptr()), fields, C.c_void_p(ix.data_ptr()),
+                                             len(ix), stream_ptr()), "halo_pack")
+            else:
+                buf.copy_(fields[:, ix].reshape(-1))
+        send, recv = dict(self.sbuf), dict(self.rbuf)
+        if self.via_host:
+            for q in send:
+                self.hbuf[("s", q)].copy_(send[q])
+                send[q] = self.hbuf[("s", q)]
+            for q in recv:
+                recv[q] = self.hbuf[("r", q)]
+        if gpu:
+            torch.cuda.current_stream().synchronize()
+        ops = []
+        for q in self.peers:
+            if q in send:
+                ops.append(dist.P2POp(dist.isend, send[q], q, group=self.group))
+            if q in recv:
+                ops.append(dist.P2POp(dist.irecv, recv[q], q, group=self.group))
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+        if self.via_host:
+            for q in recv:
+                self.rbuf[q].copy_(recv[q])
+        for q, buf in self.rbuf.items():
+            ix = self.idx[("r", q)]
+            if gpu:
+                check(lib.bssn_halo_unpack_f64(fields, C.c_void_p(buf.data_ptr()), C.c_void_p(ix.data_ptr()),
+                                               len(ix), stream_ptr()), "halo_unpack")
+            else:
+                fields[:, ix] = buf.reshape(NVARS, -1)
+
+
+class PartitionedRK4:
+    """One rank's share of a partitioned RK4 evolution on its GPU: the
+    rank's box mesh, an RK4 plan on it run stage by stage, and the halo
+    exchange of the stage input before each stage."""
+
+    def __init__(self, spec: MeshSpec, rank: int, world: int, params=None, group=None,
+                 flags=PLAN_ENFORCE_STAGES, tile=None):
+        import torch
+        self.part = partition(spec, world)
+        self.sub = subdomain(spec, self.part, rank)
+        self.mesh = Mesh(self.sub.spec)
+        # stages run one by one (eagerly) around the exchanges
+        self.plan = RK4Plan(self.mesh, params or default_params(), flags & ~PLAN_GRAPH)
+        if tile is not None:
+            self.plan.set_tile(tile)
+        im = (C.c_void_p * NVARS)()
+        check(lib.bssn_rk4_plan_stage_state(self.plan.h, im), "stage_state")
+        self.im = im
+        self.ex = HaloExchange(self.sub, torch.device("cuda"), group)
+
+    def step(self, U, dt):
+        """Advance the rank's local state U ((24, n_local) CUDA tensor) by one
+        RK4 step; the halo nodes are refreshed before every stage."""
+        u = ptrs(U)
+        for stage in range(4):
+            self.ex.run(u if stage == 0 else self.im)
+            check(lib.bssn_rk4_plan_stage(self.plan.h, u, dt, stage, stream_ptr()), "plan_stage")
+
+    def close(self):
+        self.plan.close()
+        self.mesh.close()

@@ -360,6 +360,36 @@ int bssn_remesh_decide_f64(bssn_mesh mesh, const double* const* unzip_dev, const
     return st;
 }
 
+int bssn_mesh_partition(const BssnBlockDesc* blocks, int nblocks, int nparts, int32_t* part) {
+    return bssn::mesh_partition(blocks, nblocks, nparts, part);
+}
+
+int bssn_rk4_plan_stage(bssn_rk4_plan plan, double* const* u_dev, double dt, int stage,
+                        bssn_stream_t stream) {
+    if (!plan || !u_dev || stage < 0 || stage > 3) return BSSN_EINVAL;
+    for (int v = 0; v < bssn::NVARS; v++)
+        if (!u_dev[v]) return BSSN_EINVAL;
+    return bssn::plan_enqueue_stage(plan->p, u_dev, dt, stage, S(stream));
+}
+
+int bssn_rk4_plan_stage_state(bssn_rk4_plan plan, double** im_dev) {
+    if (!plan || !im_dev) return BSSN_EINVAL;
+    for (int v = 0; v < bssn::NVARS; v++) im_dev[v] = plan->p->im + (int64_t)v * plan->p->n_nodes;
+    return 0;
+}
+
+int bssn_halo_pack_f64(double* buf_dev, const double* const* u_dev, const int64_t* idx_dev,
+                       int64_t n, bssn_stream_t stream) {
+    if (n < 0 || (n > 0 && (!buf_dev || !u_dev || !idx_dev))) return BSSN_EINVAL;
+    return bssn::launch_halo_pack(buf_dev, u_dev, idx_dev, n, S(stream));
+}
+
+int bssn_halo_unpack_f64(double* const* u_dev, const double* buf_dev, const int64_t* idx_dev,
+                         int64_t n, bssn_stream_t stream) {
+    if (n < 0 || (n > 0 && (!buf_dev || !u_dev || !idx_dev))) return BSSN_EINVAL;
+    return bssn::launch_halo_unpack(u_dev, buf_dev, idx_dev, n, S(stream));
+}
+
 int bssn_tile_count(void) { return bssn::tile_count(); }
 
 long bssn_tile_selfcheck(int tile) { return bssn::tile_selfcheck(tile); }

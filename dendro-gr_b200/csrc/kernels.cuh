@@ -21,6 +21,11 @@ int launch_unzip(const MeshState* m, double* const* unz, const double* const* zi
                  int nvars, cudaStream_t s);
 int launch_zip(const MeshState* m, double* const* zip, const double* const* unz,
                int nvars, cudaStream_t s);
+// halo exchange buffers: buf[v*n + i] = u[v][idx[i]] and back
+int launch_halo_pack(double* buf, const double* const* u, const int64_t* idx, int64_t n,
+                     cudaStream_t s);
+int launch_halo_unpack(double* const* u, const double* buf, const int64_t* idx, int64_t n,
+                       cudaStream_t s);
 int launch_zip_stage(const MeshState* m, int stage, double* const* im, double* const* acc,
                      double* const* u, const double* const* R, double dt, int enforce,
                      double chi_floor, int* status, cudaStream_t s);

@@ -208,6 +208,30 @@ int mesh_tasks_side(MeshState* m, int tile, int side, const BrickTask** tasks, i
     return 0;
 }
 
+// Split the blocks into nparts ranges of their Z-order (the order of their
+// origins' Morton keys) holding about equal numbers of interior zones, as the
+// reference partitions its octree along a space-filling curve.
+int mesh_partition(const BssnBlockDesc* blocks, int nblocks, int nparts, int32_t* part) {
+    if (!blocks || nblocks <= 0 || nparts <= 0 || !part) return BSSN_EINVAL;
+    std::vector<int> order(nblocks);
+    for (int b = 0; b < nblocks; b++) order[b] = b;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return morton_key(blocks[a]) < morton_key(blocks[b]);
+    });
+    double total = 0;
+    for (int b = 0; b < nblocks; b++) total += std::pow((double)(blocks[b].sz - 6), 3);
+    double acc = 0;
+    for (int i = 0; i < nblocks; i++) {
+        const int b = order[i];
+        const double z = std::pow((double)(blocks[b].sz - 6), 3);
+        // the part holding this block's zone midpoint
+        int r = (int)((acc + 0.5 * z) / total * nparts);
+        part[b] = r < nparts ? r : nparts - 1;
+        acc += z;
+    }
+    return 0;
+}
+
 int mesh_tasks(MeshState* m, int tile, const BrickTask** tasks, int* ntasks) {
     return mesh_tasks_side(m, tile, 0, tasks, ntasks);
 }
@@ -223,6 +247,52 @@ int launch_unzip(const MeshState* m, double* const* unz, const double* const* zi
     if (m->n_pad_chunks == 0) return 0;
     unzip_kernel<<<m->n_pad_chunks, CHUNK, 0, s>>>(u, z, nvars, m->d_blocks, m->d_pad_chunks,
                                                    m->G[0], m->G[1], m->G[2]);
+    return cuda_status(cudaGetLastError());
+}
+
+namespace {
+__global__ void __launch_bounds__(256) halo_pack_kernel(double* __restrict__ buf, ConstVars u,
+                                                        const int64_t* __restrict__ idx, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t node = idx[i];
+#pragma unroll
+        for (int v = 0; v < NVARS; v++) buf[v * n + i] = __ldg(u.p[v] + node);
+    }
+}
+__global__ void __launch_bounds__(256) halo_unpack_kernel(MutVars u, const double* __restrict__ buf,
+                                                          const int64_t* __restrict__ idx, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t node = idx[i];
+        double v[NVARS];
+#pragma unroll
+        for (int q = 0; q < NVARS; q++) v[q] = __ldg(buf + q * n + i);
+#pragma unroll
+        for (int q = 0; q < NVARS; q++) u.p[q][node] = v[q];
+    }
+}
+int halo_grid(int64_t n) {
+    int64_t b = (n + 255) / 256;
+    return (int)(b < 1 ? 1 : (b > 148 * 32 ? 148 * 32 : b));
+}
+}  // namespace
+
+int launch_halo_pack(double* buf, const double* const* u, const int64_t* idx, int64_t n,
+                     cudaStream_t s) {
+    if (n <= 0) return 0;
+    ConstVars cu;
+    for (int v = 0; v < NVARS; v++) cu.p[v] = u[v];
+    halo_pack_kernel<<<halo_grid(n), 256, 0, s>>>(buf, cu, idx, n);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_halo_unpack(double* const* u, const double* buf, const int64_t* idx, int64_t n,
+                       cudaStream_t s) {
+    if (n <= 0) return 0;
+    MutVars mu;
+    for (int v = 0; v < NVARS; v++) mu.p[v] = u[v];
+    halo_unpack_kernel<<<halo_grid(n), 256, 0, s>>>(mu, buf, idx, n);
     return cuda_status(cudaGetLastError());
 }
 

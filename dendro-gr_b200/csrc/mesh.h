@@ -60,6 +60,7 @@ int mesh_tasks_side(MeshState* m, int tile, int side, const BrickTask** tasks, i
 int mesh_scratch(MeshState* m, int64_t zones);
 // Scratch zones a split tile needs for the task list (tile, side), capped.
 int64_t split_need(MeshState* m, int tile, int side);
+int mesh_partition(const BssnBlockDesc* blocks, int nblocks, int nparts, int32_t* part);
 int mesh_generate(int mode, const int32_t dims[3], const double p[4], uint64_t seed,
                   double xmin, double L, BssnBlockDesc* blocks, int* nblocks,
                   int32_t G[3], double* h);

@@ -126,7 +126,7 @@ int plan_tile(const Plan* p, int side) {
     auto it = p->mesh->tuned.find(p->direct ? kAllZOrder : side);
     const int t = it == p->mesh->tuned.end() ? -1 : it->second;
     if (p->direct) return (t >= 0 && tile_mode(t) == 1) ? t : default_split_tile();
-    return t >= 0 ? t : 0;
+    return t >= 0 ? t : default_split_tile();
 }
 
 int plan_set_tile(Plan* p, int side, int tile) {
@@ -213,7 +213,10 @@ int plan_rhs(Plan* p, cudaStream_t s, KernelTimer* tm, const double* const* src)
     return 0;
 }
 
-int plan_enqueue(Plan* p, double* const* u, double dt, cudaStream_t s) {
+// One RK4 stage (0..3) of the step from state u: stage 0 reads u, the others
+// the plan's intermediate stage state; stages 0..2 write that state and the
+// accumulator, stage 3 writes u.  Each form's own sequence (see the header).
+int plan_enqueue_stage(Plan* p, double* const* u, double dt, int stage, cudaStream_t s) {
     MeshState* m = p->mesh;
     double* Pp[NVARS];
     double* Rp[NVARS];
@@ -224,37 +227,25 @@ int plan_enqueue(Plan* p, double* const* u, double dt, cudaStream_t s) {
     set_ptrs(p->im, p->n_nodes, Ip);
     set_ptrs(p->acc, p->n_nodes, Ap);
     const int enf = (p->flags & BSSN_PLAN_ENFORCE_STAGES) ? 1 : 0;
-    if (p->direct) {
+    const double* const* src = stage == 0 ? (const double* const*)u : (const double* const*)Ip;
+    if (p->direct || plan_zipped_rhs(p)) {
         double* Rz[NVARS];
         set_ptrs(p->Rz, p->n_nodes, Rz);
-        for (int stage = 0; stage < 4; stage++) {
-            const double* const* src = stage == 0 ? (const double* const*)u : (const double* const*)Ip;
-            int st = plan_rhs(p, s, nullptr, src);
-            if (!st) st = launch_node_stage(stage, Ip, Ap, u, Rz, p->n_nodes, dt, enf,
-                                            p->prm.chi_floor, p->status, s);
-            if (st) return st;
-        }
-        return 0;
+        int st = p->direct ? 0 : launch_unzip(m, Pp, src, NVARS, s);
+        if (!st) st = plan_rhs(p, s, nullptr, p->direct ? src : nullptr);
+        if (!st) st = launch_node_stage(stage, Ip, Ap, u, Rz, p->n_nodes, dt, enf, p->prm.chi_floor,
+                                        p->status, s);
+        return st;
     }
-    if (plan_zipped_rhs(p)) {
-        double* Rz[NVARS];
-        set_ptrs(p->Rz, p->n_nodes, Rz);
-        for (int stage = 0; stage < 4; stage++) {
-            const double* const* src = stage == 0 ? (const double* const*)u : (const double* const*)Ip;
-            int st = launch_unzip(m, Pp, src, NVARS, s);
-            if (!st) st = plan_rhs(p, s, nullptr, nullptr);
-            if (!st) st = launch_node_stage(stage, Ip, Ap, u, Rz, p->n_nodes, dt, enf,
-                                            p->prm.chi_floor, p->status, s);
-            if (st) return st;
-        }
-        return 0;
-    }
+    int st = launch_unzip(m, Pp, src, NVARS, s);
+    if (!st) st = plan_rhs(p, s, nullptr, nullptr);
+    if (!st) st = launch_zip_stage(m, stage, Ip, Ap, u, Rp, dt, enf, p->prm.chi_floor, p->status, s);
+    return st;
+}
+
+int plan_enqueue(Plan* p, double* const* u, double dt, cudaStream_t s) {
     for (int stage = 0; stage < 4; stage++) {
-        const double* const* src = stage == 0 ? (const double* const*)u : (const double* const*)Ip;
-        int st = launch_unzip(m, Pp, src, NVARS, s);
-        if (!st) st = plan_rhs(p, s, nullptr, nullptr);
-        if (!st) st = launch_zip_stage(m, stage, Ip, Ap, u, Rp, dt, enf, p->prm.chi_floor,
-                                       p->status, s);
+        const int st = plan_enqueue_stage(p, u, dt, stage, s);
         if (st) return st;
     }
     return 0;

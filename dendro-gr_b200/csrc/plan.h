@@ -36,6 +36,7 @@ struct Plan {
 int plan_create(MeshState* m, const BssnParams& prm, int flags, Plan** out);
 void plan_destroy(Plan* p);
 int plan_step(Plan* p, double* const* u, double dt, cudaStream_t s);
+int plan_enqueue_stage(Plan* p, double* const* u, double dt, int stage, cudaStream_t s);
 int plan_autotune(Plan* p, double* const* u, int reps, cudaStream_t s, float* times_out);
 int plan_tile(const Plan* p, int side);
 int plan_set_tile(Plan* p, int side, int tile);

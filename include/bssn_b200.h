@@ -300,8 +300,8 @@ int bssn_rk4_plan_step(bssn_rk4_plan plan, double* const* u_dev, double dt,
  * increasing side order, 1e30 for tiles not timed. */
 int bssn_rk4_plan_autotune(bssn_rk4_plan plan, double* const* u_dev, int reps,
                            bssn_stream_t stream, float* times);
-/* The tile the plan runs for block side `side` (the autotuned one; before
- * tuning 0, or for direct plans the default split tile). */
+/* The tile the plan runs for block side `side` (the autotuned or pinned
+ * one; before either, the split 7x7x7 tile). */
 int bssn_rk4_plan_tile(bssn_rk4_plan plan, int side);
 /* Pin the tile for block side `side` (0: every side; direct plans take one
  * split tile for all sides), as the autotuner would; the next step
@@ -343,6 +343,37 @@ int bssn_mesh_generate(int mode, const int32_t dims[3], const double p[4],
                        uint64_t seed, double xmin, double L,
                        BssnBlockDesc* blocks, int* nblocks, int32_t G[3],
                        double* h);
+
+/* ---------------------------------------------------------------------- */
+/* Multi-GPU form: the blocks are split along their Z-order and each rank
+ * evolves its own blocks on the bounding box of their padded regions in the
+ * node grid; before each stage the halo nodes its blocks read but other
+ * ranks own are exchanged (the reference's ghostExchangeStart / RecvSync
+ * around its unzip, rkBSSN.cpp:620-641, over MPI; here any point-to-point
+ * transport, e.g. NCCL send/recv, with these pack / unpack kernels). */
+
+/* part[b] = the rank of block b: nparts Z-order ranges (Morton keys of the
+ * blocks' origins) with about equal interior-zone counts; the reference
+ * partitions its octree along a space-filling curve (CMakeLists.txt:51).
+ * Host only. */
+int bssn_mesh_partition(const BssnBlockDesc* blocks, int nblocks, int nparts,
+                        int32_t* part);
+/* One RK4 stage (0..3) of a plan's step (the per-stage body of
+ * rkBSSN.cpp:764-860): stage 0 reads u_dev, stages 1..3 the plan's stage
+ * state; stages 0..2 write the stage state and the accumulator, stage 3
+ * writes u_dev.  Four calls with the same u_dev and dt make one step of
+ * bssn_rk4_plan_step (eagerly, no graph), with room for a halo exchange
+ * before each. */
+int bssn_rk4_plan_stage(bssn_rk4_plan plan, double* const* u_dev, double dt,
+                        int stage, bssn_stream_t stream);
+/* The 24 device arrays of the plan's intermediate stage state (G[0]*G[1]*G[2]
+ * doubles each; stages 1..3 read it). */
+int bssn_rk4_plan_stage_state(bssn_rk4_plan plan, double** im_dev);
+/* buf_dev[v*n + i] = u_dev[v][idx_dev[i]] for the 24 variables, and back. */
+int bssn_halo_pack_f64(double* buf_dev, const double* const* u_dev,
+                       const int64_t* idx_dev, int64_t n, bssn_stream_t stream);
+int bssn_halo_unpack_f64(double* const* u_dev, const double* buf_dev,
+                         const int64_t* idx_dev, int64_t n, bssn_stream_t stream);
 
 /* Number of compiled tiles and their brick shape (bx, by, bz, threads).
  * A tile runs its brick shape either fused (one kernel forms the derivatives

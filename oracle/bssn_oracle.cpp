@@ -795,6 +795,7 @@ void orc_zip(double** zip, const double** unzip, const OrcBlock* blks,
         int64_t o[3];
         for (int d = 0; d < 3; d++) o[d] = std::min<int64_t>(g[d] / 6, M[d] - 1);
         const int b = owner[o[0] + (size_t)M[0] * (o[1] + (size_t)M[1] * o[2])];
+        if (b < 0) continue;  // octant without a block (the box of one rank of a partition)
         const int s = blks[b].sz;
         const int64_t i = g[0] - blks[b].g0[0] + 3, j = g[1] - blks[b].g0[1] + 3,
                       k = g[2] - blks[b].g0[2] + 3;
