@@ -40,36 +40,12 @@ def partition(spec: MeshSpec, nparts: int) -> np.ndarray:
     return part
 
 
-def _owner_blocks(spec: MeshSpec) -> np.ndarray:
-    """Block owning each node of the grid, as an array [z, y, x]: the block
-    whose octants contain the node's octant (the last octant on an axis for
-    the grid's upper boundary nodes)."""
-    G = np.asarray(spec.G, dtype=np.int64)
-    M = (G - 1) // OCT
-    omap = np.full((M[2], M[1], M[0]), -1, dtype=np.int32)
-    for b in range(spec.nblocks):
-        blk = spec.blocks[b]
-        o = np.array(blk.g0[:], dtype=np.int64) // OCT
-        w = (int(blk.sz) - 7) // OCT
-        omap[o[2]:o[2] + w, o[1]:o[1] + w, o[0]:o[0] + w] = b
-    assert (omap >= 0).all(), "blocks must tile the grid"
-    ox = np.minimum(np.arange(G[0]) // OCT, M[0] - 1)
-    oy = np.minimum(np.arange(G[1]) // OCT, M[1] - 1)
-    oz = np.minimum(np.arange(G[2]) // OCT, M[2] - 1)
-    return omap[oz[:, None, None], oy[None, :, None], ox[None, None, :]]
-
-
-def _needed_mask(spec: MeshSpec, mine) -> np.ndarray:
-    """Nodes read by the ghost fill of the given blocks: their padded boxes
-    (3 nodes around the interior) clipped to the grid, as a mask [z, y, x]."""
-    G = spec.G
-    mask = np.zeros((G[2], G[1], G[0]), dtype=bool)
-    for b in mine:
-        blk = spec.blocks[int(b)]
-        lo = [max(int(blk.g0[d]) - 3, 0) for d in range(3)]
-        hi = [min(int(blk.g0[d]) + int(blk.sz) - 3, G[d]) for d in range(3)]
-        mask[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]] = True
-    return mask
+def _padded_box(blk, G):
+    """Inclusive node range [lo, hi] per axis read by a block's ghost fill:
+    its padded region (3 nodes around the interior) clipped to the grid."""
+    lo = np.array([max(int(blk.g0[d]) - 3, 0) for d in range(3)], dtype=np.int64)
+    hi = np.array([min(int(blk.g0[d]) + int(blk.sz) - 4, int(G[d]) - 1) for d in range(3)], dtype=np.int64)
+    return lo, hi
 
 
 @dataclass
@@ -90,39 +66,65 @@ class Subdomain:
 
 def subdomain(spec: MeshSpec, part: np.ndarray, rank: int) -> Subdomain:
     """Build rank `rank`'s box mesh and halo lists (host, from the global
-    mesh; every rank computes the same lists for its peers)."""
-    world = int(part.max()) + 1
+    block list; every rank computes its own lists).  All arrays span the
+    rank's box only: every node the rank sends (owned by it) or receives
+    (read by its blocks) lies in the box, and lexicographic (z, y, x) order
+    is the same in the box and in the grid, so a send list (ordered on the
+    sender's box) matches the receive list (ordered on the receiver's box)."""
     G = np.asarray(spec.G, dtype=np.int64)
-    owner = part[_owner_blocks(spec)]                      # rank owning each node
-    needed = [_needed_mask(spec, np.nonzero(part == r)[0]) for r in range(world)]
+    M = (G - 1) // OCT
     mine = np.nonzero(part == rank)[0]
-    # box: the union of the padded boxes (clipped to the grid), widened to
-    # whole octants so the box is a grid of its own (6M+1 nodes per axis,
-    # block origins on octant corners)
-    z, y, x = np.nonzero(needed[rank])
-    lo = np.array([x.min(), y.min(), z.min()], dtype=np.int64) // OCT * OCT
-    hi = np.array([x.max(), y.max(), z.max()], dtype=np.int64)
+    pads = [_padded_box(spec.blocks[b], G) for b in range(spec.nblocks)]
+    # box: the union of the rank's padded boxes, widened to whole octants so
+    # the box is a grid of its own (6M+1 nodes per axis, block origins on
+    # octant corners)
+    lo = np.min([pads[b][0] for b in mine], axis=0) // OCT * OCT
+    hi = np.max([pads[b][1] for b in mine], axis=0)
     hi = np.minimum(lo + (hi - lo + OCT - 1) // OCT * OCT, G - 1)
     L = hi - lo + 1
 
-    def to_local(gidx):
-        gx = gidx % G[0]
-        gy = (gidx // G[0]) % G[1]
-        gz = gidx // (G[0] * G[1])
-        return (gx - lo[0]) + L[0] * ((gy - lo[1]) + L[1] * (gz - lo[2]))
+    def touching(b):
+        return bool((pads[b][0] <= hi).all() and (pads[b][1] >= lo).all())
 
-    flat_owner = owner.ravel()
+    near = [b for b in range(spec.nblocks) if touching(b)]
+    # owner rank of every box node: the rank of the block whose octants hold
+    # the node's octant (the zip's owner rule); octant range of the box
+    olo = lo // OCT
+    ohi = np.minimum(hi // OCT, M - 1)
+    omap = np.full(tuple((ohi - olo + 1)[::-1]), -1, dtype=np.int32)
+    for b in near:
+        blk = spec.blocks[b]
+        o = np.array(blk.g0[:], dtype=np.int64) // OCT
+        w = (int(blk.sz) - 7) // OCT
+        a = np.maximum(o, olo) - olo
+        e = np.minimum(o + w - 1, ohi) - olo + 1
+        if (e > a).all():
+            omap[a[2]:e[2], a[1]:e[1], a[0]:e[0]] = part[b]
+    ax = [np.minimum((np.arange(L[d]) + lo[d]) // OCT, M[d] - 1) - olo[d] for d in range(3)]
+    owner = omap[ax[2][:, None, None], ax[1][None, :, None], ax[0][None, None, :]].ravel()
+
+    def mask_of(blocks):
+        m = np.zeros((L[2], L[1], L[0]), dtype=bool)
+        for b in blocks:
+            a = np.maximum(pads[b][0], lo) - lo
+            e = np.minimum(pads[b][1], hi) - lo + 1
+            if (e > a).all():
+                m[a[2]:e[2], a[1]:e[1], a[0]:e[0]] = True
+        return m.ravel()
+
+    needed = mask_of(mine)
     send, recv = {}, {}
-    for q in range(world):
-        if q == rank:
-            continue
-        r_ids = np.nonzero(needed[rank].ravel() & (flat_owner == q))[0]
-        s_ids = np.nonzero(needed[q].ravel() & (flat_owner == rank))[0]
+    for q in sorted(set(int(part[b]) for b in near) - {rank}):
+        r_ids = np.nonzero(needed & (owner == q))[0]
+        s_ids = np.nonzero(mask_of([b for b in near if part[b] == q]) & (owner == rank))[0]
         if len(r_ids):
-            recv[q] = to_local(r_ids).astype(np.int64)
+            recv[q] = r_ids.astype(np.int64)
         if len(s_ids):
-            send[q] = to_local(s_ids).astype(np.int64)
-    own_ids = np.nonzero(flat_owner == rank)[0]
+            send[q] = s_ids.astype(np.int64)
+    owned = np.nonzero(owner == rank)[0].astype(np.int64)
+    ox = owned % L[0] + lo[0]
+    oy = (owned // L[0]) % L[1] + lo[1]
+    oz = owned // (L[0] * L[1]) + lo[2]
     # the rank's blocks, origins shifted into the box, offsets renumbered
     blocks = (BssnBlockDesc * len(mine))()
     off = 0
@@ -137,8 +139,8 @@ def subdomain(spec: MeshSpec, part: np.ndarray, rank: int) -> Subdomain:
     origin = tuple(spec.origin3[d] + float(lo[d]) * spec.h for d in range(3))
     local = MeshSpec(blocks, len(mine), tuple(int(v) for v in L), spec.h, spec.xmin,
                      np.array([int(spec.blocks[int(b)].sz) for b in mine], dtype=np.int32), origin)
-    return Subdomain(local, tuple(int(v) for v in lo), mine, send, recv,
-                     to_local(own_ids).astype(np.int64), own_ids.astype(np.int64))
+    return Subdomain(local, tuple(int(v) for v in lo), mine, send, recv, owned,
+                     (ox + G[0] * (oy + G[1] * oz)).astype(np.int64))
 
 
 class HaloExchange:
@@ -156,7 +158,7 @@ class HaloExchange:
         gpu = device.type == "cuda"
         # gloo moves host tensors only: device buffers then go through pinned
         # host copies
-        self.via_host = gpu and dist.get_backend(group) == "gloo"
+        self.via_host = bool(self.peers) and gpu and dist.get_backend(group) == "gloo"
         self.idx = {}
         self.sbuf, self.rbuf, self.hbuf = {}, {}, {}
         for q in self.peers:
@@ -188,8 +190,8 @@ class HaloExchange:
                 send[q] = self.hbuf[("s", q)]
             for q in recv:
                 recv[q] = self.hbuf[("r", q)]
-        if gpu:
-            torch.cuda.current_stream().synchronize()
+        # NCCL orders its transfers after the packing on the current stream;
+        # the gloo path's device-to-host copies above are synchronous
         ops = []
         for q in self.peers:
             if q in send:
