@@ -36,8 +36,30 @@ class OrcParams(C.Structure):
                 ("eps_cako_other", C.c_double)]
 
 
-def params(ko_sigma=0.4, eta=2.0, cako=False):
-    return OrcParams(ko_sigma, (1, 1, 1, 1), (1.0, 0.0), eta, eta, 40.0, int(cako), 0.99, 0.3)
+def params(ko_sigma=0.4, eta=2.0, cako=False, lam=(1, 1, 1, 1), lam_f=(1.0, 0.0),
+           eta_outer=None, eta_width=40.0):
+    """The oracle's parameter block (BSSN_GR/src/parameters.h names:
+    BSSN_KO_SIGMA, BSSN_LAMBDA, BSSN_LAMBDA_F, RIT_ETA_CENTRAL / OUTER /
+    WIDTH, BSSN_CAKO_ENABLED with the epsilons 0.99 / 0.3)."""
+    outer = eta if eta_outer is None else eta_outer
+    return OrcParams(ko_sigma, tuple(lam), tuple(lam_f), eta, outer, eta_width, int(cako), 0.99, 0.3)
+
+
+# Parameter sets beyond the workloads' defaults: r-dependent eta, CAKO
+# dissipation, gauge switches (lambda) and an alpha-dependent beta driver.
+PARAM_SETS = {
+    "default": {},
+    "eta_r": dict(ko_sigma=0.1, eta=2.0, eta_outer=0.5, eta_width=3.0),
+    "cako_lambda": dict(cako=True, lam=(1, 0, 1, 0), lam_f=(1.0, 0.5)),
+}
+
+
+def device_params(name, chi_floor=1e-4):
+    """The same set as the library's BssnParams (CHI_FLOOR added)."""
+    import bssn_b200 as B
+    o = params(**PARAM_SETS[name])
+    return B.BssnParams(o.ko_sigma, tuple(o.lambda_), tuple(o.lambda_f), o.eta_central, o.eta_outer,
+                        o.eta_width, o.cako_enabled, o.eps_cako_gauge, o.eps_cako_other, chi_floor)
 
 
 def P(a):

@@ -136,6 +136,25 @@ def test_mesh_rhs_mixed_sizes(B, O):
         assert err.max() <= 1e-12, (t, err.max(), int(err.argmax()))
 
 
+@pytest.mark.parametrize("pset", ["eta_r", "cako_lambda"])
+def test_mesh_rhs_parameter_sets(B, O, pset):
+    """Split (default) and fused tiles against the oracle with r-dependent
+    eta, CAKO dissipation and other gauge parameters."""
+    spec = B.generate_mesh(1, (2, 1, 1), seed=1, xmin=-8.25)
+    mo = ol.MeshOracle(spec, O)
+    Uz = mo.unzip(mo.initial_data())
+    ref = mo.rhs(Uz, ol.params(**ol.PARAM_SETS[pset]))
+    m = B.Mesh(spec)
+    dU = dev(Uz)
+    mask = ol.interior_mask(spec)
+    for t in (-1, 0):
+        dR = torch.zeros_like(dU)
+        m.rhs(dR, dU, ol.device_params(pset), tile=t)
+        torch.cuda.synchronize()
+        err = ol.rel_err(ref[:, mask], dR.cpu().numpy()[:, mask])
+        assert err.max() <= 1e-12, (t, err.max(), int(err.argmax()))
+
+
 def test_initial_data_config1(B, O):
     spec = B.generate_mesh(0, (8, 8, 8))
     mo = ol.MeshOracle(spec, O)

@@ -74,6 +74,22 @@ def test_rhs_vs_reference_live(O, REF, side, bflag):
     assert err.max() <= 1e-12, (err.max(), int(err.argmax()))
 
 
+@pytest.mark.parametrize("pset", ["eta_r", "cako_lambda"])
+@pytest.mark.parametrize("side,bflag", [(13, 63), (19, 0)])
+def test_rhs_vs_reference_live_params(O, REF, pset, side, bflag):
+    """The restated right-hand side against the reference's generated
+    equations with r-dependent eta, CAKO and other gauge parameters."""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import make_golden as mg
+    prm = ol.params(**ol.PARAM_SETS[pset])
+    U, pmin, pmax = mg.golden_input(side, 2.0 / (side - 7), (0.1, -1.1, -0.95), 1e-8, side + bflag)
+    a = mg.interior(REF.bssnrhs(U, 0, pmin, pmax, side, bflag, prm), side)
+    b = mg.interior(O.bssnrhs(U, 0, pmin, pmax, side, bflag, prm), side)
+    err = ol.rel_err(a, b)
+    assert err.max() <= 1e-12, (err.max(), int(err.argmax()))
+
+
 def test_flat_space_rhs_is_zero(O):
     side = 13
     U = np.zeros((24, side ** 3))
