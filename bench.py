@@ -84,7 +84,7 @@ def kernel_bytes(sides, chosen, modes, n_nodes, direct):
 # dram__bytes_write.sum of one launch over that launch's algorithmic bytes),
 # from ncu captures of the 7x7x7 split tile on the uniform 512-block workload
 # (13^3 blocks); scales a full pass's algorithmic bytes to its DRAM traffic.
-TRAFFIC_RATIO = {"deriv": 0.92, "eq": 1.21}
+TRAFFIC_RATIO = {"deriv": 1.09, "eq": 1.35}
 
 
 def step_bytes(sides, n_nodes):
