@@ -17,8 +17,9 @@ int launch_enforce(double* const* u, int64_t n, double chi_floor, int* status,
 int launch_initial_data(double* const* u, const int32_t G[3], const double xmin[3],
                         double h, const double bh[6], double m1, double m2,
                         double chi_floor, double eps, uint64_t seed, cudaStream_t s);
+// small_only: the blocks smaller than kDirectMinSide only
 int launch_unzip(const MeshState* m, double* const* unz, const double* const* zip,
-                 int nvars, cudaStream_t s);
+                 int nvars, cudaStream_t s, bool small_only = false);
 int launch_zip(const MeshState* m, double* const* zip, const double* const* unz,
                int nvars, cudaStream_t s);
 // halo exchange buffers: buf[v*n + i] = u[v][idx[i]] and back

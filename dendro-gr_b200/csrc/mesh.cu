@@ -83,9 +83,10 @@ __global__ void __launch_bounds__(CHUNK) zip_kernel(MutVars zip, ConstVars unz, 
 }
 
 void make_chunks(const std::vector<BssnBlockDesc>& blocks, bool interior,
-                 std::vector<Chunk>& out) {
+                 std::vector<Chunk>& out, int max_side = 1 << 30) {
     out.clear();
     for (size_t b = 0; b < blocks.size(); b++) {
+        if (blocks[b].sz > max_side) continue;
         const int64_t s = interior ? blocks[b].sz - 6 : blocks[b].sz;
         const int64_t n = s * s * s;
         for (int64_t st = 0; st < n; st += CHUNK) {
@@ -120,14 +121,17 @@ int mesh_create(const BssnBlockDesc* blocks, int nblocks, const int32_t G[3],
         const int64_t s = blocks[b].sz;
         m->unzip_size = std::max<int64_t>(m->unzip_size, blocks[b].offset + s * s * s);
     }
-    std::vector<Chunk> pad, inner;
+    std::vector<Chunk> pad, inner, small;
     make_chunks(m->blocks, false, pad);
     make_chunks(m->blocks, true, inner);
+    make_chunks(m->blocks, false, small, kDirectMinSide - 1);
     m->n_pad_chunks = (int)pad.size();
     m->n_int_chunks = (int)inner.size();
+    m->n_pad_chunks_small = (int)small.size();
     int st = upload(m->blocks, &m->d_blocks);
     if (!st) st = upload(pad, &m->d_pad_chunks);
     if (!st) st = upload(inner, &m->d_int_chunks);
+    if (!st) st = upload(small, &m->d_pad_chunks_small);
     if (st) {
         mesh_destroy(m);
         return st;
@@ -140,6 +144,7 @@ void mesh_destroy(MeshState* m) {
     if (!m) return;
     cudaFree(m->d_blocks);
     cudaFree(m->d_pad_chunks);
+    cudaFree(m->d_pad_chunks_small);
     cudaFree(m->d_int_chunks);
     cudaFree(m->d_partial);
     cudaFree(m->d_elems);
@@ -237,16 +242,18 @@ int mesh_tasks(MeshState* m, int tile, const BrickTask** tasks, int* ntasks) {
 }
 
 int launch_unzip(const MeshState* m, double* const* unz, const double* const* zip,
-                 int nvars, cudaStream_t s) {
+                 int nvars, cudaStream_t s, bool small_only) {
     MutVars u = {};
     ConstVars z = {};
     for (int v = 0; v < nvars; v++) {
         u.p[v] = unz[v];
         z.p[v] = zip[v];
     }
-    if (m->n_pad_chunks == 0) return 0;
-    unzip_kernel<<<m->n_pad_chunks, CHUNK, 0, s>>>(u, z, nvars, m->d_blocks, m->d_pad_chunks,
-                                                   m->G[0], m->G[1], m->G[2]);
+    const int n = small_only ? m->n_pad_chunks_small : m->n_pad_chunks;
+    if (n == 0) return 0;
+    unzip_kernel<<<n, CHUNK, 0, s>>>(u, z, nvars, m->d_blocks,
+                                     small_only ? m->d_pad_chunks_small : m->d_pad_chunks,
+                                     m->G[0], m->G[1], m->G[2]);
     return cuda_status(cudaGetLastError());
 }
 

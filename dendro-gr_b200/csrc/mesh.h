@@ -13,6 +13,12 @@
 
 namespace bssn {
 
+// Blocks at least this large stage the split derivative pass straight from
+// the zipped stage state in the plan's zipped-right-hand-side form: a brick's
+// tile is a stack of short rows in a padded block of that size anyway, so
+// reading the node grid costs no more and their ghost fill is skipped.
+constexpr int kDirectMinSide = 55;
+
 // A run of consecutive points of one block handled by one CTA.
 struct Chunk {
     int32_t blk;
@@ -29,6 +35,9 @@ struct MeshState {
     Chunk* d_int_chunks = nullptr;
     int n_pad_chunks = 0;
     int n_int_chunks = 0;
+    // ghost-fill chunks of the blocks smaller than kDirectMinSide only
+    Chunk* d_pad_chunks_small = nullptr;
+    int n_pad_chunks_small = 0;
     // brick task lists per (tile shape, block side; side 0 = all blocks):
     // (device pointer, count)
     std::map<std::pair<int, int>, std::pair<BrickTask*, int>> tasks;

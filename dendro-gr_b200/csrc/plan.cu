@@ -200,14 +200,20 @@ int plan_rhs(Plan* p, cudaStream_t s, KernelTimer* tm, const double* const* src)
         }
         return 0;
     }
+    // zipped right-hand side: blocks of kDirectMinSide and more stage from
+    // the zipped stage state `src` (no ghost fill for them)
+    RhsArgs Ad = A;
+    if (zrhs && src)
+        for (int v = 0; v < NVARS; v++) Ad.u.p[v] = src[v];
     for (int side : p->sides) {
         const int t = plan_tile(p, side);
         const BrickTask* tk;
         int nt;
         int st = mesh_tasks_side(m, t, side, &tk, &nt);
+        const bool direct = zrhs && src && side >= kDirectMinSide;
         if (!st)
-            st = launch_rhs_tasks(t, A, m->d_blocks, tk, nt, s, m->d_scratch, m->scratch_zones, tm,
-                                  zrhs ? m->G : nullptr, false);
+            st = launch_rhs_tasks(t, direct ? Ad : A, m->d_blocks, tk, nt, s, m->d_scratch,
+                                  m->scratch_zones, tm, zrhs ? m->G : nullptr, direct);
         if (st) return st;
     }
     return 0;
@@ -231,8 +237,9 @@ int plan_enqueue_stage(Plan* p, double* const* u, double dt, int stage, cudaStre
     if (p->direct || plan_zipped_rhs(p)) {
         double* Rz[NVARS];
         set_ptrs(p->Rz, p->n_nodes, Rz);
-        int st = p->direct ? 0 : launch_unzip(m, Pp, src, NVARS, s);
-        if (!st) st = plan_rhs(p, s, nullptr, p->direct ? src : nullptr);
+        // ghost fill of the blocks staged from padded blocks only
+        int st = p->direct ? 0 : launch_unzip(m, Pp, src, NVARS, s, true);
+        if (!st) st = plan_rhs(p, s, nullptr, src);
         if (!st) st = launch_node_stage(stage, Ip, Ap, u, Rz, p->n_nodes, dt, enf, p->prm.chi_floor,
                                         p->status, s);
         return st;
@@ -415,7 +422,7 @@ int plan_autotune(Plan* p, double* const* u, int reps, cudaStream_t s, float* ti
 // The stage state the timing functions run the right-hand side on: the
 // padded P of the last ghost fill, or (direct) the zipped intermediate state.
 const double* const* timing_src(Plan* p, double* buf[NVARS]) {
-    if (!p->direct) return nullptr;
+    if (!p->direct && !plan_zipped_rhs(p)) return nullptr;
     set_ptrs(p->im, p->n_nodes, buf);
     return (const double* const*)buf;
 }
