@@ -197,22 +197,31 @@ eq_kernel(RhsArgs A, const BssnBlockDesc* __restrict__ blocks,
     extern __shared__ __align__(16) double ring[];  // [kRingPairs][T][2] | vals [NVARS][T]
     const int tid = threadIdx.x;
     const int task = blockIdx.x / PARTS;
-    const int l = (blockIdx.x % PARTS) * kEqThreads + tid;  // zone index in the brick
-    if (l >= Bk::NZ) return;
     const BrickTask tk = tasks[task];
-    const int r0 = l % BX, r1 = (l / BX) % BY, r2 = l / (BX * BY);
-    if (r0 >= tk.e[0] || r1 >= tk.e[1] || r2 >= tk.e[2]) return;
     const BssnBlockDesc blk = blocks[tk.blk];
     const int o[3] = {tk.o[0], tk.o[1], tk.o[2]};
-    const int rt[3] = {r0, r1, r2};
+    // the zones that run: the brick's extent, or on the zipped grid only the
+    // zones owning their node (a brick on a block's upper face loses its last
+    // layer there unless the face lies on the grid's upper boundary); the
+    // threads are packed onto them, so no lane idles on a skipped zone
+    int ex[3] = {tk.e[0], tk.e[1], tk.e[2]};
+    if (g.gx) {
+        const int n = blk.sz - 2 * PW;
+        const int gd[3] = {g.gx, g.gy, g.gz};
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+            if (o[d] + ex[d] == n && blk.g0[d] + n - 1 != gd[d] - 1) ex[d]--;
+    }
+    const int j = (blockIdx.x % PARTS) * kEqThreads + tid;  // the thread's zone among them
+    if (j >= ex[0] * ex[1] * ex[2]) return;
+    const int r0 = j % ex[0], r1 = (j / ex[0]) % ex[1], r2 = j / (ex[0] * ex[1]);
+    const int l = r0 + BX * (r1 + BY * r2);  // zone index in the brick (scratch position)
     const int za0 = o[0] + PW + r0, za1 = o[1] + PW + r1, za2 = o[2] + PW + r2;
     const int64_t pidx = blk.offset + za0 + (int64_t)blk.sz * (za1 + (int64_t)blk.sz * za2);
     int64_t node = pidx;
-    if (g.gx) {
-        if (!owns_node(blk, o, rt, g)) return;
+    if (g.gx)
         node = (blk.g0[0] + za0 - PW) +
                (int64_t)g.gx * ((blk.g0[1] + za1 - PW) + (int64_t)g.gy * (blk.g0[2] + za2 - PW));
-    }
     const int64_t in_idx = zip_in ? node : pidx;
     const double2* in = reinterpret_cast<const double2*>(S) + (int64_t)task * Bk::NZ + l;
     double2* col = reinterpret_cast<double2*>(ring) + tid;   // this thread's ring column
