@@ -121,7 +121,9 @@ TileEntry make_split_tile(int shape, int fused) {
     return TileEntry{BX, BY, BZ, Bk::THREADS, Bk::SMEM_BYTES, nullptr, 1, shape, fused};
 }
 
-// tiles 0..2: fused; 3..5: the same shapes split; 6..7: split-only shapes
+// tiles 0..2: fused; 3..5: the same shapes split; 6..9: split-only shapes
+// (13x5x5 and 9x9x5 fit the 25-zone interiors of 31^3 blocks with few idle
+// threads)
 // (rhs_split.cu's shape order).  `fused` is the tile a single-block launch
 // of the shape runs (the nearest fused shape for split-only ones).
 const TileEntry* tile_table(int* count) {
@@ -134,6 +136,8 @@ const TileEntry* tile_table(int* count) {
         make_split_tile<8, 4, 4>(2, 2),
         make_split_tile<7, 7, 7>(3, 1),
         make_split_tile<8, 8, 8>(4, 0),
+        make_split_tile<13, 5, 5>(5, 1),
+        make_split_tile<9, 9, 5>(6, 1),
     };
     *count = (int)(sizeof(table) / sizeof(table[0]));
     return table;
@@ -267,6 +271,8 @@ long tile_selfcheck(int tile) {
     if (is(8, 4, 4)) return check_tile_shape<8, 4, 4>();
     if (is(7, 7, 7)) return check_tile_shape<7, 7, 7>();
     if (is(8, 8, 8)) return check_tile_shape<8, 8, 8>();
+    if (is(13, 5, 5)) return check_tile_shape<13, 5, 5>();
+    if (is(9, 9, 5)) return check_tile_shape<9, 9, 5>();
     return -1;
 }
 

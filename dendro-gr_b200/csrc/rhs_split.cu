@@ -45,9 +45,9 @@ __host__ __device__ constexpr int slot_base(int step) {
 static_assert(slot_base(NVARS) == kSplitSlots, "scratch slot count");
 
 // resident derivative CTAs per SM the register allocation must allow: 3 for
-// bricks of up to 256 zones (80 registers), fewer for larger bricks
+// up to 384 threads (56 registers at 352), 2 for up to 512, else 1
 __host__ __device__ constexpr int deriv_min_ctas(int threads) {
-    return threads <= 384 ? 3 : 1;
+    return threads <= 384 ? 3 : threads <= 512 ? 2 : 1;
 }
 // equation pass: variables whose derivatives are in flight ahead of use, and
 // the per-thread ring of scratch slots (shared memory) they land in; one
@@ -297,6 +297,8 @@ const SplitEntry* split_table(int* count) {
         make_split<8, 4, 4>(),
         make_split<7, 7, 7>(),
         make_split<8, 8, 8>(),
+        make_split<13, 5, 5>(),
+        make_split<9, 9, 5>(),
     };
     *count = (int)(sizeof(table) / sizeof(table[0]));
     return table;
