@@ -46,6 +46,15 @@ FLOP_PER_ZONE_STAGE = 6535.0  # 6,439 RHS + 96 RK axpy (per zone, per stage)
 SPLIT_SLOTS = 162  # scratch doubles per zone of the split right-hand side
 
 
+def tile_pins(arg):
+    """--tile: {} (autotune), {0: t} (tile t on every bucket) or {side: tile}."""
+    if not arg:
+        return {}
+    if ":" not in arg:
+        return {0: int(arg)}
+    return {int(a): int(b) for a, b in (kv.split(":") for kv in arg.split(","))}
+
+
 def kernel_bytes(sides, chosen, modes, n_nodes, direct):
     """Algorithmic HBM bytes of one right-hand-side pass per kernel kind, as
     the plan's timing call runs it.
@@ -293,11 +302,15 @@ def run_partitioned(args, wl, B, torch, dist, world, rank, local, barrier, max_o
     zones = spec.zones()
     prm = B.default_params()
     dt = 0.25 * spec.h
-    pr = PartitionedRK4(spec, rank, world, prm, tile=args.tile if args.tile >= 0 else None)
+    pr = PartitionedRK4(spec, rank, world, prm)
+    pins = tile_pins(args.tile)
     sub = pr.sub
     U = torch.zeros((24, sub.n_nodes), dtype=torch.float64, device="cuda")
     B.initial_data(U, sub.spec)  # nodes of other ranks are replaced by the first exchange
-    if args.tile < 0:
+    if pins:
+        for side, t in pins.items():
+            pr.plan.set_tile(t, side)
+    else:
         pr.plan.autotune(U, reps=2)
     for _ in range(args.warmup):
         pr.step(U, dt)
@@ -371,8 +384,9 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--tile", type=int, default=-1,
-                    help="pin this tile on every bucket instead of autotuning (profiling runs)")
+    ap.add_argument("--tile", default="",
+                    help="pin tiles instead of autotuning (profiling runs): one tile id for every "
+                         "bucket, or side:tile pairs such as 13:6,19:6,31:8,55:6")
     ap.add_argument("--partition", action="store_true",
                     help="multi-GPU form: one mesh N times larger, partitioned along the Z-order "
                          "of its blocks, halo exchange before every RK4 stage (mixed workloads)")
@@ -425,8 +439,11 @@ def main():
 
     # ---- batched, graph-captured plan
     plan = B.RK4Plan(mesh, prm, B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
-    if args.tile >= 0:
-        chosen, table = plan.set_tile(args.tile), {}
+    pins = tile_pins(args.tile)
+    if pins:
+        for side, t in pins.items():
+            chosen = plan.set_tile(t, side)
+        table = {}
     else:
         chosen, table = plan.autotune(U, reps=2)
     for _ in range(args.warmup):
