@@ -72,6 +72,8 @@ def _sig():
                                        P(BssnBlockDesc), P(i), P(C.c_int32), P(d)]
     lib.bssn_rk4_plan_create.argtypes = [vp, P(BssnParams), i, P(vp)]
     lib.bssn_rk4_plan_step.argtypes = [vp, vp, d, vp]
+    lib.bssn_rk4_plan_diagnostics.argtypes = [vp, vp, P(d), d, P(d), P(d), vp, vp]
+    lib.bssn_rk4_plan_step_diag.argtypes = [vp, vp, d, P(d), d, P(d), P(d), vp, vp]
     lib.bssn_rk4_plan_autotune.argtypes = [vp, vp, i, vp, P(C.c_float)]
     lib.bssn_rk4_plan_tile.argtypes = [vp, i]
     lib.bssn_rk4_plan_set_tile.argtypes = [vp, i, i]
@@ -323,6 +325,27 @@ class RK4Plan:
 
     def step(self, U, dt, stream=None):
         check(lib.bssn_rk4_plan_step(self.h, ptrs(U), dt, stream_ptr(stream)), "rk4_plan_step")
+
+    def _diag_args(self, norms, bh, radii):
+        spec = self.mesh.spec
+        assert norms.is_cuda and norms.dtype.is_floating_point and norms.numel() >= 4
+        return ((C.c_double * 3)(*spec.origin3), spec.h, (C.c_double * 6)(*bh),
+                (C.c_double * 2)(*radii), C.c_void_p(norms.data_ptr()))
+
+    def diagnostics(self, U, norms, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0), radii=(0.5, 0.5), stream=None):
+        """Masked L2 norms of ham, mom0..2 of the state U into the CUDA
+        tensor `norms` (4 doubles), on the device."""
+        xm, h, b, r, nd = self._diag_args(norms, bh, radii)
+        check(lib.bssn_rk4_plan_diagnostics(self.h, ptrs(U), xm, h, b, r, nd, stream_ptr(stream)),
+              "rk4_plan_diagnostics")
+
+    def step_diag(self, U, dt, norms, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0), radii=(0.5, 0.5),
+                  stream=None):
+        """One step, then the constraint norms of the new state into `norms`
+        (one graph with PLAN_GRAPH)."""
+        xm, h, b, r, nd = self._diag_args(norms, bh, radii)
+        check(lib.bssn_rk4_plan_step_diag(self.h, ptrs(U), dt, xm, h, b, r, nd, stream_ptr(stream)),
+              "rk4_plan_step_diag")
 
     def autotune(self, U, reps=3, stream=None):
         sides = sorted(set(self.mesh.spec.sides.tolist()))

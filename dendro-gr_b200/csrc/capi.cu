@@ -1,6 +1,7 @@
 // The extern "C" entry points of include/bssn_b200.h: argument checks and
 // kernel launches.  No entry point allocates device memory except the mesh
-// handle's creation and its first use of a tile shape (task list upload).
+// handle's creation and its first use of a tile shape (task list upload),
+// plan creation, and the first diagnostics call of a plan.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -185,6 +186,42 @@ int bssn_rk4_plan_step(bssn_rk4_plan plan, double* const* u_dev, double dt,
     for (int v = 0; v < bssn::NVARS; v++)
         if (!u_dev[v]) return BSSN_EINVAL;
     return bssn::plan_step(plan->p, u_dev, dt, S(stream));
+}
+
+namespace {
+int diag_args(const double xmin[3], double h, const double bh[6], const double radii[2],
+              double* norms_dev, bssn::DiagArgs* d) {
+    if (!xmin || !bh || !radii || !norms_dev || !(h > 0.0)) return BSSN_EINVAL;
+    for (int i = 0; i < 3; i++) d->xmin[i] = xmin[i];
+    for (int i = 0; i < 6; i++) d->bh[i] = bh[i];
+    d->radii[0] = radii[0];
+    d->radii[1] = radii[1];
+    d->h = h;
+    d->norms = norms_dev;
+    return BSSN_OK;
+}
+}  // namespace
+
+int bssn_rk4_plan_diagnostics(bssn_rk4_plan plan, double* const* u_dev, const double xmin[3],
+                              double h, const double bh[6], const double radii[2],
+                              double* norms_dev, bssn_stream_t stream) {
+    if (!plan || !u_dev) return BSSN_EINVAL;
+    for (int v = 0; v < bssn::NVARS; v++)
+        if (!u_dev[v]) return BSSN_EINVAL;
+    bssn::DiagArgs d;
+    const int st = diag_args(xmin, h, bh, radii, norms_dev, &d);
+    return st ? st : bssn::plan_diag(plan->p, u_dev, d, S(stream));
+}
+
+int bssn_rk4_plan_step_diag(bssn_rk4_plan plan, double* const* u_dev, double dt,
+                            const double xmin[3], double h, const double bh[6],
+                            const double radii[2], double* norms_dev, bssn_stream_t stream) {
+    if (!plan || !u_dev) return BSSN_EINVAL;
+    for (int v = 0; v < bssn::NVARS; v++)
+        if (!u_dev[v]) return BSSN_EINVAL;
+    bssn::DiagArgs d;
+    const int st = diag_args(xmin, h, bh, radii, norms_dev, &d);
+    return st ? st : bssn::plan_step_diag(plan->p, u_dev, dt, d, S(stream));
 }
 
 int bssn_rk4_plan_autotune(bssn_rk4_plan plan, double* const* u_dev, int reps,

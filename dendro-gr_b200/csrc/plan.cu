@@ -14,6 +14,7 @@
 
 #include "bssn_b200.h"
 #include "bssn_common.cuh"
+#include "constraints.h"
 #include "kernels.cuh"
 #include "mesh.h"
 #include "plan.h"
@@ -105,11 +106,21 @@ int plan_create(MeshState* m, const BssnParams& prm, int flags, Plan** out) {
     return 0;
 }
 
-void plan_destroy(Plan* p) {
-    if (!p) return;
+// Releases the captured graphs (the next step captures them again).
+static void drop_graphs(Plan* p) {
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->exec_diag) cudaGraphExecDestroy(p->exec_diag);
+    if (p->graph_diag) cudaGraphDestroy(p->graph_diag);
+    p->exec = p->exec_diag = nullptr;
+    p->graph = p->graph_diag = nullptr;
+}
+
+void plan_destroy(Plan* p) {
+    if (!p) return;
+    drop_graphs(p);
     if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
+    cudaFree(p->cons);
     cudaFree(p->Rz);
     cudaFree(p->P);
     cudaFree(p->R);
@@ -139,12 +150,7 @@ int plan_set_tile(Plan* p, int side, int tile) {
     } else {
         p->mesh->tuned[side] = tile;
     }
-    if (p->exec) {  // recapture with the new tile on the next step
-        cudaGraphExecDestroy(p->exec);
-        cudaGraphDestroy(p->graph);
-        p->exec = nullptr;
-        p->graph = nullptr;
-    }
+    drop_graphs(p);  // recapture with the new tile on the next step
     return 0;
 }
 
@@ -258,46 +264,115 @@ int plan_enqueue(Plan* p, double* const* u, double dt, cudaStream_t s) {
     return 0;
 }
 
+// Captures body(stream) into *graph / *exec on the plan's own capture
+// stream (the caller's stream may be the legacy default stream, which cannot
+// be captured; the graph is then launched onto the caller's stream, which
+// orders it after prior work).
+template <class F>
+static int capture(Plan* p, cudaGraph_t* graph, cudaGraphExec_t* exec, F body) {
+    if (*exec) cudaGraphExecDestroy(*exec);
+    if (*graph) cudaGraphDestroy(*graph);
+    *exec = nullptr;
+    *graph = nullptr;
+    if (!p->cap_stream && cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return BSSN_ENOMEM;
+    }
+    cudaError_t e = cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaGetLastError();  // do not leave the failure for a later launch check
+        return cuda_status(e);
+    }
+    int st = body(p->cap_stream);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(p->cap_stream, &g);
+    if (st || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return st ? st : cuda_status(e);
+    }
+    *graph = g;
+    e = cudaGraphInstantiate(exec, g, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_status(e);
+    }
+    return 0;
+}
+
 int plan_step(Plan* p, double* const* u, double dt, cudaStream_t s) {
     if (!(p->flags & BSSN_PLAN_GRAPH)) return plan_enqueue(p, u, dt, s);
     bool same = p->exec && p->graph_dt == dt;
     for (int v = 0; v < NVARS && same; v++) same = p->graph_u[v] == u[v];
     if (!same) {
-        if (p->exec) cudaGraphExecDestroy(p->exec);
-        if (p->graph) cudaGraphDestroy(p->graph);
-        p->exec = nullptr;
-        p->graph = nullptr;
-        // capture on the plan's own stream: the caller's stream may be the
-        // legacy default stream, which cannot be captured; the graph is then
-        // launched onto the caller's stream, which orders it after prior work
-        if (!p->cap_stream &&
-            cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
-            cudaGetLastError();
-            return BSSN_ENOMEM;
-        }
-        cudaError_t e = cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) {
-            cudaGetLastError();  // do not leave the failure for a later launch check
-            return cuda_status(e);
-        }
-        int st = plan_enqueue(p, u, dt, p->cap_stream);
-        cudaGraph_t g = nullptr;
-        e = cudaStreamEndCapture(p->cap_stream, &g);
-        if (st || e != cudaSuccess) {
-            if (g) cudaGraphDestroy(g);
-            cudaGetLastError();
-            return st ? st : cuda_status(e);
-        }
-        p->graph = g;
-        e = cudaGraphInstantiate(&p->exec, g, 0);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            return cuda_status(e);
-        }
+        int st = capture(p, &p->graph, &p->exec, [&](cudaStream_t cs) { return plan_enqueue(p, u, dt, cs); });
+        if (st) return st;
         for (int v = 0; v < NVARS; v++) p->graph_u[v] = u[v];
         p->graph_dt = dt;
     }
     return cuda_status(cudaGraphLaunch(p->exec, s));
+}
+
+// Constraint diagnostics of the zipped state u: ghost fill of every block
+// into the padded stage array, Hamiltonian and momentum constraints into the
+// plan's zipped constraint arrays, their masked L2 norms into d.norms.  The
+// reference's time loop computes the same norms every BSSN_IO_OUTPUT_FREQ
+// steps (BSSN_GR/src/bssnCtx.cpp:597-685, computeConstraintL2Norm).
+static int diag_prepare(Plan* p) {
+    if (p->direct || !p->P) return BSSN_ESTATE;  // needs the padded stage array
+    MeshState* m = p->mesh;
+    if (!p->cons && alloc(&p->cons, (size_t)4 * p->n_nodes)) return BSSN_ENOMEM;
+    if (!m->d_partial &&
+        cudaMalloc((void**)&m->d_partial, sizeof(double) * 5 * kNormPartials) != cudaSuccess) {
+        cudaGetLastError();
+        return BSSN_ENOMEM;
+    }
+    return 0;
+}
+
+static int enqueue_diag(Plan* p, double* const* u, const DiagArgs& d, cudaStream_t s) {
+    MeshState* m = p->mesh;
+    double* Pp[NVARS];
+    set_ptrs(p->P, m->unzip_size, Pp);
+    int st = launch_unzip(m, Pp, (const double* const*)u, NVARS, s);
+    if (st) return st;
+    double* cons[4];
+    for (int c = 0; c < 4; c++) cons[c] = p->cons + (size_t)c * p->n_nodes;
+    st = launch_constraints(m, (const double* const*)Pp, cons, s);
+    if (st) return st;
+    return launch_l2_norms(m, (const double* const*)cons, 4, d.xmin, d.h, d.bh, d.radii, m->d_partial,
+                           kNormPartials, d.norms, s);
+}
+
+int plan_diag(Plan* p, double* const* u, const DiagArgs& d, cudaStream_t s) {
+    const int st = diag_prepare(p);
+    return st ? st : enqueue_diag(p, u, d, s);
+}
+
+// One RK4 step followed by the diagnostics of the new state, captured as one
+// graph (a second one beside the plain step's) when the plan has
+// BSSN_PLAN_GRAPH, so a time loop that reports the norms every k steps
+// replays graphs only and never synchronises with the host.
+int plan_step_diag(Plan* p, double* const* u, double dt, const DiagArgs& d, cudaStream_t s) {
+    int st = diag_prepare(p);
+    if (st) return st;
+    auto body = [&](cudaStream_t cs) {
+        int r = plan_enqueue(p, u, dt, cs);
+        return r ? r : enqueue_diag(p, u, d, cs);
+    };
+    if (!(p->flags & BSSN_PLAN_GRAPH)) return body(s);
+    double key[14] = {dt, d.xmin[0], d.xmin[1], d.xmin[2], d.h, d.bh[0], d.bh[1], d.bh[2],
+                      d.bh[3], d.bh[4], d.bh[5], d.radii[0], d.radii[1], 0.0};
+    std::memcpy(&key[13], &d.norms, sizeof(double*));
+    bool same = p->exec_diag && std::memcmp(key, p->diag_key, sizeof key) == 0;
+    for (int v = 0; v < NVARS && same; v++) same = p->diag_u[v] == u[v];
+    if (!same) {
+        st = capture(p, &p->graph_diag, &p->exec_diag, body);
+        if (st) return st;
+        for (int v = 0; v < NVARS; v++) p->diag_u[v] = u[v];
+        std::memcpy(p->diag_key, key, sizeof key);
+    }
+    return cuda_status(cudaGraphLaunch(p->exec_diag, s));
 }
 
 // Project-written autotuner: for every block-size bucket of the mesh, time
@@ -366,12 +441,7 @@ int plan_autotune(Plan* p, double* const* u, int reps, cudaStream_t s, float* ti
                 for (int t = 0; t < nt; t++) times_out[i * nt + t] = tt[t];
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        if (p->exec) {  // tile choice changed: recapture on the next step
-            cudaGraphExecDestroy(p->exec);
-            cudaGraphDestroy(p->graph);
-            p->exec = nullptr;
-            p->graph = nullptr;
-        }
+        drop_graphs(p);  // tile choice changed: recapture on the next step
         return st;
     }
     int idx = 0;
@@ -407,12 +477,7 @@ int plan_autotune(Plan* p, double* const* u, int reps, cudaStream_t s, float* ti
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (p->exec) {  // tile choice changed: recapture on the next step
-        cudaGraphExecDestroy(p->exec);
-        cudaGraphDestroy(p->graph);
-        p->exec = nullptr;
-        p->graph = nullptr;
-    }
+    drop_graphs(p);  // tile choice changed: recapture on the next step
     return st;
 }
 

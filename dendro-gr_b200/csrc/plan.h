@@ -31,6 +31,24 @@ struct Plan {
     cudaStream_t cap_stream = nullptr;  // capture stream of the graph
     double* graph_u[NVARS] = {nullptr};
     double graph_dt = 0.0;
+    // constraint diagnostics: zipped ham, mom0..2 (allocated on first use)
+    // and the graph of one step followed by the diagnostics
+    double* cons = nullptr;
+    cudaGraph_t graph_diag = nullptr;
+    cudaGraphExec_t exec_diag = nullptr;
+    double* diag_u[NVARS] = {nullptr};
+    double diag_key[14] = {0};  // dt, xmin[3], h, bh[6], radii[2], norms pointer
+};
+
+// Where the diagnostics go: masked L2 norms of ham, mom0..2 over the nodes
+// farther than radii from the punctures bh (node coordinates xmin + g*h),
+// written to norms (4 doubles, device).
+struct DiagArgs {
+    double xmin[3];
+    double h;
+    double bh[6];
+    double radii[2];
+    double* norms;
 };
 
 int plan_create(MeshState* m, const BssnParams& prm, int flags, Plan** out);
@@ -43,6 +61,8 @@ int plan_set_tile(Plan* p, int side, int tile);
 int plan_time_rhs(Plan* p, int reps, cudaStream_t s, float* ms);
 int plan_time_kernels(Plan* p, int reps, cudaStream_t s, double out[6]);
 int plan_launches_per_step(Plan* p);
+int plan_diag(Plan* p, double* const* u, const DiagArgs& d, cudaStream_t s);
+int plan_step_diag(Plan* p, double* const* u, double dt, const DiagArgs& d, cudaStream_t s);
 int fp64_probe(double* scratch, int iters, cudaStream_t s, double* tflops);
 
 }  // namespace bssn

@@ -293,6 +293,26 @@ int bssn_rk4_plan_create(bssn_mesh mesh, const BssnParams* params, int flags,
                          bssn_rk4_plan* out);
 int bssn_rk4_plan_step(bssn_rk4_plan plan, double* const* u_dev, double dt,
                        bssn_stream_t stream);
+/* Constraint diagnostics of the zipped state u_dev: ghost fill of every
+ * block, Hamiltonian and momentum constraints (as bssn_constraints_f64) into
+ * plan-owned zipped arrays (4 x nodes, allocated on the first call), and
+ * their masked L2 norms (as bssn_constraint_norms_f64) into norms_dev[0..3]
+ * on the device -- the norms the reference's time loop computes every
+ * BSSN_IO_OUTPUT_FREQ steps (BSSN_GR/src/bssnCtx.cpp:597-685).  Uses the
+ * plan's padded stage array: BSSN_ESTATE for direct plans. */
+int bssn_rk4_plan_diagnostics(bssn_rk4_plan plan, double* const* u_dev,
+                              const double xmin[3], double h, const double bh[6],
+                              const double radii[2], double* norms_dev,
+                              bssn_stream_t stream);
+/* One bssn_rk4_plan_step followed by bssn_rk4_plan_diagnostics of the new
+ * state; with BSSN_PLAN_GRAPH both are captured as one graph (kept beside
+ * the plain step's graph and replayed while u_dev, dt and the diagnostic
+ * arguments are unchanged), so a loop that reports the norms every k steps
+ * never synchronises with the host. */
+int bssn_rk4_plan_step_diag(bssn_rk4_plan plan, double* const* u_dev, double dt,
+                            const double xmin[3], double h, const double bh[6],
+                            const double radii[2], double* norms_dev,
+                            bssn_stream_t stream);
 /* Autotuner: times every tile the plan can run (direct plans: split tiles
  * only) on every block-size bucket of the mesh with the state u_dev (best of
  * reps) and keeps the fastest per bucket in the mesh handle.  Blocking.
@@ -390,6 +410,65 @@ int bssn_tile_mode(int tile);
  * extent, face case and thread: the number of out-of-range reads (0 when
  * every access is in bounds), or -1 for an unknown tile. */
 long bssn_tile_selfcheck(int tile);
+
+/* ---------------------------------------------------------------------- */
+/* Checkpoint and restart: BSSNCtx::write_checkpt / restore_checkpt
+ * (BSSN_GR/src/bssnCtx.cpp:783-862, 864-1170).  Files, as the reference
+ * names them:
+ *   <prefix>_step_<i>.cp          JSON header, the reference's keys (rank 0)
+ *   <prefix>_octree_<i>_<r>.oct   rank r's mesh: grid dims, spacing, origin
+ *                                 and block list (this library's own binary
+ *                                 layout; the reference stores dendrolib
+ *                                 octants)
+ *   <prefix>_<i>_<r>.var          rank r's 24 zipped variables (binary)
+ * Binary files carry a magic word and a checksum; a file that fails either
+ * reads as BSSN_EIO.  Slot i alternates as the reference's does (see
+ * bssn_checkpoint_index); restart takes the slot of 0 and 1 with the larger
+ * step. */
+#define BSSN_EIO 7          /* checkpoint file unreadable or corrupted */
+#define BSSN_ENOENT 8       /* no checkpoint file found */
+
+typedef struct BssnCheckpointInfo {
+    double time_begin;      /* DENDRO_TS_TIME_BEGIN */
+    double time_end;        /* DENDRO_TS_TIME_END */
+    double time_current;    /* DENDRO_TS_TIME_CURRENT (and _LAST_IO_TIME) */
+    double time_step;       /* DENDRO_TS_TIME_STEP_SIZE */
+    int64_t step;           /* DENDRO_TS_STEP_CURRENT */
+    int32_t element_order;  /* DENDRO_TS_ELEMENT_ORDER (6) */
+    int32_t num_vars;       /* DENDRO_TS_NUM_VARS (24) */
+    int32_t active_comm_size; /* DENDRO_TS_ACTIVE_COMM_SZ */
+    int32_t reserved;
+    double wavelet_tol;     /* DENDRO_TS_WAVELET_TOLERANCE */
+    double load_imb_tol;    /* DENDRO_TS_LOAD_IMB_TOLERANCE */
+    double bh[2][3];        /* DENDRO_BH1_X .. DENDRO_BH2_Z */
+} BssnCheckpointInfo;
+
+/* The slot a checkpoint at `step` goes to: 0 when step % (2*freq) == 0,
+ * else 1; 3 for the first checkpoint after the punctures merged (merged
+ * nonzero and *merged_written zero; sets *merged_written).  bssnCtx.cpp:786-796. */
+int bssn_checkpoint_index(int64_t step, int freq, int merged, int* merged_written);
+/* Writes rank `rank`'s .oct and .var files of slot `index` (the 24 arrays of
+ * n_nodes doubles at u_dev, device or host memory, copied through a pinned
+ * buffer on `stream`), and the .cp header when write_header is nonzero. */
+int bssn_checkpoint_write(const char* prefix, int index, int rank, int write_header,
+                          const BssnCheckpointInfo* info, const BssnBlockDesc* blocks,
+                          int nblocks, const int32_t G[3], double h, const double origin[3],
+                          const double* const* u_dev, int64_t n_nodes,
+                          bssn_stream_t stream);
+/* Reads the .cp headers of slots 0 and 1 and returns the one with the larger
+ * step (slot 0 on a tie) in *index and *info.  BSSN_ENOENT when neither
+ * exists, BSSN_EIO when the chosen one does not parse. */
+int bssn_checkpoint_latest(const char* prefix, int* index, BssnCheckpointInfo* info);
+/* Rank r's mesh of slot `index`.  Call with blocks == NULL to get *nblocks;
+ * then with room for *nblocks descriptors. */
+int bssn_checkpoint_read_mesh(const char* prefix, int index, int rank,
+                              BssnBlockDesc* blocks, int* nblocks, int32_t G[3],
+                              double* h, double origin[3]);
+/* Rank r's 24 zipped variables of slot `index` into u_dev (device or host
+ * memory, n_nodes doubles each; n_nodes must match the file). */
+int bssn_checkpoint_read_vars(const char* prefix, int index, int rank,
+                              double* const* u_dev, int64_t n_nodes,
+                              bssn_stream_t stream);
 
 const char* bssn_version(void);
 

@@ -47,3 +47,35 @@ def test_constraint_norm_history_100_steps():
         rel = np.abs(got[h["step"]] - ref) / np.abs(ref)
         worst = max(worst, rel.max())
     assert worst <= 1e-10, worst
+
+
+def test_constraint_norm_history_in_graph():
+    """The same history through the plan's graph-captured step + diagnostics
+    (bssn_rk4_plan_step_diag every 10th step, norms copied on the device into
+    a history tensor): one host synchronisation at the end, same norms."""
+    import bssn_b200 as B
+    with open(os.path.join(HERE, "golden", "constraint_history.json")) as f:
+        gold = json.load(f)
+    spec = B.generate_mesh(0, (8, 8, 8))
+    m = B.Mesh(spec)
+    U = torch.zeros((24, spec.n_nodes), dtype=torch.float64, device="cuda")
+    B.initial_data(U, spec)
+    dt = 0.25 * spec.h
+    plan = B.RK4Plan(m, B.default_params(), B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
+    norms = torch.zeros(4, dtype=torch.float64, device="cuda")
+    hist = torch.zeros((11, 4), dtype=torch.float64, device="cuda")
+    plan.diagnostics(U, norms)
+    hist[0].copy_(norms)
+    for step in range(1, 101):
+        if step % 10 == 0:
+            plan.step_diag(U, dt, norms)
+            hist[step // 10].copy_(norms)
+        else:
+            plan.step(U, dt)
+    got = hist.cpu().numpy()
+    assert plan.violations() == gold["enforce_violations"]
+    worst = 0.0
+    for h in gold["history"]:
+        ref = np.array([float.fromhex(x) for x in h["norms"]])
+        worst = max(worst, (np.abs(got[h["step"] // 10] - ref) / np.abs(ref)).max())
+    assert worst <= 1e-10, worst
