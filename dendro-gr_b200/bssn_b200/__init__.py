@@ -195,8 +195,12 @@ class Mesh:
     def __init__(self, spec: MeshSpec):
         self.spec = spec
         self.h = C.c_void_p()
-        G = (C.c_int32 * 3)(*spec.G)
-        check(lib.bssn_mesh_create(spec.blocks, spec.nblocks, G, C.byref(self.h)), "mesh_create")
+        if getattr(spec, "boxes", None):  # multi-level mesh (levels.py)
+            from .levels import create_mesh_handle
+            self.h = create_mesh_handle(spec)
+        else:
+            G = (C.c_int32 * 3)(*spec.G)
+            check(lib.bssn_mesh_create(spec.blocks, spec.nblocks, G, C.byref(self.h)), "mesh_create")
         self.n_unzip = lib.bssn_mesh_unzip_size(self.h)
 
     def close(self):

@@ -130,13 +130,46 @@ int bssn_rhs_blocks_f64(bssn_mesh mesh, double* const* rhs_dev, const double* co
 int bssn_unzip_f64(bssn_mesh mesh, double* const* unzip_dev, const double* const* zip_dev,
                    int nvars, bssn_stream_t stream) {
     if (!mesh || !unzip_dev || !zip_dev || nvars < 1 || nvars > bssn::NVARS) return BSSN_EINVAL;
+    if (mesh->st->lv) return bssn::launch_levels_unzip(*mesh->st->lv, unzip_dev, zip_dev, nvars, S(stream));
     return bssn::launch_unzip(mesh->st, unzip_dev, zip_dev, nvars, S(stream));
 }
 
 int bssn_zip_f64(bssn_mesh mesh, double* const* zip_dev, const double* const* unzip_dev,
                  int nvars, bssn_stream_t stream) {
     if (!mesh || !unzip_dev || !zip_dev || nvars < 1 || nvars > bssn::NVARS) return BSSN_EINVAL;
+    if (mesh->st->lv) return bssn::launch_levels_zip(*mesh->st->lv, zip_dev, unzip_dev, nvars, S(stream));
     return bssn::launch_zip(mesh->st, zip_dev, unzip_dev, nvars, S(stream));
+}
+
+int bssn_mesh_create_levels(const BssnBlockDesc* blocks, int nblocks, int nlevels, const int32_t M0[3],
+                            const BssnLevelBox* boxes, bssn_mesh* out) {
+    if (!blocks || nblocks <= 0 || !out) return BSSN_EINVAL;
+    for (int b = 0; b < nblocks; b++)
+        if (!valid_side(blocks[b].sz) || blocks[b].offset < 0) return BSSN_EBLOCKSIZE;
+    bssn::LevelMaps maps;
+    int r = bssn::levels_build(blocks, nblocks, nlevels, M0, boxes, &maps);
+    if (r) return r;
+    // the node "grid" of a multi-level mesh is its concatenated level grids
+    const int32_t G[3] = {(int32_t)maps.n_nodes, 1, 1};
+    bssn::MeshState* st = nullptr;
+    r = bssn::mesh_create(blocks, nblocks, G, &st);
+    if (r) return r;
+    st->lv = new bssn::LevelsDev();
+    r = bssn::levels_upload(maps, st->lv);
+    if (r) {
+        bssn::mesh_destroy(st);
+        return r;
+    }
+    *out = new bssn_mesh_s{st};
+    return 0;
+}
+
+int bssn_mesh_levels_sync(bssn_mesh mesh, double* const* u_dev, int nvars, bssn_stream_t stream) {
+    if (!mesh || !u_dev || nvars < 1 || nvars > bssn::NVARS) return BSSN_EINVAL;
+    for (int v = 0; v < nvars; v++)
+        if (!u_dev[v]) return BSSN_EINVAL;
+    if (!mesh->st->lv) return 0;  // single-level meshes have nothing to sync
+    return bssn::launch_levels_sync(*mesh->st->lv, u_dev, nvars, S(stream));
 }
 
 int bssn_rk4_stage_f64(int stage, double* const* out_dev, const double* const* u_prev_dev,
@@ -275,6 +308,7 @@ int bssn_rk4_plan_destroy(bssn_rk4_plan plan) {
 int bssn_constraints_f64(bssn_mesh mesh, const double* const* unzip_dev, double* const* cons_dev,
                          bssn_stream_t stream) {
     if (!mesh || !unzip_dev || !cons_dev) return BSSN_EINVAL;
+    if (mesh->st->lv) return BSSN_ESTATE;  // single-level node grids only
     for (int c = 0; c < 4; c++)
         if (!cons_dev[c]) return BSSN_EINVAL;
     for (int v = 0; v < bssn::NVARS; v++)
@@ -287,6 +321,7 @@ int bssn_constraint_norms_f64(bssn_mesh mesh, const double* const* cons_dev, int
                               const double radii[2], double* norms_dev, bssn_stream_t stream) {
     if (!mesh || !cons_dev || ncons < 1 || ncons > 4 || !xmin || !bh || !radii || !norms_dev)
         return BSSN_EINVAL;
+    if (mesh->st->lv) return BSSN_ESTATE;
     for (int c = 0; c < ncons; c++)
         if (!cons_dev[c]) return BSSN_EINVAL;
     // the reduction's partial sums live in a device buffer owned by the mesh

@@ -1,0 +1,610 @@
+// Multi-level meshes: generator, host-side maps and their kernels (see
+// levels.h and the BssnLevelBox notes in include/bssn_b200.h).
+//
+// The reference gets its level transitions from dendrolib's ot::Mesh (block
+// construction and unzip with parent-to-child interpolation; absent from the
+// reference tree, called at BSSN_GR/src/rkBSSN.cpp:611-650).  This file is
+// this library's definition of them: dendrolib interpolates a child from its
+// parent element's nodal values with the element's Lagrange polynomials of
+// the element order (6, seven nodes per edge), which is the interpolation
+// used here, applied axis by axis.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <utility>
+#include <vector>
+
+#include "bssn_common.cuh"
+#include "levels.h"
+
+namespace bssn {
+
+namespace {
+
+constexpr int OCT = 6;  // node intervals per octant edge
+
+// Degree-6 Lagrange weights on nodes 0..6 at x = j + 1/2, j = 0..5:
+// w_m = prod_{k != m} (2j + 1 - 2k) / (2 (m - k)), formed as an exact
+// integer ratio and rounded once.
+void lagrange_half(double w[6][7]) {
+    for (int j = 0; j < 6; j++)
+        for (int m = 0; m < 7; m++) {
+            long long num = 1, den = 1;
+            for (int k = 0; k < 7; k++) {
+                if (k == m) continue;
+                num *= (2 * j + 1 - 2 * k);
+                den *= 2 * (m - k);
+            }
+            w[j][m] = (double)num / (double)den;
+        }
+}
+
+struct Box {
+    int32_t lo[3], n[3];
+    bool contains_cell(const int32_t o[3], int w) const {  // cell [o, o+w) inside
+        for (int d = 0; d < 3; d++)
+            if (o[d] < lo[d] || o[d] + w > lo[d] + n[d]) return false;
+        return true;
+    }
+    bool disjoint_cell(const int32_t o[3], int w) const {
+        for (int d = 0; d < 3; d++)
+            if (o[d] >= lo[d] + n[d] || o[d] + w <= lo[d]) return true;
+        return false;
+    }
+};
+
+int check_boxes(int nlevels, const int32_t M0[3], const BssnLevelBox* boxes) {
+    if (nlevels < 1 || nlevels > 16 || !M0 || !boxes) return BSSN_EINVAL;
+    for (int d = 0; d < 3; d++)
+        if (M0[d] < 1 || boxes[0].lo[d] != 0 || boxes[0].n[d] != M0[d]) return BSSN_EINVAL;
+    for (int l = 1; l < nlevels; l++)
+        for (int d = 0; d < 3; d++) {
+            const int lo = boxes[l].lo[d], n = boxes[l].n[d];
+            if (n < 2 || (lo & 1) || (n & 1)) return BSSN_EINVAL;
+            // inside level l-1's box with one level-(l-1) octant of margin
+            if (lo / 2 < boxes[l - 1].lo[d] + 1 ||
+                lo / 2 + n / 2 > boxes[l - 1].lo[d] + boxes[l - 1].n[d] - 1)
+                return BSSN_EINVAL;
+        }
+    return 0;
+}
+
+// The next finer level's box in level-l octants (n = 0: none).
+Box child_box(int nlevels, const BssnLevelBox* boxes, int l) {
+    Box c{{0, 0, 0}, {0, 0, 0}};
+    if (l + 1 < nlevels)
+        for (int d = 0; d < 3; d++) {
+            c.lo[d] = boxes[l + 1].lo[d] / 2;
+            c.n[d] = boxes[l + 1].n[d] / 2;
+        }
+    return c;
+}
+
+struct Tiler {
+    Box box, child;
+    bool has_child;
+    std::vector<std::pair<std::array<int32_t, 3>, int>> cells;  // (origin, width)
+    void tile(const int32_t o[3], int w) {
+        if (box.disjoint_cell(o, w)) return;
+        if (has_child && child.contains_cell(o, w)) return;
+        if (box.contains_cell(o, w) && (!has_child || child.disjoint_cell(o, w))) {
+            cells.push_back({{o[0], o[1], o[2]}, w});
+            return;
+        }
+        const int h = w / 2;  // w > 1 here: unit cells are resolved above
+        for (int c = 0; c < 8; c++) {
+            const int32_t oc[3] = {o[0] + (c & 1) * h, o[1] + ((c >> 1) & 1) * h, o[2] + ((c >> 2) & 1) * h};
+            tile(oc, h);
+        }
+    }
+};
+
+}  // namespace
+
+int levels_generate(int nlevels, const int32_t M0[3], const BssnLevelBox* boxes, double xmin,
+                    double h0, BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes) {
+    if (!nblocks || !n_nodes || !(h0 > 0.0)) return BSSN_EINVAL;
+    int st = check_boxes(nlevels, M0, boxes);
+    if (st) return st;
+    int64_t nodes = 0;
+    for (int l = 0; l < nlevels; l++)
+        nodes += int64_t(OCT * boxes[l].n[0] + 1) * (OCT * boxes[l].n[1] + 1) * (OCT * boxes[l].n[2] + 1);
+    if (nodes >= (int64_t(1) << 31)) return BSSN_ELIMIT;
+    int count = 0;
+    int64_t offset = 0;
+    for (int l = 0; l < nlevels; l++) {
+        Tiler t;
+        for (int d = 0; d < 3; d++) {
+            t.box.lo[d] = boxes[l].lo[d];
+            t.box.n[d] = boxes[l].n[d];
+        }
+        t.child = child_box(nlevels, boxes, l);
+        t.has_child = l + 1 < nlevels;
+        for (int32_t z = t.box.lo[2]; z < t.box.lo[2] + t.box.n[2]; z += 8)
+            for (int32_t y = t.box.lo[1]; y < t.box.lo[1] + t.box.n[1]; y += 8)
+                for (int32_t x = t.box.lo[0]; x < t.box.lo[0] + t.box.n[0]; x += 8) {
+                    const int32_t o[3] = {x, y, z};
+                    t.tile(o, 8);
+                }
+        const double h = std::ldexp(h0, -l);
+        for (auto& c : t.cells) {
+            if (blocks) {
+                BssnBlockDesc& b = blocks[count];
+                std::memset(&b, 0, sizeof b);
+                const int w = c.second;
+                b.sz = OCT * w + 7;
+                b.level = l;
+                b.offset = offset;
+                b.bflag = 0;
+                for (int d = 0; d < 3; d++) {
+                    b.g0[d] = OCT * c.first[d];
+                    b.ptmin[d] = xmin + (double)(b.g0[d] - 3) * h;
+                    b.ptmax[d] = b.ptmin[d] + (double)(b.sz - 1) * h;
+                    if (l == 0 && c.first[d] == 0) b.bflag |= 1u << (2 * d);
+                    if (l == 0 && c.first[d] + w == M0[d]) b.bflag |= 2u << (2 * d);
+                }
+            }
+            const int64_t s = OCT * c.second + 7;
+            offset += (s * s * s + 1) / 2 * 2;
+            count++;
+        }
+    }
+    *nblocks = count;
+    *n_nodes = nodes;
+    return 0;
+}
+
+namespace {
+
+struct Builder {
+    const BssnBlockDesc* blocks;
+    int nblocks, L;
+    const BssnLevelBox* boxes;
+    LevelMaps* out;
+    std::vector<std::vector<int32_t>> owner;  // per level: block of each octant of its box, -1 none
+
+    const LevelGrid& grid(int l) const { return out->grids[l]; }
+    bool in_grid(int l, const int64_t q[3]) const {
+        const LevelGrid& g = grid(l);
+        for (int d = 0; d < 3; d++)
+            if (q[d] < int64_t(OCT) * g.lo[d] || q[d] > int64_t(OCT) * (g.lo[d] + g.n[d])) return false;
+        return true;
+    }
+    int64_t node(int l, const int64_t q[3]) const {
+        const LevelGrid& g = grid(l);
+        const int64_t x = q[0] - int64_t(OCT) * g.lo[0], y = q[1] - int64_t(OCT) * g.lo[1],
+                      z = q[2] - int64_t(OCT) * g.lo[2];
+        return g.offset + x + int64_t(g.dims[0]) * (y + int64_t(g.dims[1]) * z);
+    }
+    int32_t owner_of(int l, const int64_t t[3]) const {
+        const LevelGrid& g = grid(l);
+        for (int d = 0; d < 3; d++)
+            if (t[d] < g.lo[d] || t[d] >= g.lo[d] + g.n[d]) return -1;
+        const int64_t i = (t[0] - g.lo[0]) + int64_t(g.n[0]) * ((t[1] - g.lo[1]) + int64_t(g.n[1]) * (t[2] - g.lo[2]));
+        return owner[l][i];
+    }
+    // Source of level-l index q outside level l's box (l >= 1): the coarse
+    // node or an interpolation entry.  kBad when the coarse stencil would
+    // leave level l-1's grid (cannot happen for valid boxes).
+    static constexpr int64_t kBad = std::numeric_limits<int64_t>::min();
+    int64_t coarse_source(int l, const int64_t q[3]) {
+        int64_t c[3];
+        int8_t j[3];
+        bool odd = false;
+        for (int d = 0; d < 3; d++) {
+            if ((q[d] & 1) == 0) {
+                c[d] = q[d] / 2;
+                j[d] = -1;
+            } else {
+                const int64_t clo = (q[d] - 1) / 2;  // q >= 1 here
+                const int64_t t = clo / OCT;
+                c[d] = OCT * t;
+                j[d] = (int8_t)(clo - OCT * t);
+                odd = true;
+            }
+        }
+        int64_t hi[3];
+        for (int d = 0; d < 3; d++) hi[d] = c[d] + (j[d] >= 0 ? OCT : 0);
+        if (!in_grid(l - 1, c) || !in_grid(l - 1, hi)) return kBad;
+        if (!odd) return node(l - 1, c);
+        InterpEntry e;
+        std::memset(&e, 0, sizeof e);
+        e.base = node(l - 1, c);
+        const LevelGrid& g = grid(l - 1);
+        e.stride[0] = 1;
+        e.stride[1] = g.dims[0];
+        e.stride[2] = g.dims[0] * g.dims[1];
+        for (int d = 0; d < 3; d++) e.j[d] = j[d];
+        out->interp.push_back(e);
+        return -2 - (int64_t)(out->interp.size() - 1);
+    }
+    int64_t padded_source(int l, const int64_t q[3]) {
+        if (in_grid(l, q)) return node(l, q);
+        if (l == 0) return -1;  // outside the domain
+        return coarse_source(l, q);
+    }
+};
+
+}  // namespace
+
+int levels_build(const BssnBlockDesc* blocks, int nblocks, int nlevels, const int32_t M0[3],
+                 const BssnLevelBox* boxes, LevelMaps* out) {
+    if (!blocks || nblocks <= 0 || !out) return BSSN_EINVAL;
+    int st = check_boxes(nlevels, M0, boxes);
+    if (st) return st;
+    *out = LevelMaps();
+    int64_t off = 0;
+    for (int l = 0; l < nlevels; l++) {
+        LevelGrid g;
+        for (int d = 0; d < 3; d++) {
+            g.lo[d] = boxes[l].lo[d];
+            g.n[d] = boxes[l].n[d];
+            g.dims[d] = OCT * g.n[d] + 1;
+        }
+        g.offset = off;
+        off += int64_t(g.dims[0]) * g.dims[1] * g.dims[2];
+        out->grids.push_back(g);
+    }
+    if (off >= (int64_t(1) << 31)) return BSSN_ELIMIT;
+    out->n_nodes = off;
+    Builder B{blocks, nblocks, nlevels, boxes, out, {}};
+    B.owner.resize(nlevels);
+    for (int l = 0; l < nlevels; l++)
+        B.owner[l].assign(size_t(boxes[l].n[0]) * boxes[l].n[1] * boxes[l].n[2], -1);
+    int64_t npad = 0;
+    for (int b = 0; b < nblocks; b++) {
+        const BssnBlockDesc& k = blocks[b];
+        const int w = (k.sz - 7) / OCT;
+        if (k.level < 0 || k.level >= nlevels || k.sz != OCT * w + 7 || (w != 1 && w != 2 && w != 4 && w != 8) ||
+            k.offset < 0)
+            return BSSN_EINVAL;
+        const Box child = child_box(nlevels, boxes, k.level);
+        int32_t o[3];
+        for (int d = 0; d < 3; d++) {
+            if (k.g0[d] % OCT) return BSSN_EINVAL;
+            o[d] = k.g0[d] / OCT;
+        }
+        Box box{{boxes[k.level].lo[0], boxes[k.level].lo[1], boxes[k.level].lo[2]},
+                {boxes[k.level].n[0], boxes[k.level].n[1], boxes[k.level].n[2]}};
+        if (!box.contains_cell(o, w) || (k.level + 1 < nlevels && !child.disjoint_cell(o, w)))
+            return BSSN_EINVAL;
+        for (int z = 0; z < w; z++)
+            for (int y = 0; y < w; y++)
+                for (int x = 0; x < w; x++) {
+                    const int64_t i = (o[0] + x - box.lo[0]) +
+                                      int64_t(box.n[0]) * ((o[1] + y - box.lo[1]) + int64_t(box.n[1]) * (o[2] + z - box.lo[2]));
+                    if (B.owner[k.level][i] >= 0) return BSSN_EINVAL;  // overlapping blocks
+                    B.owner[k.level][i] = b;
+                }
+        npad = std::max<int64_t>(npad, k.offset + int64_t(k.sz) * k.sz * k.sz);
+    }
+    // every octant of every level's region has a block
+    for (int l = 0; l < nlevels; l++) {
+        const Box child = child_box(nlevels, boxes, l);
+        for (int64_t i = 0; i < (int64_t)B.owner[l].size(); i++) {
+            const int32_t t[3] = {int32_t(boxes[l].lo[0] + i % boxes[l].n[0]),
+                                  int32_t(boxes[l].lo[1] + (i / boxes[l].n[0]) % boxes[l].n[1]),
+                                  int32_t(boxes[l].lo[2] + i / (int64_t(boxes[l].n[0]) * boxes[l].n[1]))};
+            const bool under = l + 1 < nlevels && child.contains_cell(t, 1);
+            if (under != (B.owner[l][i] < 0)) return BSSN_EINVAL;
+        }
+    }
+    out->n_padded = npad;
+    // ghost fill sources
+    out->unzip_src.assign(size_t(npad), -1);
+    for (int b = 0; b < nblocks; b++) {
+        const BssnBlockDesc& k = blocks[b];
+        const int s = k.sz;
+        for (int c = 0; c < s; c++)
+            for (int r = 0; r < s; r++)
+                for (int a = 0; a < s; a++) {
+                    const int64_t q[3] = {int64_t(k.g0[0]) + a - 3, int64_t(k.g0[1]) + r - 3, int64_t(k.g0[2]) + c - 3};
+                    const int64_t src = B.padded_source(k.level, q);
+                    if (src == Builder::kBad) return BSSN_EINVAL;
+                    out->unzip_src[size_t(k.offset + a + int64_t(s) * (r + int64_t(s) * c))] = src;
+                }
+    }
+    // owners
+    out->zip_src.assign(size_t(out->n_nodes), -1);
+    for (int l = 0; l < nlevels; l++) {
+        const LevelGrid& g = out->grids[l];
+        const Box child = child_box(nlevels, boxes, l);
+        const bool has_child = l + 1 < nlevels;
+        for (int64_t z = 0; z < g.dims[2]; z++)
+            for (int64_t y = 0; y < g.dims[1]; y++)
+                for (int64_t x = 0; x < g.dims[0]; x++) {
+                    const int64_t q[3] = {OCT * int64_t(g.lo[0]) + x, OCT * int64_t(g.lo[1]) + y,
+                                          OCT * int64_t(g.lo[2]) + z};
+                    const int64_t e[3] = {x, y, z};
+                    bool boundary = false, inside_child = has_child;
+                    for (int d = 0; d < 3; d++) {
+                        if (l > 0 && (e[d] == 0 || e[d] == g.dims[d] - 1)) boundary = true;
+                        if (has_child && !(q[d] > OCT * int64_t(child.lo[d]) && q[d] < OCT * int64_t(child.lo[d] + child.n[d])))
+                            inside_child = false;
+                    }
+                    if (boundary || inside_child) continue;
+                    int64_t t[3];
+                    for (int d = 0; d < 3; d++) t[d] = std::min<int64_t>(q[d] / OCT, g.lo[d] + g.n[d] - 1);
+                    int32_t b = B.owner_of(l, t);
+                    if (b < 0 && has_child) {  // on the finer box's boundary: the octant below
+                        for (int d = 0; d < 3; d++)
+                            if (q[d] == OCT * int64_t(child.lo[d])) t[d] -= 1;
+                        b = B.owner_of(l, t);
+                    }
+                    if (b < 0) return BSSN_EINVAL;
+                    const BssnBlockDesc& k = blocks[b];
+                    int64_t loc[3];
+                    for (int d = 0; d < 3; d++) {
+                        loc[d] = q[d] - k.g0[d] + 3;
+                        if (loc[d] < 3 || loc[d] > k.sz - 4) return BSSN_EINVAL;
+                    }
+                    out->zip_src[size_t(B.node(l, q))] =
+                        k.offset + loc[0] + int64_t(k.sz) * (loc[1] + int64_t(k.sz) * loc[2]);
+                }
+    }
+    // restriction, finest level first
+    out->inject_first.push_back(0);
+    for (int l = nlevels - 1; l >= 1; l--) {
+        const LevelGrid& g = out->grids[l];
+        // level l's box in level l-1 node index: [3 lo, 3 (lo + n)]
+        for (int64_t z = 3 * int64_t(g.lo[2]) + 1; z < 3 * int64_t(g.lo[2] + g.n[2]); z++)
+            for (int64_t y = 3 * int64_t(g.lo[1]) + 1; y < 3 * int64_t(g.lo[1] + g.n[1]); y++)
+                for (int64_t x = 3 * int64_t(g.lo[0]) + 1; x < 3 * int64_t(g.lo[0] + g.n[0]); x++) {
+                    const int64_t c[3] = {x, y, z}, f[3] = {2 * x, 2 * y, 2 * z};
+                    out->inject_dst.push_back(B.node(l - 1, c));
+                    out->inject_src.push_back(B.node(l, f));
+                }
+        out->inject_first.push_back((int)out->inject_dst.size());
+    }
+    // prolongation of box boundaries, coarsest first
+    out->prolong_first.push_back(0);
+    for (int l = 1; l < nlevels; l++) {
+        const LevelGrid& g = out->grids[l];
+        for (int64_t z = 0; z < g.dims[2]; z++)
+            for (int64_t y = 0; y < g.dims[1]; y++)
+                for (int64_t x = 0; x < g.dims[0]; x++) {
+                    const bool bd = x == 0 || y == 0 || z == 0 || x == g.dims[0] - 1 || y == g.dims[1] - 1 ||
+                                    z == g.dims[2] - 1;
+                    if (!bd) continue;
+                    const int64_t q[3] = {OCT * int64_t(g.lo[0]) + x, OCT * int64_t(g.lo[1]) + y,
+                                          OCT * int64_t(g.lo[2]) + z};
+                    const int64_t src = B.coarse_source(l, q);
+                    if (src == Builder::kBad) return BSSN_EINVAL;
+                    out->prolong_dst.push_back(B.node(l, q));
+                    out->prolong_src.push_back(src);
+                }
+        out->prolong_first.push_back((int)out->prolong_dst.size());
+    }
+    return 0;
+}
+
+namespace {
+
+__constant__ double kLagHalf[6][7];
+
+// grid-stride launches: at most 64 CTAs of 256 threads per SM
+int grid_for(int64_t n, int threads) {
+    const int64_t b = std::min<int64_t>((n + threads - 1) / threads, 148 * 64);
+    return (int)std::max<int64_t>(b, 1);
+}
+
+template <class T>
+int upload_vec(const std::vector<T>& v, T** d) {
+    *d = nullptr;
+    if (v.empty()) return 0;
+    if (cudaMalloc((void**)d, sizeof(T) * v.size()) != cudaSuccess) {
+        cudaGetLastError();
+        return BSSN_ENOMEM;
+    }
+    return cuda_status(cudaMemcpy(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+}
+
+// The interpolated value of one entry (x first, then y, then z; every
+// product and sum rounded in that order, as the oracle does).
+__device__ __forceinline__ double interp_value(const double* __restrict__ u, const InterpEntry& e) {
+    const int nx = e.j[0] >= 0 ? 7 : 1, ny = e.j[1] >= 0 ? 7 : 1, nz = e.j[2] >= 0 ? 7 : 1;
+    double tz = 0.0;
+    for (int c = 0; c < nz; c++) {
+        double ty = 0.0;
+        for (int b = 0; b < ny; b++) {
+            const double* row = u + e.base + (int64_t)b * e.stride[1] + (int64_t)c * e.stride[2];
+            double tx = 0.0;
+            for (int a = 0; a < nx; a++) {
+                const double w = e.j[0] >= 0 ? kLagHalf[e.j[0]][a] : 1.0;
+                const double p = __dmul_rn(w, __ldg(row + (int64_t)a * e.stride[0]));
+                tx = a == 0 ? p : __dadd_rn(tx, p);
+            }
+            const double w = e.j[1] >= 0 ? kLagHalf[e.j[1]][b] : 1.0;
+            const double p = __dmul_rn(w, tx);
+            ty = b == 0 ? p : __dadd_rn(ty, p);
+        }
+        const double w = e.j[2] >= 0 ? kLagHalf[e.j[2]][c] : 1.0;
+        const double p = __dmul_rn(w, ty);
+        tz = c == 0 ? p : __dadd_rn(tz, p);
+    }
+    return tz;
+}
+
+__device__ __forceinline__ double source_value(const double* __restrict__ u, int64_t src,
+                                               const InterpEntry* __restrict__ interp) {
+    if (src >= 0) return __ldg(u + src);
+    if (src == -1) return 0.0;
+    return interp_value(u, interp[-2 - src]);
+}
+
+__global__ void __launch_bounds__(256) levels_unzip_kernel(MutVars P, ConstVars U, int nvars,
+                                                           const int64_t* __restrict__ src,
+                                                           const InterpEntry* __restrict__ interp,
+                                                           int64_t n) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = src[p];
+        for (int v = 0; v < nvars; v++) P.p[v][p] = source_value(U.p[v], s, interp);
+    }
+}
+
+__global__ void __launch_bounds__(256) levels_zip_kernel(MutVars Rz, ConstVars R, int nvars,
+                                                         const int64_t* __restrict__ src, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = src[i];
+        for (int v = 0; v < nvars; v++) Rz.p[v][i] = s >= 0 ? __ldg(R.p[v] + s) : 0.0;
+    }
+}
+
+// dst[i] <- source value of src[i]; the sources never overlap the
+// destinations of the same launch.
+__global__ void __launch_bounds__(256) levels_copy_kernel(MutVars U, int nvars,
+                                                          const int64_t* __restrict__ dst,
+                                                          const int64_t* __restrict__ src,
+                                                          const InterpEntry* __restrict__ interp,
+                                                          int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = src[i], d = dst[i];
+        for (int v = 0; v < nvars; v++) {
+            const double* u = U.p[v];
+            U.p[v][d] = s >= 0 ? u[s] : (s == -1 ? 0.0 : interp_value(u, interp[-2 - s]));
+        }
+    }
+}
+
+}  // namespace
+
+int levels_upload(const LevelMaps& m, LevelsDev* d) {
+    *d = LevelsDev();
+    double w[6][7];
+    lagrange_half(w);
+    int st = cuda_status(cudaMemcpyToSymbol(kLagHalf, w, sizeof w));
+    if (!st) st = upload_vec(m.unzip_src, &d->unzip_src);
+    if (!st) st = upload_vec(m.zip_src, &d->zip_src);
+    if (!st) st = upload_vec(m.inject_dst, &d->inject_dst);
+    if (!st) st = upload_vec(m.inject_src, &d->inject_src);
+    if (!st) st = upload_vec(m.prolong_dst, &d->prolong_dst);
+    if (!st) st = upload_vec(m.prolong_src, &d->prolong_src);
+    if (!st) st = upload_vec(m.interp, &d->interp);
+    d->n_nodes = m.n_nodes;
+    d->n_padded = m.n_padded;
+    d->inject_first = m.inject_first;
+    d->prolong_first = m.prolong_first;
+    if (st) levels_free(d);
+    return st;
+}
+
+void levels_free(LevelsDev* d) {
+    cudaFree(d->unzip_src);
+    cudaFree(d->zip_src);
+    cudaFree(d->inject_dst);
+    cudaFree(d->inject_src);
+    cudaFree(d->prolong_dst);
+    cudaFree(d->prolong_src);
+    cudaFree(d->interp);
+    *d = LevelsDev();
+}
+
+namespace {
+int vars_in(const double* const* a, int nvars, ConstVars* c) {
+    if (nvars < 1 || nvars > NVARS) return BSSN_EINVAL;
+    for (int v = 0; v < nvars; v++) c->p[v] = a[v];
+    return 0;
+}
+int vars_out(double* const* a, int nvars, MutVars* c) {
+    if (nvars < 1 || nvars > NVARS) return BSSN_EINVAL;
+    for (int v = 0; v < nvars; v++) c->p[v] = a[v];
+    return 0;
+}
+}  // namespace
+
+int launch_levels_unzip(const LevelsDev& d, double* const* P, const double* const* U, int nvars,
+                        cudaStream_t s) {
+    MutVars p;
+    ConstVars u;
+    int st = vars_out(P, nvars, &p);
+    if (!st) st = vars_in(U, nvars, &u);
+    if (st || d.n_padded == 0) return st;
+    levels_unzip_kernel<<<grid_for(d.n_padded, 256), 256, 0, s>>>(p, u, nvars, d.unzip_src, d.interp,
+                                                                  d.n_padded);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_levels_zip(const LevelsDev& d, double* const* Rz, const double* const* R, int nvars,
+                      cudaStream_t s) {
+    MutVars z;
+    ConstVars r;
+    int st = vars_out(Rz, nvars, &z);
+    if (!st) st = vars_in(R, nvars, &r);
+    if (st || d.n_nodes == 0) return st;
+    levels_zip_kernel<<<grid_for(d.n_nodes, 256), 256, 0, s>>>(z, r, nvars, d.zip_src, d.n_nodes);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_levels_sync(const LevelsDev& d, double* const* U, int nvars, cudaStream_t s) {
+    MutVars u;
+    int st = vars_out(U, nvars, &u);
+    if (st) return st;
+    auto run = [&](const std::vector<int>& first, const int64_t* dst, const int64_t* src) {
+        for (size_t k = 0; k + 1 < first.size(); k++) {
+            const int64_t n = first[k + 1] - first[k];
+            if (n <= 0) continue;
+            levels_copy_kernel<<<grid_for(n, 256), 256, 0, s>>>(u, nvars, dst + first[k], src + first[k],
+                                                                d.interp, n);
+            const int e = cuda_status(cudaGetLastError());
+            if (e) return e;
+        }
+        return 0;
+    };
+    st = run(d.inject_first, d.inject_dst, d.inject_src);
+    return st ? st : run(d.prolong_first, d.prolong_dst, d.prolong_src);
+}
+
+}  // namespace bssn
+
+extern "C" {
+
+int bssn_mesh_generate_levels(int nlevels, const int32_t M0[3], const BssnLevelBox* boxes, double xmin,
+                              double h0, BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes) {
+    return bssn::levels_generate(nlevels, M0, boxes, xmin, h0, blocks, nblocks, n_nodes);
+}
+
+int bssn_levels_maps(const BssnBlockDesc* blocks, int nblocks, int nlevels, const int32_t M0[3],
+                     const BssnLevelBox* boxes, int64_t sizes[5], int64_t* unzip_src, int64_t* zip_src,
+                     int64_t* inject, int64_t* prolong, int64_t* interp) {
+    if (!sizes) return BSSN_EINVAL;
+    bssn::LevelMaps m;
+    const int st = bssn::levels_build(blocks, nblocks, nlevels, M0, boxes, &m);
+    if (st) return st;
+    sizes[0] = m.n_padded;
+    sizes[1] = m.n_nodes;
+    sizes[2] = (int64_t)m.inject_dst.size();
+    sizes[3] = (int64_t)m.prolong_dst.size();
+    sizes[4] = (int64_t)m.interp.size();
+    if (unzip_src) std::copy(m.unzip_src.begin(), m.unzip_src.end(), unzip_src);
+    if (zip_src) std::copy(m.zip_src.begin(), m.zip_src.end(), zip_src);
+    if (inject)
+        for (size_t i = 0; i < m.inject_dst.size(); i++) {
+            inject[2 * i] = m.inject_dst[i];
+            inject[2 * i + 1] = m.inject_src[i];
+        }
+    if (prolong)
+        for (size_t i = 0; i < m.prolong_dst.size(); i++) {
+            prolong[2 * i] = m.prolong_dst[i];
+            prolong[2 * i + 1] = m.prolong_src[i];
+        }
+    if (interp)
+        for (size_t i = 0; i < m.interp.size(); i++) {
+            const bssn::InterpEntry& e = m.interp[i];
+            int64_t* o = interp + 7 * i;
+            o[0] = e.base;
+            for (int d = 0; d < 3; d++) {
+                o[1 + d] = e.stride[d];
+                o[4 + d] = e.j[d];
+            }
+        }
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,87 @@
+// Multi-level meshes: nested level boxes with 2:1 refinement, each level's
+// region tiled with blocks, the zipped state the concatenation of one dense
+// node grid per level.  Host-side maps (built once per mesh) and the kernels
+// that use them: the ghost fill with coarse-to-fine interpolation, the owner
+// gather of the right-hand side, and the level sync (restriction by
+// injection, prolongation of fine box boundaries).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "bssn_b200.h"
+
+namespace bssn {
+
+// One level's node grid: its box in level octants, its first node in the
+// concatenated zipped arrays, and its node counts per axis (6 n + 1).
+struct LevelGrid {
+    int32_t lo[3], n[3];
+    int64_t offset;
+    int32_t dims[3];
+};
+
+// A point interpolated from the next coarser level: along every axis with
+// j[d] >= 0 a degree-6 Lagrange interpolation over the 7 nodes of a coarse
+// octant (base + m * stride[d], m = 0..6) at m = j[d] + 1/2; along the
+// others the single node at base.  Axes are interpolated x first, then y,
+// then z.
+struct InterpEntry {
+    int64_t base;
+    int32_t stride[3];
+    int8_t j[3];
+    int8_t pad[5];
+};
+static_assert(sizeof(InterpEntry) == 32, "device layout");
+
+// Source of a value: >= 0 a node of the zipped arrays, -1 zero (outside the
+// domain), <= -2 interpolation entry -2 - src.
+struct LevelMaps {
+    std::vector<LevelGrid> grids;
+    int64_t n_nodes = 0;
+    int64_t n_padded = 0;
+    std::vector<int64_t> unzip_src;              // per padded point
+    std::vector<int64_t> zip_src;                // per node: owning zone's padded index or -1
+    std::vector<int64_t> inject_dst, inject_src; // coarse node under a finer box <- fine node
+    std::vector<int> inject_first;               // per level l >= 1: first entry (size L + 1)
+    std::vector<int64_t> prolong_dst, prolong_src; // fine box-boundary node <- coarse source
+    std::vector<int> prolong_first;
+    std::vector<InterpEntry> interp;
+};
+
+struct LevelsDev {
+    int64_t* unzip_src = nullptr;
+    int64_t* zip_src = nullptr;
+    int64_t* inject_dst = nullptr;
+    int64_t* inject_src = nullptr;
+    int64_t* prolong_dst = nullptr;
+    int64_t* prolong_src = nullptr;
+    InterpEntry* interp = nullptr;
+    int64_t n_nodes = 0, n_padded = 0;
+    std::vector<int> inject_first, prolong_first;  // host copies of the level ranges
+};
+
+// Validates the boxes, tiles every level's region (its box minus the next
+// finer box) with blocks of 1, 2, 4 or 8 octants per axis, and lays them out
+// (offsets, sides 13/19/31/55, level, origin g0 in the level's node index,
+// ptmin / ptmax, physical-boundary flags on level 0).  blocks == NULL: count
+// only.  n_nodes: total zipped nodes over all levels.
+int levels_generate(int nlevels, const int32_t M0[3], const BssnLevelBox* boxes, double xmin,
+                    double h0, BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes);
+// The maps of a generated mesh (host only).
+int levels_build(const BssnBlockDesc* blocks, int nblocks, int nlevels, const int32_t M0[3],
+                 const BssnLevelBox* boxes, LevelMaps* out);
+int levels_upload(const LevelMaps& m, LevelsDev* d);
+void levels_free(LevelsDev* d);
+
+// P <- ghost fill of the zipped state U (every padded point of every block).
+int launch_levels_unzip(const LevelsDev& d, double* const* P, const double* const* U, int nvars,
+                        cudaStream_t s);
+// Rz[node] <- R[owner zone of node], 0 for nodes no block owns.
+int launch_levels_zip(const LevelsDev& d, double* const* Rz, const double* const* R, int nvars,
+                      cudaStream_t s);
+// Restriction (finest level first) then prolongation (coarsest first) on U.
+int launch_levels_sync(const LevelsDev& d, double* const* U, int nvars, cudaStream_t s);
+
+}  // namespace bssn

@@ -151,6 +151,10 @@ void mesh_destroy(MeshState* m) {
     cudaFree(m->d_elem_first);
     for (auto& t : m->tasks) cudaFree(t.second.first);
     cudaFree(m->d_scratch);
+    if (m->lv) {
+        levels_free(m->lv);
+        delete m->lv;
+    }
     delete m;
 }
 

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "bssn_b200.h"
+#include "levels.h"
 #include "remesh.h"
 #include "rhs_fused.cuh"
 
@@ -53,6 +54,9 @@ struct MeshState {
     // scratch of the split right-hand side (kSplitSlots doubles per zone)
     double* d_scratch = nullptr;
     int64_t scratch_zones = 0;
+    // multi-level meshes: the level maps (nullptr for single-level meshes,
+    // whose zipped state is one node grid of dims G)
+    LevelsDev* lv = nullptr;
 };
 
 int mesh_create(const BssnBlockDesc* blocks, int nblocks, const int32_t G[3],

@@ -45,7 +45,7 @@ int plan_create(MeshState* m, const BssnParams& prm, int flags, Plan** out) {
     const int64_t nn = (int64_t)m->G[0] * m->G[1] * m->G[2];
     p->n_nodes = nn;
     // node indices of the direct path are 32-bit
-    p->direct = (flags & BSSN_PLAN_DIRECT) && !(flags & BSSN_PLAN_PER_BLOCK) &&
+    p->direct = (flags & BSSN_PLAN_DIRECT) && !(flags & BSSN_PLAN_PER_BLOCK) && !m->lv &&
                 nn < (int64_t(1) << 31);
     int st = 0;
     if (p->direct) {
@@ -106,6 +106,12 @@ int plan_create(MeshState* m, const BssnParams& prm, int flags, Plan** out) {
     return 0;
 }
 
+// Ghost fill of every block of the mesh (through the level maps on a
+// multi-level mesh).
+static int unzip_all(MeshState* m, double* const* P, const double* const* U, cudaStream_t s) {
+    return m->lv ? launch_levels_unzip(*m->lv, P, U, NVARS, s) : launch_unzip(m, P, U, NVARS, s);
+}
+
 // Releases the captured graphs (the next step captures them again).
 static void drop_graphs(Plan* p) {
     if (p->exec) cudaGraphExecDestroy(p->exec);
@@ -158,7 +164,7 @@ int plan_set_tile(Plan* p, int side, int tile) {
 // split tile): the split passes then write each node once, from the block
 // owning it, and a node-wise kernel applies the stage (no zip gather).
 bool plan_zipped_rhs(const Plan* p) {
-    if (p->direct || !p->Rz || (p->flags & BSSN_PLAN_PER_BLOCK)) return false;
+    if (p->direct || !p->Rz || (p->flags & BSSN_PLAN_PER_BLOCK) || p->mesh->lv) return false;
     for (int side : p->sides)
         if (tile_mode(plan_tile(p, side)) != 1) return false;
     return true;
@@ -240,6 +246,21 @@ int plan_enqueue_stage(Plan* p, double* const* u, double dt, int stage, cudaStre
     set_ptrs(p->acc, p->n_nodes, Ap);
     const int enf = (p->flags & BSSN_PLAN_ENFORCE_STAGES) ? 1 : 0;
     const double* const* src = stage == 0 ? (const double* const*)u : (const double* const*)Ip;
+    if (m->lv) {
+        // multi-level mesh: ghost fill through the level maps, right-hand
+        // side per block (each with its level's spacing), owner gather into
+        // the zipped right-hand side, node-wise stage, level sync of the state
+        // just written
+        double* Rz[NVARS];
+        set_ptrs(p->Rz, p->n_nodes, Rz);
+        int st = launch_levels_unzip(*m->lv, Pp, src, NVARS, s);
+        if (!st) st = plan_rhs(p, s, nullptr, nullptr);
+        if (!st) st = launch_levels_zip(*m->lv, Rz, (const double* const*)Rp, NVARS, s);
+        if (!st)
+            st = launch_node_stage(stage, Ip, Ap, u, Rz, p->n_nodes, dt, enf, p->prm.chi_floor, p->status, s);
+        if (!st) st = launch_levels_sync(*m->lv, stage < 3 ? Ip : u, NVARS, s);
+        return st;
+    }
     if (p->direct || plan_zipped_rhs(p)) {
         double* Rz[NVARS];
         set_ptrs(p->Rz, p->n_nodes, Rz);
@@ -319,7 +340,8 @@ int plan_step(Plan* p, double* const* u, double dt, cudaStream_t s) {
 // reference's time loop computes the same norms every BSSN_IO_OUTPUT_FREQ
 // steps (BSSN_GR/src/bssnCtx.cpp:597-685, computeConstraintL2Norm).
 static int diag_prepare(Plan* p) {
-    if (p->direct || !p->P) return BSSN_ESTATE;  // needs the padded stage array
+    // needs the padded stage array and a single-level node grid
+    if (p->direct || !p->P || p->mesh->lv) return BSSN_ESTATE;
     MeshState* m = p->mesh;
     if (!p->cons && alloc(&p->cons, (size_t)4 * p->n_nodes)) return BSSN_ENOMEM;
     if (!m->d_partial &&
@@ -334,7 +356,7 @@ static int enqueue_diag(Plan* p, double* const* u, const DiagArgs& d, cudaStream
     MeshState* m = p->mesh;
     double* Pp[NVARS];
     set_ptrs(p->P, m->unzip_size, Pp);
-    int st = launch_unzip(m, Pp, (const double* const*)u, NVARS, s);
+    int st = unzip_all(m, Pp, (const double* const*)u, s);
     if (st) return st;
     double* cons[4];
     for (int c = 0; c < 4; c++) cons[c] = p->cons + (size_t)c * p->n_nodes;
@@ -394,7 +416,7 @@ int plan_autotune(Plan* p, double* const* u, int reps, cudaStream_t s, float* ti
     } else {
         double* Pp[NVARS];
         set_ptrs(p->P, m->unzip_size, Pp);
-        st = launch_unzip(m, Pp, (const double* const*)u, NVARS, s);
+        st = unzip_all(m, Pp, (const double* const*)u, s);
         if (st) return st;
         double* Rp[NVARS];
         set_ptrs(p->R, m->unzip_size, Rp);

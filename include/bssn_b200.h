@@ -412,6 +412,59 @@ int bssn_tile_mode(int tile);
 long bssn_tile_selfcheck(int tile);
 
 /* ---------------------------------------------------------------------- */
+/* Multi-level meshes (the level-transition ghost fill of dendrolib's
+ * ot::Mesh, absent from the reference tree; call sites
+ * BSSN_GR/src/rkBSSN.cpp:611-650).  Level l has node spacing h0 / 2^l and
+ * a box of level-l octants (6 node intervals each); level 0's box is the
+ * whole domain (M0 octants per axis); the box of level l >= 1 lies inside
+ * level l-1's box with at least one level-(l-1) octant of margin and starts
+ * and ends on level-(l-1) octant corners (even lo and n).  Level l's blocks
+ * tile its box minus level l+1's box.  The zipped state of every variable is
+ * the concatenation of one dense node grid per level, (6 n + 1) nodes per
+ * axis, node (x, y, z) of level l at offset_l + x + dx (y + dy z) with
+ * coordinates relative to the box corner.  Ghost fill of a level-l block:
+ * level-l nodes where its padded points lie in level l's box, otherwise the
+ * level-(l-1) node (even fine index on every axis) or a degree-6 Lagrange
+ * interpolation over the 7 nodes of the enclosing level-(l-1) octant along
+ * every odd axis (x, then y, then z).  Level sync after every stage: level-
+ * (l-1) nodes strictly inside level l's box take the coincident level-l
+ * value (finest level first); level-l nodes on its box boundary take the
+ * level-(l-1) value or interpolation (coarsest first).  A node no block owns
+ * (under a finer box, on a fine box boundary) gets its value only from the
+ * sync. */
+typedef struct BssnLevelBox {
+    int32_t lo[3];          /* first octant, in level-l octants */
+    int32_t n[3];           /* octants per axis */
+} BssnLevelBox;
+/* Tiles the levels with blocks (sides 13/19/31/55, level, g0 = first
+ * interior node in the level's global node index, ptmin/ptmax from
+ * xmin + (g0 - 3) h_l, physical-boundary flags on level 0).  blocks == NULL
+ * returns the count only.  *n_nodes: zipped nodes of all levels (< 2^31).
+ * Host only. */
+int bssn_mesh_generate_levels(int nlevels, const int32_t M0[3], const BssnLevelBox* boxes,
+                              double xmin, double h0, BssnBlockDesc* blocks, int* nblocks,
+                              int64_t* n_nodes);
+/* Mesh handle of a generated multi-level mesh.  bssn_unzip_f64 and
+ * bssn_zip_f64 on it use the level maps; RK4 plans on it run the padded form
+ * (ghost fill, right-hand side per block with its own spacing, owner gather,
+ * node-wise stage, level sync). */
+int bssn_mesh_create_levels(const BssnBlockDesc* blocks, int nblocks, int nlevels,
+                            const int32_t M0[3], const BssnLevelBox* boxes, bssn_mesh* out);
+/* Level sync of a zipped state (after initial data or any outside update). */
+int bssn_mesh_levels_sync(bssn_mesh mesh, double* const* u_dev, int nvars,
+                          bssn_stream_t stream);
+/* Host-only copies of the level maps, for tests: per padded point the
+ * ghost-fill source (>= 0 node, -1 zero, <= -2 interpolation entry
+ * -2 - src), per node the owning zone's padded index (-1: none), and the
+ * injection / prolongation pairs (dst node, src as above).  Call with NULL
+ * arrays to get the sizes (sizes[0..4] = padded points, nodes, injections,
+ * prolongations, interpolation entries); interp receives per entry
+ * {base, stride x, stride y, stride z, jx, jy, jz} as int64. */
+int bssn_levels_maps(const BssnBlockDesc* blocks, int nblocks, int nlevels, const int32_t M0[3],
+                     const BssnLevelBox* boxes, int64_t sizes[5], int64_t* unzip_src,
+                     int64_t* zip_src, int64_t* inject, int64_t* prolong, int64_t* interp);
+
+/* ---------------------------------------------------------------------- */
 /* Checkpoint and restart: BSSNCtx::write_checkpt / restore_checkpt
  * (BSSN_GR/src/bssnCtx.cpp:783-862, 864-1170).  Files, as the reference
  * names them:

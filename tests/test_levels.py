@@ -1,0 +1,155 @@
+"""Multi-level meshes on the CPU: the library's generator and host-built
+level maps (csrc/levels.cu) against the independent geometric oracle
+(oracle_levels.py) -- every ghost-fill source, owner and sync entry, applied
+to the same seeded state, bit-identical -- and the interpolation exact on
+polynomials of degree <= 6."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.join(os.path.dirname(HERE), "dendro-gr_b200"))
+
+import oracle_lib as ol  # noqa: E402
+from oracle_levels import LevelOracle, lagrange_half  # noqa: E402
+
+B = pytest.importorskip("bssn_b200")
+from bssn_b200 import levels as LV  # noqa: E402
+
+MESHES = {
+    "two": ((4, 4, 4), [((2, 2, 2), (4, 4, 4))]),
+    "three": ((6, 6, 6), [((2, 4, 2), (6, 4, 8)), ((6, 10, 6), (4, 2, 6))]),
+}
+
+
+@pytest.fixture(scope="module")
+def O():
+    return ol.oracle()
+
+
+def eval_maps(maps, Z, W):
+    """The library's maps applied in numpy: ghost fill and sync."""
+    itp = maps["interp"]
+
+    def value(src):
+        out = np.zeros((Z.shape[0], len(src)))
+        pos = src >= 0
+        out[:, pos] = Z[:, src[pos]]
+        ent = itp[-2 - src[src <= -2]]
+        sel = np.nonzero(src <= -2)[0]
+        n = np.where(ent[:, 4:7] >= 0, 7, 1)
+        for pat in np.unique(n @ np.array([1, 10, 100])):
+            m = (n @ np.array([1, 10, 100])) == pat
+            e, s = ent[m], sel[m]
+            nx, ny, nz = pat % 10, (pat // 10) % 10, pat // 100
+            w = [W[np.maximum(e[:, 4 + d], 0)] if (nx, ny, nz)[d] == 7 else np.ones((len(e), 1)) for d in range(3)]
+            tz = None
+            for c in range(nz):
+                ty = None
+                for b in range(ny):
+                    tx = None
+                    for a in range(nx):
+                        t = w[0][:, a] * Z[:, e[:, 0] + a * e[:, 1] + b * e[:, 2] + c * e[:, 3]]
+                        tx = t if a == 0 else tx + t
+                    t = w[1][:, b] * tx
+                    ty = t if b == 0 else ty + t
+                t = w[2][:, c] * ty
+                tz = t if c == 0 else tz + t
+            out[:, s] = tz
+        return out
+
+    return value
+
+
+@pytest.mark.parametrize("name", sorted(MESHES))
+def test_generator_tiles_levels(name):
+    M0, boxes = MESHES[name]
+    spec = LV.generate_levels(M0, boxes)
+    bl = spec.as_numpy()
+    assert set(bl["sz"].tolist()) <= {13, 19, 31, 55}
+    assert (bl["bflag"][bl["level"] > 0] == 0).all()
+    assert spec.h == spec.h0 / 2 ** len(boxes)
+    # the block offsets are increasing and non-overlapping
+    ends = bl["offset"] + bl["sz"].astype(np.int64) ** 3
+    assert (bl["offset"][1:] >= ends[:-1]).all()
+    LO = LevelOracle(spec, ol.oracle())
+    for l, (lo, n) in enumerate(LO.boxes):
+        under = np.zeros(tuple(n[::-1]), dtype=bool)
+        if l + 1 < LO.L:
+            clo, cn = LO.boxes[l + 1][0] // 2 - lo, LO.boxes[l + 1][1] // 2
+            under[clo[2]:clo[2] + cn[2], clo[1]:clo[1] + cn[1], clo[0]:clo[0] + cn[0]] = True
+        assert ((LO.octs[l] >= 0) == ~under).all(), l
+    assert LO.n_nodes == spec.n_nodes
+
+
+@pytest.mark.parametrize("name", sorted(MESHES))
+def test_maps_match_oracle(name, O):
+    M0, boxes = MESHES[name]
+    spec = LV.generate_levels(M0, boxes)
+    LO = LevelOracle(spec, O)
+    maps = LV.level_maps(spec)
+    W = lagrange_half()
+    rng = np.random.default_rng(7)
+    Z = rng.standard_normal((3, spec.n_nodes))
+    value = eval_maps(maps, Z, W)
+    # ghost fill
+    Z24 = np.zeros((ol.NVARS, spec.n_nodes))
+    Z24[:3] = Z
+    ref = LO.unzip(Z24)[:3]
+    got = value(maps["unzip_src"])
+    assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))
+    # owners
+    assert np.array_equal(maps["zip_src"], LO.owners())
+    # sync: injections then prolongations, in the library's list order
+    S = Z.copy()
+    inj, pro = maps["inject"], maps["prolong"]
+    lv_node = np.searchsorted(np.array(LO.offsets[1:]), inj[:, 0], side="right")
+    for l in sorted(set(lv_node.tolist()), reverse=True):
+        m = lv_node == l
+        S[:, inj[m, 0]] = S[:, inj[m, 1]]
+    pl = np.searchsorted(np.array(LO.offsets[1:]), pro[:, 0], side="right")
+    for l in sorted(set(pl.tolist())):
+        m = pl == l
+        S[:, pro[m, 0]] = eval_maps(maps, S, W)(pro[m, 1])
+    Z24 = np.zeros((ol.NVARS, spec.n_nodes))
+    Z24[:3] = Z
+    ref = LO.sync(Z24)[:3]
+    assert np.array_equal(S.view(np.uint64), ref.view(np.uint64))
+
+
+def test_interpolation_exact_on_degree_6(O):
+    """A degree-6 polynomial in x, y, z per level grid: the ghost fill of
+    the finer blocks reproduces it outside their box (rounding only)."""
+    M0, boxes = MESHES["two"]
+    spec = LV.generate_levels(M0, boxes)
+    LO = LevelOracle(spec, O)
+    Z = np.zeros((ol.NVARS, spec.n_nodes))
+
+    def poly(x, y, z):
+        return 0.3 + x ** 6 / 4096 - 0.2 * x * y ** 3 * z ** 2 / 512 + 0.1 * y ** 5 / 1024 - z ** 4 / 256 + x * y
+
+    coords = []
+    for l, (lo, n) in enumerate(LO.boxes):
+        h = spec.h0 / 2 ** l
+        d = LO.dims[l]
+        z, y, x = np.meshgrid(*[np.arange(k) for k in d[::-1]], indexing="ij")
+        pts = [spec.xmin + (OCTL + o) * h for OCTL, o in zip((x.ravel(), y.ravel(), z.ravel()), 6 * lo)]
+        coords.append(pts)
+        Z[0, LO.offsets[l]:LO.offsets[l] + int(np.prod(d))] = poly(*pts)
+    P = LO.unzip(Z)
+    bl = spec.as_numpy()
+    worst = 0.0
+    for b in np.nonzero(bl["level"] == 1)[0]:
+        s = int(bl["sz"][b])
+        h = spec.h0 / 2
+        i = np.arange(s)
+        zz, yy, xx = np.meshgrid(i, i, i, indexing="ij")
+        q = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], axis=1) + bl["g0"][b] - 3
+        x, y, z = [spec.xmin + q[:, k] * h for k in range(3)]
+        exact = poly(x, y, z)
+        got = P[0, int(bl["offset"][b]):int(bl["offset"][b]) + s ** 3]
+        worst = max(worst, np.abs(got - exact).max() / np.abs(exact).max())
+    assert worst < 1e-12, worst
