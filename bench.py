@@ -10,7 +10,7 @@ RHS over all blocks, zip + stage update + constraint enforcement}), replayed
 as a CUDA graph.  Prints one JSON line (see the keys below).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload mix20k|mix4k|uniform512|small]
+                  [--workload mix20k|mix4k|uniform512|small|levels]
 
 Under torchrun each rank evolves its own replica of the workload (weak
 scaling); the time is the max over ranks.
@@ -37,7 +37,30 @@ WORKLOADS = {
     "mix4k": (1, (7, 5, 4), "mixed-level plain-path size: ~4,000 blocks"),
     "uniform512": (0, (8, 8, 8), "uniform octree of 512 blocks of 13^3"),
     "small": (1, (2, 2, 2), "small mix for profiler captures"),
+    "levels": (2, (24, 7), "multi-level: [-400,400]^3, 7 nested levels of 24^3-octant boxes "
+                           "halving toward the punctures at (+-4,0,0)"),
 }
+
+
+def level_boxes(M0, nlevels):
+    """Boxes of levels 1.. for the `levels` workload: each level's box is
+    M0 of its own octants per axis, centred on the origin, so it covers the
+    middle half of its parent's box."""
+    boxes, lo = [], 0
+    for _ in range(1, nlevels):
+        lo = 2 * lo + M0 // 2
+        boxes.append(((lo,) * 3, (M0,) * 3))
+    return boxes
+
+
+def workload_spec(B, wl):
+    """The mesh of a workload: a seeded single-level octree, or the nested
+    multi-level mesh of `levels`."""
+    mode, dims, _ = WORKLOADS[wl]
+    if mode == 2:
+        from bssn_b200 import levels as LV
+        return LV.generate_levels((dims[0],) * 3, level_boxes(dims[0], dims[1]), xmin=-400.0, L=800.0)
+    return B.generate_mesh(mode, dims, MIX, seed=SEED_MESH)
 SEED_MESH = 20261203
 MIX = (0.7, 0.2, 0.08, 0.02)
 FLOP_PER_ZONE_STAGE = 6535.0  # 6,439 RHS + 96 RK axpy (per zone, per stage)
@@ -264,7 +287,7 @@ def run_reference(args, wl):
         return
     import bssn_b200 as B
     mode, dims, desc = WORKLOADS[wl]
-    spec = B.generate_mesh(mode, dims, MIX, seed=SEED_MESH)
+    spec = workload_spec(B, wl)
     rates = []
     for _ in range(args.warmup):
         cpu_reference_rate(spec.sides, seconds=2.0)
@@ -427,13 +450,17 @@ def main():
         return
 
     mode, dims, desc = WORKLOADS[wl]
-    spec = B.generate_mesh(mode, dims, MIX, seed=SEED_MESH)
+    spec = workload_spec(B, wl)
     zones = spec.zones()
     prm = B.default_params()
     dt = 0.25 * spec.h
     mesh = B.Mesh(spec)
     U = torch.zeros((24, spec.n_nodes), dtype=torch.float64, device="cuda")
-    B.initial_data(U, spec)
+    if mode == 2:
+        from bssn_b200 import levels as LV
+        LV.initial_data_levels(U, spec, mesh=mesh, bh=(4.0, 0.0, 0.0, -4.0, 0.0, 0.0))
+    else:
+        B.initial_data(U, spec)
     U0 = None
     stream = torch.cuda.current_stream()
 
@@ -607,7 +634,9 @@ def main():
                       "zones": zones, "sides": {str(s): int((spec.sides == s).sum()) for s in sorted(set(spec.sides.tolist()))},
                       "nodes": spec.n_nodes, "dt_over_dx": 0.25,
                       "l2": "inputs larger than L2 (24 x %.3g nodes x 8 B)" % spec.n_nodes,
-                      "parallelism": f"replicas x{world}", "tiles": {str(k): int(v) for k, v in chosen.items()}},
+                      "parallelism": f"replicas x{world}", "tiles": {str(k): int(v) for k, v in chosen.items()},
+                      "levels": ([{"lo": list(lo), "n": list(n)} for lo, n in spec.boxes]
+                                 if getattr(spec, "boxes", None) else None)},
            "roofline": roofline,
            "step_hbm": {"bytes_per_step": sb, "achieved_gbs": sb / (ms_step * 1e-3) / 1e9,
                         "frac": sb / (ms_step * 1e-3) / 1e9 / hbm_peak},

@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -429,21 +430,38 @@ __device__ __forceinline__ double interp_value(const double* __restrict__ u, con
     return tz;
 }
 
-__device__ __forceinline__ double source_value(const double* __restrict__ u, int64_t src,
-                                               const InterpEntry* __restrict__ interp) {
-    if (src >= 0) return __ldg(u + src);
-    if (src == -1) return 0.0;
-    return interp_value(u, interp[-2 - src]);
+// One pass of the separable ghost fill (PassTask): inputs from the zipped
+// state (first pass) or from the previous pass's results.
+__global__ void __launch_bounds__(256) levels_pass_kernel(ConstVars U, double* __restrict__ it, int64_t n_it,
+                                                          int nvars, const PassTask* __restrict__ tasks,
+                                                          int64_t n, int from_u) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const PassTask t = tasks[i];
+        for (int v = 0; v < nvars; v++) {
+            const double* in = from_u ? U.p[v] : it + (int64_t)v * n_it;
+            double acc = 0.0;
+            for (int k = 0; k < t.n; k++) {
+                const double w = t.n == 7 ? kLagHalf[t.j][k] : 1.0;
+                const double p = __dmul_rn(w, in[t.in[k]]);
+                acc = k == 0 ? p : __dadd_rn(acc, p);
+            }
+            it[(int64_t)v * n_it + t.out] = acc;
+        }
+    }
 }
 
+// Ghost fill: zipped node, zero, or a third-pass result (interpolated point).
 __global__ void __launch_bounds__(256) levels_unzip_kernel(MutVars P, ConstVars U, int nvars,
                                                            const int64_t* __restrict__ src,
-                                                           const InterpEntry* __restrict__ interp,
-                                                           int64_t n) {
+                                                           const double* __restrict__ it, int64_t n_it,
+                                                           int64_t zbase, int64_t n) {
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
          p += (int64_t)gridDim.x * blockDim.x) {
         const int64_t s = src[p];
-        for (int v = 0; v < nvars; v++) P.p[v][p] = source_value(U.p[v], s, interp);
+        for (int v = 0; v < nvars; v++)
+            P.p[v][p] = s >= 0 ? __ldg(U.p[v] + s)
+                               : (s == -1 ? 0.0 : it[(int64_t)v * n_it + zbase + (-2 - s)]);
     }
 }
 
@@ -475,12 +493,100 @@ __global__ void __launch_bounds__(256) levels_copy_kernel(MutVars U, int nvars,
 
 }  // namespace
 
+namespace {
+
+// The three passes of the separable ghost fill for the interpolated padded
+// points of m, deduplicated (a row or point needed by several padded
+// points is computed once), and the ghost-fill sources with interpolation
+// entries replaced by third-pass results.  Slots: first pass [0, n0),
+// second [n0, n0 + n1), third after.
+void build_passes(const LevelMaps& m, std::vector<PassTask>& tasks, int64_t n_task[3],
+                  std::vector<int64_t>& unzip_code) {
+    std::vector<PassTask> pass[3];
+    std::unordered_map<int64_t, int32_t> key[3];
+    auto task = [&](int stage, int64_t k, auto make) -> int32_t {
+        auto it = key[stage].find(k);
+        if (it != key[stage].end()) return it->second;
+        PassTask t = make();
+        t.out = (int32_t)pass[stage].size();
+        pass[stage].push_back(t);
+        key[stage].emplace(k, t.out);
+        return t.out;
+    };
+    auto blank = []() {
+        PassTask t;
+        std::memset(&t, 0, sizeof t);
+        return t;
+    };
+    std::vector<int32_t> zslot(m.interp.size(), -1);
+    unzip_code = m.unzip_src;
+    for (auto& src : unzip_code) {
+        if (src > -2) continue;
+        const int64_t ie = -2 - src;
+        if (zslot[ie] < 0) {
+            const InterpEntry& e = m.interp[ie];
+            const int nn[3] = {e.j[0] >= 0 ? 7 : 1, e.j[1] >= 0 ? 7 : 1, e.j[2] >= 0 ? 7 : 1};
+            const int64_t zk = e.base * 512 + (e.j[0] + 1) * 64 + (e.j[1] + 1) * 8 + (e.j[2] + 1);
+            zslot[ie] = task(2, zk, [&]() {
+                PassTask z = blank();
+                z.n = (int8_t)nn[2];
+                z.j = e.j[2] >= 0 ? e.j[2] : 0;
+                for (int c = 0; c < nn[2]; c++) {
+                    const int64_t plane = e.base + (int64_t)c * e.stride[2];
+                    z.in[c] = task(1, plane * 64 + (e.j[0] + 1) * 8 + (e.j[1] + 1), [&]() {
+                        PassTask y = blank();
+                        y.n = (int8_t)nn[1];
+                        y.j = e.j[1] >= 0 ? e.j[1] : 0;
+                        for (int b = 0; b < nn[1]; b++) {
+                            const int64_t row = plane + (int64_t)b * e.stride[1];
+                            y.in[b] = task(0, row * 8 + (e.j[0] + 1), [&]() {
+                                PassTask x = blank();
+                                x.n = (int8_t)nn[0];
+                                x.j = e.j[0] >= 0 ? e.j[0] : 0;
+                                for (int a = 0; a < nn[0]; a++) x.in[a] = (int32_t)(row + (int64_t)a * e.stride[0]);
+                                return x;
+                            });
+                        }
+                        return y;
+                    });
+                }
+                return z;
+            });
+        }
+        src = -2 - (int64_t)zslot[ie];
+    }
+    // second-pass inputs and outputs after the first pass, third after both
+    const int32_t n0 = (int32_t)pass[0].size(), n1 = (int32_t)pass[1].size();
+    for (auto& t : pass[1]) t.out += n0;
+    for (auto& t : pass[2]) {
+        t.out += n0 + n1;
+        for (int k = 0; k < t.n; k++) t.in[k] += n0;
+    }
+    tasks.clear();
+    for (int k = 0; k < 3; k++) {
+        n_task[k] = (int64_t)pass[k].size();
+        tasks.insert(tasks.end(), pass[k].begin(), pass[k].end());
+    }
+}
+
+}  // namespace
+
 int levels_upload(const LevelMaps& m, LevelsDev* d) {
     *d = LevelsDev();
     double w[6][7];
     lagrange_half(w);
+    std::vector<PassTask> tasks;
+    std::vector<int64_t> code;
+    build_passes(m, tasks, d->n_task, code);
+    d->n_it = d->n_task[0] + d->n_task[1] + d->n_task[2];
     int st = cuda_status(cudaMemcpyToSymbol(kLagHalf, w, sizeof w));
-    if (!st) st = upload_vec(m.unzip_src, &d->unzip_src);
+    if (!st) st = upload_vec(code, &d->unzip_src);
+    if (!st) st = upload_vec(tasks, &d->tasks);
+    if (!st && d->n_it > 0 &&
+        cudaMalloc((void**)&d->it, sizeof(double) * NVARS * d->n_it) != cudaSuccess) {
+        cudaGetLastError();
+        st = BSSN_ENOMEM;
+    }
     if (!st) st = upload_vec(m.zip_src, &d->zip_src);
     if (!st) st = upload_vec(m.inject_dst, &d->inject_dst);
     if (!st) st = upload_vec(m.inject_src, &d->inject_src);
@@ -497,6 +603,8 @@ int levels_upload(const LevelMaps& m, LevelsDev* d) {
 
 void levels_free(LevelsDev* d) {
     cudaFree(d->unzip_src);
+    cudaFree(d->tasks);
+    cudaFree(d->it);
     cudaFree(d->zip_src);
     cudaFree(d->inject_dst);
     cudaFree(d->inject_src);
@@ -526,8 +634,18 @@ int launch_levels_unzip(const LevelsDev& d, double* const* P, const double* cons
     int st = vars_out(P, nvars, &p);
     if (!st) st = vars_in(U, nvars, &u);
     if (st || d.n_padded == 0) return st;
-    levels_unzip_kernel<<<grid_for(d.n_padded, 256), 256, 0, s>>>(p, u, nvars, d.unzip_src, d.interp,
-                                                                  d.n_padded);
+    int64_t first = 0;
+    for (int k = 0; k < 3; k++) {  // rows in x, rows in y, points
+        if (d.n_task[k] > 0) {
+            levels_pass_kernel<<<grid_for(d.n_task[k], 256), 256, 0, s>>>(u, d.it, d.n_it, nvars, d.tasks + first,
+                                                                          d.n_task[k], k == 0);
+            st = cuda_status(cudaGetLastError());
+            if (st) return st;
+        }
+        first += d.n_task[k];
+    }
+    levels_unzip_kernel<<<grid_for(d.n_padded, 256), 256, 0, s>>>(p, u, nvars, d.unzip_src, d.it, d.n_it,
+                                                                  d.n_task[0] + d.n_task[1], d.n_padded);
     return cuda_status(cudaGetLastError());
 }
 

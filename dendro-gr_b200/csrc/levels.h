@@ -50,8 +50,28 @@ struct LevelMaps {
     std::vector<InterpEntry> interp;
 };
 
+// One 1-D interpolation of the separable ghost fill: out = sum over k < n
+// of W[j][k] * in[k], in k order (n = 7; n = 1 is a copy with weight 1).
+// The first pass reads zipped nodes and writes x-interpolated rows, the
+// second reads those and writes y-interpolated rows, the third the points;
+// the values are bit-identical to the per-point interpolation (same
+// products, same order of sums), each computed once however many padded
+// points share it.
+struct PassTask {
+    int32_t out;
+    int32_t in[7];
+    int8_t j, n;
+    int16_t pad;
+};
+static_assert(sizeof(PassTask) == 36, "device layout");
+
 struct LevelsDev {
+    // per padded point: >= 0 node, -1 zero, <= -2 third-pass result -2 - src
     int64_t* unzip_src = nullptr;
+    PassTask* tasks = nullptr;  // the three passes back to back
+    int64_t n_task[3] = {0, 0, 0};
+    double* it = nullptr;       // pass results, [var][n_it]
+    int64_t n_it = 0;
     int64_t* zip_src = nullptr;
     int64_t* inject_dst = nullptr;
     int64_t* inject_src = nullptr;

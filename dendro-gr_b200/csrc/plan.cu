@@ -580,6 +580,12 @@ int plan_launches_per_step(Plan* p) {
             rhs += rhs_launch_count(t, nt, m->scratch_zones);
         }
     }
+    if (m->lv) {  // ghost fill, owner gather, stage, one launch per non-empty sync segment
+        int sync = 0;
+        for (const auto* f : {&m->lv->inject_first, &m->lv->prolong_first})
+            for (size_t k = 0; k + 1 < f->size(); k++) sync += (*f)[k + 1] > (*f)[k] ? 1 : 0;
+        return 4 * (rhs + 3 + sync);
+    }
     return 4 * (rhs + (p->direct ? 1 : 2));
 }
 
