@@ -136,3 +136,81 @@ def level_maps(spec: LevelMeshSpec):
     check(lib.bssn_levels_maps(spec.blocks, spec.nblocks, spec.nlevels, M, cb, sizes, unz.ctypes.data,
                                zp.ctypes.data, inj.ctypes.data, pro.ctypes.data, itp.ctypes.data), "levels_maps")
     return dict(unzip_src=unz, zip_src=zp, inject=inj[:ninj], prolong=pro[:npro], interp=itp[:nint])
+
+
+lib.bssn_levels_transfer.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+
+
+def transfer(mesh_from, U_old, mesh_to, U_new, stream=None):
+    """U_new on mesh_to's hierarchy from U_old on mesh_from's (same level-0
+    domain): same-level copies where the old grid has the node, else the
+    coarse node or interpolation from the new coarser level; then the level
+    sync.  Blocking."""
+    check(lib.bssn_levels_transfer(mesh_from.h, _rows(U_old), mesh_to.h, _rows(U_new), NVARS,
+                                   stream_ptr(stream)), "levels_transfer")
+
+
+def regrid_boxes(spec: LevelMeshSpec, flags, max_levels=None):
+    """New level boxes (levels 1.., level-l octants) from per-block refine
+    flags, the box-hierarchy form of the reference's remesh (refine where
+    the test flags a block, coarsen where nothing asks for the level):
+
+    * level l+1 must cover every flagged level-l block, every flagged level-
+      (l+1) block (still wanted fine), and level l+2's new box with one
+      level-(l+1) octant of margin;
+    * each box is widened by one parent octant (two of its own) on every
+      side, aligned to parent octant corners, and clamped inside its parent
+      with one parent octant of margin (flags closer to the domain boundary than that are
+      covered only as far as the clamp allows);
+    * a level nothing asks for is dropped with every finer one; at most one
+      level finer than the current finest is added (max_levels caps the
+      total).
+    Returns [(lo, n)] for levels 1.. (empty: a single-level mesh)."""
+    flags = np.asarray(flags).astype(bool)
+    bl = spec.as_numpy()
+    L = spec.nlevels
+    top = L + 1 if max_levels is None else min(L + 1, max_levels)
+    req = [None] * (top + 1)   # req[l]: (lo, hi) of level l in level-l octants, hi exclusive
+    for l in range(top - 1, 0, -1):
+        parts = []
+        for lev, scale in ((l - 1, 2), (l, 1)):
+            for b in np.nonzero(flags & (bl["level"] == lev))[0]:
+                o = np.asarray(bl["g0"][b], dtype=np.int64) // OCT
+                w = (int(bl["sz"][b]) - 7) // OCT
+                parts.append((o * scale, (o + w) * scale))
+        if req[l + 1] is not None:
+            lo, hi = req[l + 1]
+            parts.append((lo // 2 - 1, -(-hi // 2) + 1))
+        if not parts:
+            continue
+        lo = np.min([p[0] for p in parts], axis=0) - 2
+        hi = np.max([p[1] for p in parts], axis=0) + 2
+        req[l] = (lo - (lo % 2), hi + (hi % 2))
+    boxes = []
+    plo, pn = np.zeros(3, dtype=np.int64), np.asarray(spec.M0, dtype=np.int64)
+    for l in range(1, top):
+        if req[l] is None:
+            break
+        lo, hi = req[l]
+        lo = np.maximum(lo, 2 * (plo + 1))
+        hi = np.minimum(hi, 2 * (plo + pn - 1))
+        if np.any(hi - lo < 2):
+            break
+        boxes.append((tuple(int(x) for x in lo), tuple(int(x) for x in hi - lo)))
+        plo, pn = lo, hi - lo
+    return boxes
+
+
+def remesh(mesh, U, flags, max_levels=None, stream=None):
+    """Regrid a level mesh from refine flags and carry the state over:
+    returns (spec, mesh, U) on the new hierarchy (the old mesh and state are
+    left as they are)."""
+    import torch
+    spec = mesh.spec
+    boxes = regrid_boxes(spec, flags.cpu().numpy() if hasattr(flags, "cpu") else flags, max_levels)
+    from . import Mesh
+    new = generate_levels(spec.M0, boxes, xmin=spec.xmin, L=spec.h0 * OCT * spec.M0[0])
+    nmesh = Mesh(new)
+    V = torch.empty((NVARS, new.n_nodes), dtype=torch.float64, device=U.device)
+    transfer(mesh, U, nmesh, V, stream)
+    return new, nmesh, V

@@ -164,6 +164,15 @@ int bssn_mesh_create_levels(const BssnBlockDesc* blocks, int nblocks, int nlevel
     return 0;
 }
 
+int bssn_levels_transfer(bssn_mesh from, const double* const* u_old_dev, bssn_mesh to,
+                         double* const* u_new_dev, int nvars, bssn_stream_t stream) {
+    if (!from || !to || !u_old_dev || !u_new_dev || nvars < 1 || nvars > bssn::NVARS) return BSSN_EINVAL;
+    if (!from->st->lv || !to->st->lv) return BSSN_ESTATE;  // level meshes only
+    for (int v = 0; v < nvars; v++)
+        if (!u_old_dev[v] || !u_new_dev[v]) return BSSN_EINVAL;
+    return bssn::levels_transfer(*from->st->lv, u_old_dev, *to->st->lv, u_new_dev, nvars, S(stream));
+}
+
 int bssn_mesh_levels_sync(bssn_mesh mesh, double* const* u_dev, int nvars, bssn_stream_t stream) {
     if (!mesh || !u_dev || nvars < 1 || nvars > bssn::NVARS) return BSSN_EINVAL;
     for (int v = 0; v < nvars; v++)

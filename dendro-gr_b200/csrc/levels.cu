@@ -597,6 +597,7 @@ int levels_upload(const LevelMaps& m, LevelsDev* d) {
     d->n_padded = m.n_padded;
     d->inject_first = m.inject_first;
     d->prolong_first = m.prolong_first;
+    d->grids = m.grids;
     if (st) levels_free(d);
     return st;
 }
@@ -677,6 +678,102 @@ int launch_levels_sync(const LevelsDev& d, double* const* U, int nvars, cudaStre
     };
     st = run(d.inject_first, d.inject_dst, d.inject_src);
     return st ? st : run(d.prolong_first, d.prolong_dst, d.prolong_src);
+}
+
+namespace {
+
+__global__ void __launch_bounds__(256) levels_move_kernel(MutVars Un, ConstVars Uo, int nvars,
+                                                          const int64_t* __restrict__ dst,
+                                                          const int64_t* __restrict__ src, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t d = dst[i], s = src[i];
+        for (int v = 0; v < nvars; v++) Un.p[v][d] = __ldg(Uo.p[v] + s);
+    }
+}
+
+bool same_box(const LevelGrid& a, const LevelGrid& b) {
+    for (int d = 0; d < 3; d++)
+        if (a.lo[d] != b.lo[d] || a.n[d] != b.n[d]) return false;
+    return true;
+}
+
+}  // namespace
+
+int levels_transfer(const LevelsDev& from, const double* const* U_old, const LevelsDev& to,
+                    double* const* U_new, int nvars, cudaStream_t s) {
+    if (from.grids.empty() || to.grids.empty() || !same_box(from.grids[0], to.grids[0])) return BSSN_EINVAL;
+    MutVars un;
+    ConstVars uo;
+    int st = vars_out(U_new, nvars, &un);
+    if (!st) st = vars_in(U_old, nvars, &uo);
+    if (st) return st;
+    // the new hierarchy's grids, for its coarse sources
+    LevelMaps nm;
+    nm.grids = to.grids;
+    Builder B{nullptr, 0, (int)to.grids.size(), nullptr, &nm, {}};
+    std::vector<int64_t> cdst, csrc, fdst, fsrc;
+    std::vector<int> cfirst{0}, ffirst{0};
+    for (int l = 0; l < (int)to.grids.size(); l++) {
+        const LevelGrid& g = to.grids[l];
+        const bool has_old = l < (int)from.grids.size();
+        for (int64_t z = 0; z < g.dims[2]; z++)
+            for (int64_t y = 0; y < g.dims[1]; y++)
+                for (int64_t x = 0; x < g.dims[0]; x++) {
+                    const int64_t q[3] = {OCT * int64_t(g.lo[0]) + x, OCT * int64_t(g.lo[1]) + y,
+                                          OCT * int64_t(g.lo[2]) + z};
+                    bool in_old = has_old;
+                    if (has_old) {
+                        const LevelGrid& o = from.grids[l];
+                        for (int d = 0; d < 3; d++)
+                            if (q[d] < OCT * int64_t(o.lo[d]) || q[d] > OCT * int64_t(o.lo[d] + o.n[d])) in_old = false;
+                    }
+                    const int64_t dst = B.node(l, q);
+                    if (in_old) {
+                        const LevelGrid& o = from.grids[l];
+                        cdst.push_back(dst);
+                        csrc.push_back(o.offset + (q[0] - OCT * int64_t(o.lo[0])) +
+                                       int64_t(o.dims[0]) * ((q[1] - OCT * int64_t(o.lo[1])) +
+                                                             int64_t(o.dims[1]) * (q[2] - OCT * int64_t(o.lo[2]))));
+                    } else {
+                        if (l == 0) return BSSN_EINVAL;  // level 0 is the same grid
+                        const int64_t src = B.coarse_source(l, q);
+                        if (src == Builder::kBad) return BSSN_EINVAL;
+                        fdst.push_back(dst);
+                        fsrc.push_back(src);
+                    }
+                }
+        cfirst.push_back((int)cdst.size());
+        ffirst.push_back((int)fdst.size());
+    }
+    int64_t *dcd = nullptr, *dcs = nullptr, *dfd = nullptr, *dfs = nullptr;
+    InterpEntry* dit = nullptr;
+    st = upload_vec(cdst, &dcd);
+    if (!st) st = upload_vec(csrc, &dcs);
+    if (!st) st = upload_vec(fdst, &dfd);
+    if (!st) st = upload_vec(fsrc, &dfs);
+    if (!st) st = upload_vec(nm.interp, &dit);
+    // level by level: copies from the old state, then the nodes filled from
+    // the new level below (complete by then)
+    for (size_t l = 0; l + 1 < cfirst.size() && !st; l++) {
+        const int64_t nc = cfirst[l + 1] - cfirst[l], nf = ffirst[l + 1] - ffirst[l];
+        if (nc > 0) {
+            levels_move_kernel<<<grid_for(nc, 256), 256, 0, s>>>(un, uo, nvars, dcd + cfirst[l], dcs + cfirst[l], nc);
+            st = cuda_status(cudaGetLastError());
+        }
+        if (!st && nf > 0) {
+            levels_copy_kernel<<<grid_for(nf, 256), 256, 0, s>>>(un, nvars, dfd + ffirst[l], dfs + ffirst[l], dit, nf);
+            st = cuda_status(cudaGetLastError());
+        }
+    }
+    if (!st) st = launch_levels_sync(to, U_new, nvars, s);
+    if (!st) st = cuda_status(cudaStreamSynchronize(s));
+    cudaFree(dcd);
+    cudaFree(dcs);
+    cudaFree(dfd);
+    cudaFree(dfs);
+    cudaFree(dit);
+    return st;
 }
 
 }  // namespace bssn

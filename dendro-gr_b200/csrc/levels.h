@@ -80,6 +80,7 @@ struct LevelsDev {
     InterpEntry* interp = nullptr;
     int64_t n_nodes = 0, n_padded = 0;
     std::vector<int> inject_first, prolong_first;  // host copies of the level ranges
+    std::vector<LevelGrid> grids;                  // host copy of the level grids
 };
 
 // Validates the boxes, tiles every level's region (its box minus the next
@@ -103,5 +104,13 @@ int launch_levels_zip(const LevelsDev& d, double* const* Rz, const double* const
                       cudaStream_t s);
 // Restriction (finest level first) then prolongation (coarsest first) on U.
 int launch_levels_sync(const LevelsDev& d, double* const* U, int nvars, cudaStream_t s);
+// Transfer of a state between two hierarchies on the same domain (after a
+// remesh): every node of level l of the new hierarchy takes the old level-l
+// node where the old level l has it, else the coincident node or the
+// interpolation from the new level l-1 (levels in increasing order); then
+// the new hierarchy's sync.  Builds its maps on the host and allocates
+// device memory for them; blocking.
+int levels_transfer(const LevelsDev& from, const double* const* U_old, const LevelsDev& to,
+                    double* const* U_new, int nvars, cudaStream_t s);
 
 }  // namespace bssn

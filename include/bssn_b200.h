@@ -450,6 +450,17 @@ int bssn_mesh_generate_levels(int nlevels, const int32_t M0[3], const BssnLevelB
  * node-wise stage, level sync). */
 int bssn_mesh_create_levels(const BssnBlockDesc* blocks, int nblocks, int nlevels,
                             const int32_t M0[3], const BssnLevelBox* boxes, bssn_mesh* out);
+/* State transfer after a remesh (BSSNCtx::grid_transfer,
+ * BSSN_GR/src/bssnCtx.cpp:1319-1340, which calls dendrolib's
+ * DVec::grid_transfer; the remesh loop is bssnCtx.cpp:393-445): u_new on
+ * the hierarchy `to` from u_old on `from` (same level-0 domain).  Every node
+ * of level l of `to` takes the node of level l of `from` where that grid has
+ * it, otherwise the coincident level-(l-1) node or the ghost-fill
+ * interpolation from `to`'s level l-1 (levels in increasing order); then
+ * the level sync of `to`.  Builds its maps on the host and allocates (and
+ * frees) device memory for them; blocking. */
+int bssn_levels_transfer(bssn_mesh from, const double* const* u_old_dev, bssn_mesh to,
+                         double* const* u_new_dev, int nvars, bssn_stream_t stream);
 /* Level sync of a zipped state (after initial data or any outside update). */
 int bssn_mesh_levels_sync(bssn_mesh mesh, double* const* u_dev, int nvars,
                           bssn_stream_t stream);

@@ -205,3 +205,22 @@ class LevelOracle:
                 out = np.ascontiguousarray(acc + cc * k)
                 self.O.lib.orc_enforce(rows(out), C.c_int64(self.n_nodes), C.c_double(chi_floor))
                 return self.sync(out)
+
+
+def transfer(LO_old, Z_old, LO_new):
+    """State on LO_new's hierarchy from Z_old on LO_old's: per new level,
+    in increasing order, the old same-level node where the old grid has it,
+    else the coincident node or interpolation from the new level below; then
+    the new hierarchy's sync."""
+    Z = np.zeros((NVARS, LO_new.n_nodes))
+    for l, (lo, n) in enumerate(LO_new.boxes):
+        d = LO_new.dims[l]
+        z, y, x = np.meshgrid(*[np.arange(k) for k in d[::-1]], indexing="ij")
+        q = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1) + OCT * lo
+        old = LO_old.in_grid(l, q) if l < LO_old.L else np.zeros(len(q), dtype=bool)
+        if old.any():
+            Z[:, LO_new.node(l, q[old])] = Z_old[:, LO_old.node(l, q[old])]
+        if (~old).any():
+            assert l > 0
+            Z[:, LO_new.node(l, q[~old])] = LO_new.coarse_values(Z, l, q[~old])
+    return LO_new.sync(Z)

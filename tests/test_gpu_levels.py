@@ -83,3 +83,63 @@ def test_rk4_steps_vs_oracle(name, O):
         # levels agree where they coincide: the sync leaves no coarse node
         # under a finer box different from the fine node
         assert np.isfinite(got).all()
+
+
+def test_transfer_bit_exact(O):
+    """Transfer to a different hierarchy (one more level, a moved box) and
+    to the same one (identity) against the oracle's transfer."""
+    from oracle_levels import transfer as otransfer
+    B, LV, spec, LO = setup("two", O)
+    rng = np.random.default_rng(5)
+    Z = LO.sync(rng.standard_normal((24, spec.n_nodes)))
+    m = B.Mesh(spec)
+    for boxes in ([((2, 2, 2), (4, 4, 4)), ((6, 6, 6), (4, 4, 4))], [((2, 2, 2), (4, 2, 4))],
+                  list(MESHES["two"][1])):
+        new = LV.generate_levels(spec.M0, boxes)
+        nm = B.Mesh(new)
+        dV = torch.empty((24, new.n_nodes), dtype=torch.float64, device="cuda")
+        LV.transfer(m, dev(Z), nm, dV)
+        ref = otransfer(LO, Z, LevelOracle(new, O))
+        got = dV.cpu().numpy()
+        assert np.array_equal(got.view(np.uint64), ref.view(np.uint64)), boxes
+        if boxes == list(MESHES["two"][1]):
+            assert np.array_equal(got.view(np.uint64), Z.view(np.uint64))
+        nm.close()
+
+
+def test_remesh_during_evolution(O):
+    """Evolve, flag blocks with the exact wavelet test on the GPU (the 30 %
+    with the largest score ratio), regrid, transfer and evolve on: the GPU
+    against the oracle fed the same flags."""
+    from oracle_levels import transfer as otransfer
+    B, LV, spec, LO = setup("two", O)
+    Z0 = LO.initial_data(eps=1e-8)
+    m = B.Mesh(spec)
+    dt = 0.25 * spec.h
+    prm = B.default_params()
+    dZ = dev(Z0)
+    plan = B.RK4Plan(m, prm, B.PLAN_ENFORCE_STAGES)
+    Z = Z0
+    for _ in range(2):
+        plan.step(dZ, dt)
+        Z = LO.rk4_step(Z, dt, ol.params())
+    P = torch.zeros((24, m.n_unzip), dtype=torch.float64, device="cuda")
+    m.unzip(P, dZ)
+    _, ratio, _ = B.wavelet_scores(m, P, tol=1e-6)
+    r = ratio.cpu().numpy()
+    flags = (r >= np.quantile(r, 0.7)).astype(np.uint8)
+    new, nm, dV = LV.remesh(m, dZ, flags)
+    assert new.nlevels >= 2
+    LN = LevelOracle(new, O)
+    V = otransfer(LO, Z, LN)
+    assert ol.rel_err(V, dV.cpu().numpy()).max() <= 1e-13
+    plan2 = B.RK4Plan(nm, prm, B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
+    dt2 = 0.25 * new.h
+    for _ in range(2):
+        plan2.step(dV, dt2)
+        V = LN.rk4_step(V, dt2, ol.params())
+    torch.cuda.synchronize()
+    assert plan.violations() == 0 and plan2.violations() == 0
+    got = dV.cpu().numpy()
+    assert np.isfinite(got).all()
+    assert ol.rel_err(V, got).max() <= 1e-13

@@ -153,3 +153,24 @@ def test_interpolation_exact_on_degree_6(O):
         got = P[0, int(bl["offset"][b]):int(bl["offset"][b]) + s ** 3]
         worst = max(worst, np.abs(got - exact).max() / np.abs(exact).max())
     assert worst < 1e-12, worst
+
+
+def test_regrid_policy():
+    """Box hierarchies from refine flags: nothing flagged -> one level;
+    flagged finest blocks keep their level and add one finer; a flag near
+    the domain boundary is covered up to the nesting clamp; every result is
+    a valid hierarchy (the generator accepts it)."""
+    M0, boxes = MESHES["two"]
+    spec = LV.generate_levels(M0, boxes)
+    bl = spec.as_numpy()
+    assert LV.regrid_boxes(spec, np.zeros(spec.nblocks)) == []
+    fine = (bl["level"] == 1).astype(np.uint8)
+    nb = LV.regrid_boxes(spec, fine)
+    assert nb[0] == ((2, 2, 2), (4, 4, 4)) and nb[1] == ((6, 6, 6), (4, 4, 4))
+    assert LV.regrid_boxes(spec, fine, max_levels=2) == [((2, 2, 2), (4, 4, 4))]
+    corner = np.zeros(spec.nblocks, dtype=np.uint8)
+    corner[np.nonzero((bl["level"] == 0) & np.all(bl["g0"] == 0, axis=1))[0]] = 1
+    nb = LV.regrid_boxes(spec, corner)
+    assert nb == [((2, 2, 2), (2, 2, 2))]
+    for flags in (fine, corner, np.ones(spec.nblocks)):
+        LV.generate_levels(M0, LV.regrid_boxes(spec, flags))
