@@ -325,6 +325,17 @@ int bssn_constraints_f64(bssn_mesh mesh, const double* const* unzip_dev, double*
     return bssn::launch_constraints(mesh->st, unzip_dev, cons_dev, S(stream));
 }
 
+int bssn_constraints_psi4_f64(bssn_mesh mesh, const double* const* unzip_dev, double* const* cons_dev,
+                              bssn_stream_t stream) {
+    if (!mesh || !unzip_dev || !cons_dev) return BSSN_EINVAL;
+    if (mesh->st->lv) return BSSN_ESTATE;  // single-level node grids only
+    for (int c = 0; c < 6; c++)
+        if (!cons_dev[c]) return BSSN_EINVAL;
+    for (int v = 0; v < bssn::NVARS; v++)
+        if (!unzip_dev[v]) return BSSN_EINVAL;
+    return bssn::launch_constraints(mesh->st, unzip_dev, cons_dev, S(stream), true);
+}
+
 int bssn_constraint_norms_f64(bssn_mesh mesh, const double* const* cons_dev, int ncons,
                               const double xmin[3], double h, const double bh[6],
                               const double radii[2], double* norms_dev, bssn_stream_t stream) {

@@ -89,6 +89,16 @@ __device__ __forceinline__ double Dmix(const Blk& b, const double* u, int inner,
                b.bflag & (1u << (2 * outer + 1)), b.cf[outer]);
 }
 
+// PSI4: also the Weyl scalar psi4 into out.p[4] (real) and out.p[5]
+// (imaginary) -- CodeGen/constraints.py:45-244, per point as
+// BSSN_GR/src/physcon.cpp:72-85 (coordinates ptmin + a h of the padded
+// index a, zero on the z axis): the tetrad r = (x, y, z), theta =
+// (xz, yz, -(x^2 + y^2)), phi = (-y, x, 0) made orthonormal by Gram-Schmidt
+// in the physical metric gt / chi, m = (theta + i phi) / sqrt 2, and
+// psi4 = -(P1 + P2 - P3 - P4) real, P1 + P2 - P3 - P4 imaginary, with
+// P1 = R_ij M^ij, P2 = A_temp At_ij M^ij, P3 = (MR_ij Uu_ij - NR_ij Vv_ij)/chi
+// and P4 the (At r) and d chi products of the definition.
+template <bool PSI4>
 __device__ void constraints_node(const ConstVars& P, const MutVars& out, const BssnBlockDesc& bd,
                                  int64_t q, int gx, int gy, int gz) {
     const int s = bd.sz, N = s - 6;
@@ -237,10 +247,87 @@ __device__ void constraints_node(const ConstVars& P, const MutVars& out, const B
         m -= 2.0 / 3.0 * dK[a];
         out.p[1 + a][node] = m;
     }
+    if constexpr (PSI4) {
+        double crd[3];
+        for (int d = 0; d < 3; d++) {
+            const double h = (bd.ptmax[d] - bd.ptmin[d]) / (s - 1);
+            crd[d] = __dadd_rn(bd.ptmin[d], __dmul_rn((double)b.a[d], h));
+        }
+        if (fabs(crd[0]) <= 1e-7 && fabs(crd[1]) <= 1e-7) {
+            out.p[4][node] = 0.0;
+            out.p[5][node] = 0.0;
+            return;
+        }
+        const double ichi = 1.0 / chi;
+        auto dot = [&](const double* p, const double* r) {  // in the physical metric
+            double t = 0.0;
+            for (int bb = 0; bb < 3; bb++)
+                for (int a = 0; a < 3; a++) t += Gm(a, bb) * ichi * p[a] * r[bb];
+            return t;
+        };
+        const double cx = crd[0], cy = crd[1], cz = crd[2];
+        double rv[3] = {cx, cy, cz}, th[3] = {cx * cz, cy * cz, -(cx * cx + cy * cy)}, ph[3] = {-cy, cx, 0.0};
+        {
+            const double nr = sqrt(dot(rv, rv));
+            for (int a = 0; a < 3; a++) rv[a] /= nr;
+            const double p1 = dot(th, th), p2 = dot(rv, th);
+            for (int a = 0; a < 3; a++) th[a] -= p2 * rv[a];
+            const double nt = sqrt(p1 - p2 * p2);
+            for (int a = 0; a < 3; a++) th[a] /= nt;
+            const double f1 = dot(ph, ph), f2 = dot(rv, ph), f3 = dot(th, ph);
+            for (int a = 0; a < 3; a++) ph[a] -= f2 * rv[a] + f3 * th[a];
+            const double np = sqrt(f1 - f2 * f2 - f3 * f3);
+            for (int a = 0; a < 3; a++) ph[a] /= np;
+        }
+        const double s2 = 1.0 / sqrt(2.0);
+        double mr[3], mi[3];
+        for (int a = 0; a < 3; a++) {
+            mr[a] = th[a] * s2;
+            mi[a] = ph[a] * s2;
+        }
+        double Av[3];
+        for (int a = 0; a < 3; a++) Av[a] = AM(a, 0) * rv[0] + AM(a, 1) * rv[1] + AM(a, 2) * rv[2];
+        double rdc = 0.0, mrdc = 0.0, midc = 0.0, rA = 0.0, mrA = 0.0, miA = 0.0;
+        for (int a = 0; a < 3; a++) {
+            rdc += rv[a] * dchi[a];
+            mrdc += mr[a] * dchi[a];
+            midc += mi[a] * dchi[a];
+            rA += Av[a] * rv[a];
+            mrA += mr[a] * Av[a];
+            miA += mi[a] * Av[a];
+        }
+        const double Atmp = ichi * ichi * (rA + K * chi / 3.0 + 0.5 * rdc);
+        double p1r = 0.0, p1i = 0.0, q2r = 0.0, q2i = 0.0, s3r = 0.0, s3i = 0.0;
+        for (int a = 0; a < 3; a++)
+            for (int bb = 0; bb < 3; bb++) {
+                const double MMab = mr[a] * mr[bb] - mi[a] * mi[bb];
+                const double NNab = mr[a] * mi[bb] + mr[bb] * mi[a];
+                p1r += R[sym(a, bb)] * MMab;
+                p1i += R[sym(a, bb)] * NNab;
+                q2r += AM(a, bb) * MMab;
+                q2i += AM(a, bb) * NNab;
+                const double MRab = mr[a] * rv[bb] - mr[bb] * rv[a];
+                const double NRab = mi[a] * rv[bb] - mi[bb] * rv[a];
+                double uu = 0.0, vv = 0.0;
+                for (int c = 0; c < 3; c++) {
+                    double t = dA[sym(c, a)][bb];
+                    for (int mm = 0; mm < 3; mm++) t += C2[mm][sym(c, a)] * AM(mm, bb);
+                    uu += mr[c] * t;
+                    vv += mi[c] * t;
+                }
+                s3r += MRab * uu - NRab * vv;
+                s3i += NRab * uu + MRab * vv;
+            }
+        const double p4r = ichi * ichi * (mrA * (mrA + 0.5 * mrdc) - miA * (miA + 0.5 * midc));
+        const double p4i = ichi * ichi * (mrA * (miA + 0.5 * midc) + miA * (mrA + 0.5 * mrdc));
+        out.p[4][node] = -(p1r + Atmp * q2r - ichi * s3r - p4r);
+        out.p[5][node] = p1i + Atmp * q2i - ichi * s3i - p4i;
+    }
 }
 
 // One CTA per chunk of up to 1024 interior points of a block, 256 threads
 // striding over it (the node function needs up to 255 registers).
+template <bool PSI4>
 __global__ void __launch_bounds__(256) constraints_kernel(ConstVars P, MutVars out,
                                                           const BssnBlockDesc* __restrict__ blocks,
                                                           const Chunk* __restrict__ chunks, int gx,
@@ -248,7 +335,7 @@ __global__ void __launch_bounds__(256) constraints_kernel(ConstVars P, MutVars o
     const Chunk ck = chunks[blockIdx.x];
     const BssnBlockDesc bd = blocks[ck.blk];
     for (int r = threadIdx.x; r < ck.count; r += blockDim.x)
-        constraints_node(P, out, bd, ck.start + r, gx, gy, gz);
+        constraints_node<PSI4>(P, out, bd, ck.start + r, gx, gy, gz);
 }
 
 }  // namespace
@@ -304,14 +391,18 @@ __global__ void l2_final_kernel(const double* partial, int nblocks, int nc, doub
 }
 
 int launch_constraints(const MeshState* m, const double* const* P, double* const* out,
-                       cudaStream_t s) {
+                       cudaStream_t s, bool psi4) {
     ConstVars p;
     MutVars o = {};
     for (int v = 0; v < NVARS; v++) p.p[v] = P[v];
-    for (int c = 0; c < 4; c++) o.p[c] = out[c];
+    for (int c = 0; c < (psi4 ? 6 : 4); c++) o.p[c] = out[c];
     if (m->n_int_chunks == 0) return 0;
-    constraints_kernel<<<m->n_int_chunks, 256, 0, s>>>(p, o, m->d_blocks, m->d_int_chunks,
-                                                        m->G[0], m->G[1], m->G[2]);
+    if (psi4)
+        constraints_kernel<true><<<m->n_int_chunks, 256, 0, s>>>(p, o, m->d_blocks, m->d_int_chunks,
+                                                                  m->G[0], m->G[1], m->G[2]);
+    else
+        constraints_kernel<false><<<m->n_int_chunks, 256, 0, s>>>(p, o, m->d_blocks, m->d_int_chunks,
+                                                                   m->G[0], m->G[1], m->G[2]);
     return cuda_status(cudaGetLastError());
 }
 

@@ -174,6 +174,14 @@ int bssn_initial_data_f64(double* const* u_dev, const int32_t G[3],
  * cons_dev[0..3] = ham, mom0, mom1, mom2 (owned nodes only). */
 int bssn_constraints_f64(bssn_mesh mesh, const double* const* unzip_dev,
                          double* const* cons_dev, bssn_stream_t stream);
+/* The same constraints plus the Weyl scalar psi4 for gravitational-wave
+ * extraction (the psi4_real / psi4_img outputs of physical_constraints,
+ * BSSN_GR/src/physcon.cpp:12-89; definition CodeGen/constraints.py:45-244):
+ * cons_dev[0..5] = ham, mom0, mom1, mom2, psi4 real, psi4 imaginary (owned
+ * nodes; psi4 = 0 on the z axis, |x|, |y| <= 1e-7, as the reference sets
+ * it). */
+int bssn_constraints_psi4_f64(bssn_mesh mesh, const double* const* unzip_dev,
+                              double* const* cons_dev, bssn_stream_t stream);
 /* Masked L2 norms sqrt(sum c^2 / N) over the zipped nodes farther than
  * radii[0] / radii[1] from the punctures bh = {x1,y1,z1,x2,y2,z2}
  * (computeConstraintL2Norm, BSSN_GR/include/grUtils.tcc:36-134); node

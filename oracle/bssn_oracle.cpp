@@ -912,6 +912,126 @@ void orc_physical_constraints(double** cons, const double** u, unsigned offset,
             }
 }
 
+// The Weyl scalar psi4 (CodeGen/constraints.py:45-244; per point as
+// BSSN_GR/src/physcon.cpp:72-85, zero on the z axis): the tetrad r, theta,
+// phi made orthonormal by Gram-Schmidt in the physical metric gt / chi at
+// the point's coordinates x = pmin + i h, then
+//   psi4 = -(P1 + P2 - P3 - P4) (real part), P1 + P2 - P3 - P4 (imaginary)
+// with P1 = R_ij M^ij, P2 = A_temp At_ij M^ij, P3 = (MR Uu - NR Vv) / chi,
+// P4 the (At r) and d chi products (M, N, MR, NR, Uu, Vv as defined there).
+void orc_psi4(double* re, double* im, const double** u, unsigned offset, const double* pmin,
+              const double* pmax, const unsigned* sz, unsigned bflag, double* ws) {
+    std::vector<double> own;
+    const int nx = sz[0], ny = sz[1], nz = sz[2];
+    const size_t n = (size_t)nx * ny * nz;
+    if (!ws) {
+        own.resize((size_t)WS_SLABS * n);
+        ws = own.data();
+    }
+    const double h[3] = {(pmax[0] - pmin[0]) / (nx - 1),
+                         (pmax[1] - pmin[1]) / (ny - 1),
+                         (pmax[2] - pmin[2]) / (nz - 1)};
+    for (int v = 0; v < NVARS; v++)
+        var_derivs(ws, v, u[v] + offset, h, sz, bflag, kNeedsD2[v]);
+    Pt P;
+    for (int k = 3; k < nz - 3; k++)
+        for (int j = 3; j < ny - 3; j++)
+            for (int i = 3; i < nx - 3; i++) {
+                const size_t pp = i + nx * (j + ny * (size_t)k);
+                const double x = pmin[0] + i * h[0], y = pmin[1] + j * h[1], z = pmin[2] + k * h[2];
+                if (std::fabs(x) <= 1e-7 && std::fabs(y) <= 1e-7) {
+                    re[offset + pp] = 0.0;
+                    im[offset + pp] = 0.0;
+                    continue;
+                }
+                gather_point(P, u, offset, ws, n, pp);
+                double g[3][3], ig[3][3], C1[3][3][3], C2[3][3][3], CalGt[3], R[3][3];
+                conformal_geometry(P, g, ig, C1, C2, CalGt);
+                ricci(P, g, ig, C1, C2, CalGt, R);
+                const double chi = P.u[U_CHI], K = P.u[U_K], ichi = 1.0 / chi;
+                double gd[3][3], A[3][3];
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) {
+                        gd[a][b] = g[a][b] * ichi;
+                        A[a][b] = P.u[U_SYMAT0 + sym(a, b)];
+                    }
+                auto dot = [&](const double* p, const double* q) {
+                    double t = 0.0;
+                    for (int b = 0; b < 3; b++)
+                        for (int a = 0; a < 3; a++) t += gd[a][b] * p[a] * q[b];
+                    return t;
+                };
+                double rv[3] = {x, y, z}, th[3] = {x * z, y * z, -(x * x + y * y)}, ph[3] = {-y, x, 0.0};
+                const double nr = std::sqrt(dot(rv, rv));
+                for (int a = 0; a < 3; a++) rv[a] /= nr;
+                {
+                    const double p1 = dot(th, th), p2 = dot(rv, th);
+                    for (int a = 0; a < 3; a++) th[a] -= p2 * rv[a];
+                    const double nt = std::sqrt(p1 - p2 * p2);
+                    for (int a = 0; a < 3; a++) th[a] /= nt;
+                }
+                {
+                    const double p1 = dot(ph, ph), p2 = dot(rv, ph), p3 = dot(th, ph);
+                    for (int a = 0; a < 3; a++) ph[a] -= p2 * rv[a] + p3 * th[a];
+                    const double np = std::sqrt(p1 - p2 * p2 - p3 * p3);
+                    for (int a = 0; a < 3; a++) ph[a] /= np;
+                }
+                const double s2 = 1.0 / std::sqrt(2.0);
+                double mr[3], mi[3];
+                for (int a = 0; a < 3; a++) {
+                    mr[a] = th[a] * s2;
+                    mi[a] = ph[a] * s2;
+                }
+                double MM[3][3], NN[3][3], MR[3][3], NR[3][3], Uu[3][3], Vv[3][3];
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) {
+                        MM[a][b] = mr[a] * mr[b] - mi[a] * mi[b];
+                        NN[a][b] = mr[a] * mi[b] + mr[b] * mi[a];
+                        MR[a][b] = mr[a] * rv[b] - mr[b] * rv[a];
+                        NR[a][b] = mi[a] * rv[b] - mi[b] * rv[a];
+                        double uu = 0.0, vv = 0.0;
+                        for (int c = 0; c < 3; c++) {
+                            double t = P.d1[U_SYMAT0 + sym(c, a)][b];
+                            for (int m = 0; m < 3; m++) t += C2[m][c][a] * A[m][b];
+                            uu += mr[c] * t;
+                            vv += mi[c] * t;
+                        }
+                        Uu[a][b] = uu;
+                        Vv[a][b] = vv;
+                    }
+                double Av[3];
+                for (int a = 0; a < 3; a++) Av[a] = A[a][0] * rv[0] + A[a][1] * rv[1] + A[a][2] * rv[2];
+                double rdc = 0.0, mrdc = 0.0, midc = 0.0, rA = 0.0, mrA = 0.0, miA = 0.0;
+                for (int a = 0; a < 3; a++) {
+                    rdc += rv[a] * P.d1[U_CHI][a];
+                    mrdc += mr[a] * P.d1[U_CHI][a];
+                    midc += mi[a] * P.d1[U_CHI][a];
+                    rA += Av[a] * rv[a];
+                    mrA += mr[a] * Av[a];
+                    miA += mi[a] * Av[a];
+                }
+                const double Atmp = ichi * ichi * (rA + K * chi / 3.0 + 0.5 * rdc);
+                // symmetric contractions: diagonal + 2 x upper triangle
+                auto sym_dot = [](const double S[3][3], const double T[3][3]) {
+                    double d = S[0][0] * T[0][0] + S[1][1] * T[1][1] + S[2][2] * T[2][2];
+                    return d + 2.0 * (S[0][1] * T[0][1] + S[0][2] * T[0][2] + S[1][2] * T[1][2]);
+                };
+                const double p1r = sym_dot(R, MM), p1i = sym_dot(R, NN);
+                const double p2r = Atmp * sym_dot(A, MM), p2i = Atmp * sym_dot(A, NN);
+                double s3r = 0.0, s3i = 0.0;
+                for (int b = 0; b < 3; b++)
+                    for (int a = 0; a < 3; a++) {
+                        s3r += MR[a][b] * Uu[a][b] - NR[a][b] * Vv[a][b];
+                        s3i += NR[a][b] * Uu[a][b] + MR[a][b] * Vv[a][b];
+                    }
+                const double p3r = ichi * s3r, p3i = ichi * s3i;
+                const double p4r = ichi * ichi * (mrA * (mrA + 0.5 * mrdc) - miA * (miA + 0.5 * midc));
+                const double p4i = ichi * ichi * (mrA * (miA + 0.5 * midc) + miA * (mrA + 0.5 * mrdc));
+                re[offset + pp] = -(p1r + p2r - p3r - p4r);
+                im[offset + pp] = p1i + p2i - p3i - p4i;
+            }
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

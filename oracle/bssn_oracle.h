@@ -111,6 +111,10 @@ int64_t orc_rk4_step(double** u, const OrcBlock* blks, int nblk,
 void orc_physical_constraints(double** cons, const double** u, unsigned offset,
                               const double* pmin, const double* pmax,
                               const unsigned* sz, unsigned bflag, double* ws);
+/* --- The Weyl scalar psi4 (CodeGen/constraints.py:45-244) on a block's
+ * interior: re / im arrays indexed like u (offset + point). */
+void orc_psi4(double* re, double* im, const double** u, unsigned offset, const double* pmin,
+              const double* pmax, const unsigned* sz, unsigned bflag, double* ws);
 
 
 /* --- remesh (the absent dendrolib wavelet transform behind isReMeshWAMR,

@@ -199,6 +199,24 @@ def oracle_constraints(spec, Uz, lib=None):
     return MeshOracle(spec, O).zip(Cz, nvars=4)[:4]
 
 
+def oracle_psi4(spec, Uz, lib=None):
+    """psi4 (real, imaginary) on every zipped node from the padded state Uz,
+    by orc_psi4 per block (pinned to the reference's physconeqs.cpp) and the
+    oracle's zip."""
+    O = lib or oracle()
+    Cz = np.zeros((NVARS, spec.n_unzip))
+    ws = np.zeros(288 * 55 ** 3)
+    for b in range(spec.nblocks):
+        blk = spec.blocks[b]
+        s = int(blk.sz)
+        pm = np.array(blk.ptmin[:])
+        px = np.array(blk.ptmax[:])
+        sz = (C.c_uint * 3)(s, s, s)
+        O.lib.orc_psi4(P(Cz[0]), P(Cz[1]), rows(Uz), C.c_uint(int(blk.offset)), P(pm), P(px), sz,
+                       C.c_uint(int(blk.bflag)), P(ws))
+    return MeshOracle(spec, O).zip(Cz, nvars=2)[:2]
+
+
 def l2_norms(spec, Cn, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0), radii=(0.5, 0.5)):
     """sqrt(sum c^2 / N) over nodes outside both puncture radii
     (grUtils.tcc:36-134)."""

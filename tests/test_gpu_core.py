@@ -238,6 +238,31 @@ def test_autotune_picks_a_tile_per_bucket(B):
 
 
 @pytest.mark.parametrize("mesh", ["uniform", "mix"])
+def test_psi4_vs_oracle(B, O, mesh):
+    """psi4 with the constraints (bssn_constraints_psi4_f64) against the
+    oracle's psi4, which is pinned to the reference's physconeqs.cpp; the
+    punctures sit off the grid's z axis nodes, psi4 = 0 on the axis."""
+    import ctypes as C
+    spec = B.generate_mesh(0, (4, 4, 4)) if mesh == "uniform" else B.generate_mesh(1, (2, 1, 1), seed=1, xmin=-8.25)
+    mo = ol.MeshOracle(spec, O)
+    Uz = mo.unzip(mo.initial_data(eps=1e-6))
+    ref = ol.oracle_psi4(spec, Uz, O)
+    m = B.Mesh(spec)
+    cons = torch.zeros((6, spec.n_nodes), dtype=torch.float64, device="cuda")
+    cp = (C.c_void_p * 6)(*[cons[c].data_ptr() for c in range(6)])
+    B.lib.bssn_constraints_psi4_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    assert B.lib.bssn_constraints_psi4_f64(m.h, B.ptrs(dev(Uz)), cp, B.stream_ptr()) == 0
+    torch.cuda.synchronize()
+    got = cons.cpu().numpy()
+    assert np.abs(ref).max() > 1e-6
+    err = np.abs(got[4:6] - ref).max(axis=1) / np.abs(ref).max(axis=1)
+    assert err.max() <= 1e-12, err
+    # the constraint fields of the same call equal the plain constraints'
+    ham = ol.oracle_constraints(spec, Uz, O)
+    assert ol.rel_err(ham, got[:4]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("mesh", ["uniform", "mix"])
 def test_constraints_and_norms_vs_oracle(B, O, mesh):
     spec = B.generate_mesh(0, (4, 4, 4)) if mesh == "uniform" else B.generate_mesh(1, (2, 1, 1), seed=1, xmin=-8.25)
     mo = ol.MeshOracle(spec, O)

@@ -137,6 +137,28 @@ def test_constraints_vs_reference_live(O, REF, side, bflag):
     assert err.max() <= 1e-12, err
 
 
+@pytest.mark.parametrize("side,bflag", [(13, 0), (19, 63), (31, 21)])
+def test_psi4_vs_reference_live(O, REF, side, bflag):
+    """The restated Weyl scalar psi4 against the reference's own
+    physconeqs.cpp (cons[4], cons[5] of physical_constraints)."""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import make_golden as mg
+    U, pmin, pmax = mg.golden_input(side, 2.0 / (side - 7), (0.1, -1.1, -0.95), 1e-6, 40 + side)
+    n = side ** 3
+    sz = (ol.C.c_uint * 3)(side, side, side)
+    cr = np.zeros((24, n))
+    REF.lib.ref_physical_constraints(ol.rows(cr), ol.rows(U), ol.C.c_uint(0), ol.P(pmin), ol.P(pmax), sz,
+                                     ol.C.c_uint(bflag), ol.P(np.zeros(138 * n)))
+    re, im = np.zeros(n), np.zeros(n)
+    O.lib.orc_psi4(ol.P(re), ol.P(im), ol.rows(U), ol.C.c_uint(0), ol.P(pmin), ol.P(pmax), sz,
+                   ol.C.c_uint(bflag), ol.P(np.zeros(288 * n)))
+    a = mg.interior(cr, side)[4:6]
+    b = mg.interior(np.concatenate([np.stack([re, im]), np.zeros((22, n))]), side)[:2]
+    err = np.abs(a - b).max(axis=1) / np.abs(a).max(axis=1)
+    assert err.max() <= 1e-12, err
+
+
 def test_oracle_rk4_matches_reference_history_10_steps(O, REF):
     """The restated RHS inside the restated RK4 reproduces, after 10 steps,
     the constraint norms of the reference-RHS evolution in the committed
