@@ -182,6 +182,30 @@ int bssn_constraints_f64(bssn_mesh mesh, const double* const* unzip_dev,
  * it). */
 int bssn_constraints_psi4_f64(bssn_mesh mesh, const double* const* unzip_dev,
                               double* const* cons_dev, bssn_stream_t stream);
+/* Gravitational-wave extraction from psi4 (extractFarFieldPsi4,
+ * BSSN_GR/include/gwExtract.h:48-190): psi4 on spheres of the given radii
+ * about the origin, interpolated from a single-level node grid (G nodes per
+ * axis, node (i,j,k) at xmin + (i,j,k) h) with the degree-6 Lagrange
+ * polynomial over the 7^3 nodes of the enclosing octant, and decomposed
+ * into the spin-weight -2 harmonics of every (l, m), l = 2..lmax, m = -l..l
+ * (Goldberg et al. 1967 convention: -2Y_22 = sqrt(5/pi)/8 (1+cos th)^2
+ * e^{2i ph}):
+ *   coeff_dev[(r * nmodes + k) * 2 + {0,1}] = 4 pi sum_p w_p psi4(p)
+ *                                             conj(-2Y_lm(p)),  k in (l, m) order
+ *   l2_dev[r * 2 + {0,1}] = sum_p (Re psi4)^2, sum_p (Im psi4)^2
+ * over n_theta Gauss-Legendre nodes in cos(theta) x 2 n_theta uniform phi
+ * (weights sum to 4 pi; the reference integrates with a Lebedev rule).
+ * Points outside the grid are skipped, as the reference skips points
+ * outside its mesh.  nmodes = bssn_gw_modes_count(lmax).  Allocates and
+ * frees device memory for its tables; blocking. */
+int bssn_gw_modes_count(int lmax);
+int bssn_gw_extract_f64(const double* psi4_re_dev, const double* psi4_im_dev, const int32_t G[3],
+                        const double xmin[3], double h, int nradii, const double* radii, int lmax,
+                        int ntheta, double* coeff_dev, double* l2_dev, bssn_stream_t stream);
+/* The quadrature and harmonics the extraction uses (host only, for tests):
+ * per point theta, phi, weight; y = -2Y_lm per mode and point as (re, im)
+ * pairs, mode-major.  Any output may be NULL. */
+int bssn_gw_sphere_tables(int lmax, int ntheta, double* theta, double* phi, double* w, double* y);
 /* Masked L2 norms sqrt(sum c^2 / N) over the zipped nodes farther than
  * radii[0] / radii[1] from the punctures bh = {x1,y1,z1,x2,y2,z2}
  * (computeConstraintL2Norm, BSSN_GR/include/grUtils.tcc:36-134); node
