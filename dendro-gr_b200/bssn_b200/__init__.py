@@ -195,7 +195,7 @@ class Mesh:
     def __init__(self, spec: MeshSpec):
         self.spec = spec
         self.h = C.c_void_p()
-        if getattr(spec, "boxes", None):  # multi-level mesh (levels.py)
+        if getattr(spec, "boxes", None) or getattr(spec, "patches", None):  # multi-level mesh (levels.py)
             from .levels import create_mesh_handle
             self.h = create_mesh_handle(spec)
         else:

@@ -25,6 +25,10 @@ class BssnLevelBox(C.Structure):
     _fields_ = [("lo", C.c_int32 * 3), ("n", C.c_int32 * 3)]
 
 
+class BssnPatch(C.Structure):
+    _fields_ = [("level", C.c_int32), ("parent", C.c_int32), ("lo", C.c_int32 * 3), ("n", C.c_int32 * 3)]
+
+
 lib.bssn_mesh_generate_levels.argtypes = [C.c_int, C.POINTER(C.c_int32), C.POINTER(BssnLevelBox), C.c_double,
                                           C.c_double, C.POINTER(BssnBlockDesc), C.POINTER(C.c_int),
                                           C.POINTER(C.c_int64)]
@@ -33,6 +37,13 @@ lib.bssn_mesh_create_levels.argtypes = [C.POINTER(BssnBlockDesc), C.c_int, C.c_i
 lib.bssn_mesh_levels_sync.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
 lib.bssn_levels_maps.argtypes = [C.POINTER(BssnBlockDesc), C.c_int, C.c_int, C.POINTER(C.c_int32),
                                  C.POINTER(BssnLevelBox), C.POINTER(C.c_int64)] + [C.c_void_p] * 5
+lib.bssn_mesh_generate_patches.argtypes = [C.c_int, C.POINTER(C.c_int32), C.POINTER(BssnPatch), C.c_double,
+                                           C.c_double, C.POINTER(BssnBlockDesc), C.POINTER(C.c_int),
+                                           C.POINTER(C.c_int64)]
+lib.bssn_mesh_create_patches.argtypes = [C.POINTER(BssnBlockDesc), C.c_int, C.c_int, C.POINTER(C.c_int32),
+                                         C.POINTER(BssnPatch), C.POINTER(C.c_void_p)]
+lib.bssn_patches_maps.argtypes = [C.POINTER(BssnBlockDesc), C.c_int, C.c_int, C.POINTER(C.c_int32),
+                                  C.POINTER(BssnPatch), C.POINTER(C.c_int64)] + [C.c_void_p] * 5
 
 
 @dataclass
@@ -42,26 +53,44 @@ class LevelMeshSpec(MeshSpec):
     M0: tuple = (1, 1, 1)
     boxes: list = field(default_factory=list)   # [(lo, n)] per level, level octants
     h0: float = 0.0
+    # [(level, parent, lo, n)] per patch when a level holds several patches
+    # (None: one patch per level, the boxes above)
+    patches: list = None
+
+    @property
+    def patch_list(self):
+        if self.patches is not None:
+            return list(self.patches)
+        return [(l, l - 1, lo, n) for l, (lo, n) in enumerate(self.boxes)]
 
     @property
     def nlevels(self):
-        return len(self.boxes)
+        return 1 + max(p[0] for p in self.patch_list)
+
+    def c_patches(self):
+        pl = self.patch_list
+        arr = (BssnPatch * len(pl))()
+        for i, (lev, par, lo, n) in enumerate(pl):
+            arr[i].level, arr[i].parent = lev, par
+            arr[i].lo[:] = list(lo)
+            arr[i].n[:] = list(n)
+        return arr
 
     def c_boxes(self):
-        arr = (BssnLevelBox * self.nlevels)()
+        arr = (BssnLevelBox * len(self.boxes))()
         for l, (lo, n) in enumerate(self.boxes):
             arr[l].lo[:] = list(lo)
             arr[l].n[:] = list(n)
         return arr
 
     def grids(self):
-        """Per level: dict(lo, n, dims, offset, h, origin) of its node grid."""
+        """Per patch: dict(level, lo, n, dims, offset, h, origin) of its node grid."""
         out, off = [], 0
-        for l, (lo, n) in enumerate(self.boxes):
+        for lev, _, lo, n in self.patch_list:
             dims = tuple(OCT * int(x) + 1 for x in n)
-            h = self.h0 / 2 ** l
+            h = self.h0 / 2 ** lev
             origin = tuple(self.xmin + OCT * int(lo[d]) * h for d in range(3))
-            out.append(dict(lo=tuple(lo), n=tuple(n), dims=dims, offset=off, h=h, origin=origin))
+            out.append(dict(level=lev, lo=tuple(lo), n=tuple(n), dims=dims, offset=off, h=h, origin=origin))
             off += dims[0] * dims[1] * dims[2]
         return out
 
@@ -88,11 +117,35 @@ def generate_levels(M0, boxes, xmin=-8.0, L=16.0):
     return spec
 
 
+def generate_patches(M0, patches, xmin=-8.0, L=16.0):
+    """Patch 0 = the domain [xmin, xmin + L]^3 in M0 octants per axis;
+    patches = [(level, parent, lo, n)] of patches 1.. (parents listed first,
+    boxes in their own level's octants)."""
+    allp = [(0, -1, (0, 0, 0), tuple(M0))] + [(int(a), int(b), tuple(lo), tuple(n)) for a, b, lo, n in patches]
+    h0 = L / (OCT * M0[0])
+    nlev = 1 + max(p[0] for p in allp)
+    spec = LevelMeshSpec(None, 0, (0, 1, 1), h0 / 2 ** (nlev - 1), xmin, None, None, tuple(M0), [], h0, allp)
+    cp = spec.c_patches()
+    M = (C.c_int32 * 3)(*M0)
+    n = C.c_int(0)
+    nn = C.c_int64(0)
+    check(lib.bssn_mesh_generate_patches(len(allp), M, cp, xmin, h0, None, C.byref(n), C.byref(nn)),
+          "mesh_generate_patches")
+    blocks = (BssnBlockDesc * n.value)()
+    check(lib.bssn_mesh_generate_patches(len(allp), M, cp, xmin, h0, blocks, C.byref(n), C.byref(nn)),
+          "mesh_generate_patches")
+    spec.blocks, spec.nblocks = blocks, n.value
+    spec.G = (int(nn.value), 1, 1)
+    spec.sides = np.array([blocks[b].sz for b in range(n.value)], dtype=np.int32)
+    return spec
+
+
 def create_mesh_handle(spec: LevelMeshSpec):
     h = C.c_void_p()
     M = (C.c_int32 * 3)(*spec.M0)
-    check(lib.bssn_mesh_create_levels(spec.blocks, spec.nblocks, spec.nlevels, M, spec.c_boxes(), C.byref(h)),
-          "mesh_create_levels")
+    pl = spec.patch_list
+    check(lib.bssn_mesh_create_patches(spec.blocks, spec.nblocks, len(pl), M, spec.c_patches(), C.byref(h)),
+          "mesh_create_patches")
     return h
 
 
@@ -108,8 +161,8 @@ def sync(mesh, U, stream=None):
 
 def initial_data_levels(U, spec: LevelMeshSpec, mesh=None, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0), m1=0.5,
                         m2=0.5, chi_floor=1e-4, eps=1e-8, seed=20261203, stream=None):
-    """Brill-Lindquist data on every level grid (noise seed + level), then
-    the level sync when a mesh handle is given."""
+    """Brill-Lindquist data on every patch grid (noise seed + patch index),
+    then the level sync when a mesh handle is given."""
     b = (C.c_double * 6)(*bh)
     for l, g in enumerate(spec.grids()):
         G = (C.c_int32 * 3)(*g["dims"])
@@ -123,18 +176,19 @@ def initial_data_levels(U, spec: LevelMeshSpec, mesh=None, bh=(1.0, 0.0, 0.0, -1
 def level_maps(spec: LevelMeshSpec):
     """The library's host-built maps as numpy arrays (for tests)."""
     M = (C.c_int32 * 3)(*spec.M0)
-    cb = spec.c_boxes()
+    cb = spec.c_patches()
+    npch = len(spec.patch_list)
     sizes = (C.c_int64 * 5)()
-    check(lib.bssn_levels_maps(spec.blocks, spec.nblocks, spec.nlevels, M, cb, sizes, None, None, None, None,
-                               None), "levels_maps")
+    check(lib.bssn_patches_maps(spec.blocks, spec.nblocks, npch, M, cb, sizes, None, None, None, None,
+                                None), "patches_maps")
     npad, nn, ninj, npro, nint = [int(x) for x in sizes]
     unz = np.zeros(npad, dtype=np.int64)
     zp = np.zeros(nn, dtype=np.int64)
     inj = np.zeros((max(ninj, 1), 2), dtype=np.int64)
     pro = np.zeros((max(npro, 1), 2), dtype=np.int64)
     itp = np.zeros((max(nint, 1), 7), dtype=np.int64)
-    check(lib.bssn_levels_maps(spec.blocks, spec.nblocks, spec.nlevels, M, cb, sizes, unz.ctypes.data,
-                               zp.ctypes.data, inj.ctypes.data, pro.ctypes.data, itp.ctypes.data), "levels_maps")
+    check(lib.bssn_patches_maps(spec.blocks, spec.nblocks, npch, M, cb, sizes, unz.ctypes.data,
+                                zp.ctypes.data, inj.ctypes.data, pro.ctypes.data, itp.ctypes.data), "patches_maps")
     return dict(unzip_src=unz, zip_src=zp, inject=inj[:ninj], prolong=pro[:npro], interp=itp[:nint])
 
 

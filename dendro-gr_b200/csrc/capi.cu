@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <vector>
 
 #include "bssn_b200.h"
 #include "bssn_common.cuh"
@@ -141,13 +142,31 @@ int bssn_zip_f64(bssn_mesh mesh, double* const* zip_dev, const double* const* un
     return bssn::launch_zip(mesh->st, zip_dev, unzip_dev, nvars, S(stream));
 }
 
+namespace {
+int create_patch_mesh(const BssnBlockDesc* blocks, int nblocks, const std::vector<bssn::PatchDef>& P,
+                      const int32_t M0[3], bssn_mesh* out);
+}
+
 int bssn_mesh_create_levels(const BssnBlockDesc* blocks, int nblocks, int nlevels, const int32_t M0[3],
                             const BssnLevelBox* boxes, bssn_mesh* out) {
+    return create_patch_mesh(blocks, nblocks, bssn::chain_patches(nlevels, boxes), M0, out);
+}
+
+int bssn_mesh_create_patches(const BssnBlockDesc* blocks, int nblocks, int npatches, const int32_t M0[3],
+                             const BssnPatch* patches, bssn_mesh* out) {
+    return create_patch_mesh(blocks, nblocks, bssn::patches_from(npatches, patches), M0, out);
+}
+
+}  // extern "C"
+
+namespace {
+int create_patch_mesh(const BssnBlockDesc* blocks, int nblocks, const std::vector<bssn::PatchDef>& P,
+                      const int32_t M0[3], bssn_mesh* out) {
     if (!blocks || nblocks <= 0 || !out) return BSSN_EINVAL;
     for (int b = 0; b < nblocks; b++)
         if (!valid_side(blocks[b].sz) || blocks[b].offset < 0) return BSSN_EBLOCKSIZE;
     bssn::LevelMaps maps;
-    int r = bssn::levels_build(blocks, nblocks, nlevels, M0, boxes, &maps);
+    int r = bssn::levels_build(blocks, nblocks, P, M0, &maps);
     if (r) return r;
     // the node "grid" of a multi-level mesh is its concatenated level grids
     const int32_t G[3] = {(int32_t)maps.n_nodes, 1, 1};
@@ -163,6 +182,9 @@ int bssn_mesh_create_levels(const BssnBlockDesc* blocks, int nblocks, int nlevel
     *out = new bssn_mesh_s{st};
     return 0;
 }
+}  // namespace
+
+extern "C" {
 
 int bssn_levels_transfer(bssn_mesh from, const double* const* u_old_dev, bssn_mesh to,
                          double* const* u_new_dev, int nvars, bssn_stream_t stream) {

@@ -58,41 +58,63 @@ struct Box {
     }
 };
 
-int check_boxes(int nlevels, const int32_t M0[3], const BssnLevelBox* boxes) {
-    if (nlevels < 1 || nlevels > 16 || !M0 || !boxes) return BSSN_EINVAL;
+int check_patches(const std::vector<PatchDef>& P, const int32_t M0[3]) {
+    const int np = (int)P.size();
+    if (np < 1 || np > 64 || !M0) return BSSN_EINVAL;
+    if (P[0].level != 0 || P[0].parent != -1) return BSSN_EINVAL;
     for (int d = 0; d < 3; d++)
-        if (M0[d] < 1 || boxes[0].lo[d] != 0 || boxes[0].n[d] != M0[d]) return BSSN_EINVAL;
-    for (int l = 1; l < nlevels; l++)
+        if (M0[d] < 1 || P[0].lo[d] != 0 || P[0].n[d] != M0[d]) return BSSN_EINVAL;
+    for (int p = 1; p < np; p++) {
+        const PatchDef& c = P[p];
+        if (c.parent < 0 || c.parent >= p || c.level < 1 || c.level > 15 || P[c.parent].level != c.level - 1)
+            return BSSN_EINVAL;
+        const PatchDef& q = P[c.parent];
         for (int d = 0; d < 3; d++) {
-            const int lo = boxes[l].lo[d], n = boxes[l].n[d];
+            const int lo = c.lo[d], n = c.n[d];
             if (n < 2 || (lo & 1) || (n & 1)) return BSSN_EINVAL;
-            // inside level l-1's box with one level-(l-1) octant of margin
-            if (lo / 2 < boxes[l - 1].lo[d] + 1 ||
-                lo / 2 + n / 2 > boxes[l - 1].lo[d] + boxes[l - 1].n[d] - 1)
-                return BSSN_EINVAL;
+            // inside the parent with one parent octant of margin
+            if (lo / 2 < q.lo[d] + 1 || lo / 2 + n / 2 > q.lo[d] + q.n[d] - 1) return BSSN_EINVAL;
         }
+        // patches of one level at least one parent octant apart, so no
+        // block's padding reaches another patch of its level
+        for (int r = 1; r < p; r++) {
+            if (P[r].level != c.level) continue;
+            bool apart = false;
+            for (int d = 0; d < 3; d++)
+                apart = apart || c.lo[d] + c.n[d] + 2 <= P[r].lo[d] || P[r].lo[d] + P[r].n[d] + 2 <= c.lo[d];
+            if (!apart) return BSSN_EINVAL;
+        }
+    }
     return 0;
 }
 
-// The next finer level's box in level-l octants (n = 0: none).
-Box child_box(int nlevels, const BssnLevelBox* boxes, int l) {
-    Box c{{0, 0, 0}, {0, 0, 0}};
-    if (l + 1 < nlevels)
-        for (int d = 0; d < 3; d++) {
-            c.lo[d] = boxes[l + 1].lo[d] / 2;
-            c.n[d] = boxes[l + 1].n[d] / 2;
+// The boxes of patch p's children in p's level octants.
+std::vector<Box> children_of(const std::vector<PatchDef>& P, int p) {
+    std::vector<Box> out;
+    for (size_t c = 0; c < P.size(); c++)
+        if (P[c].parent == p) {
+            Box b;
+            for (int d = 0; d < 3; d++) {
+                b.lo[d] = P[c].lo[d] / 2;
+                b.n[d] = P[c].n[d] / 2;
+            }
+            out.push_back(b);
         }
-    return c;
+    return out;
 }
 
 struct Tiler {
-    Box box, child;
-    bool has_child;
+    Box box;
+    std::vector<Box> kids;
     std::vector<std::pair<std::array<int32_t, 3>, int>> cells;  // (origin, width)
     void tile(const int32_t o[3], int w) {
         if (box.disjoint_cell(o, w)) return;
-        if (has_child && child.contains_cell(o, w)) return;
-        if (box.contains_cell(o, w) && (!has_child || child.disjoint_cell(o, w))) {
+        bool apart = true;
+        for (const Box& k : kids) {
+            if (k.contains_cell(o, w)) return;
+            apart = apart && k.disjoint_cell(o, w);
+        }
+        if (box.contains_cell(o, w) && apart) {
             cells.push_back({{o[0], o[1], o[2]}, w});
             return;
         }
@@ -106,25 +128,57 @@ struct Tiler {
 
 }  // namespace
 
-int levels_generate(int nlevels, const int32_t M0[3], const BssnLevelBox* boxes, double xmin,
-                    double h0, BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes) {
+std::vector<PatchDef> chain_patches(int nlevels, const BssnLevelBox* boxes) {
+    std::vector<PatchDef> P;
+    if (nlevels < 1 || nlevels > 16 || !boxes) return P;
+    for (int l = 0; l < nlevels; l++) {
+        PatchDef q;
+        q.level = l;
+        q.parent = l - 1;
+        for (int d = 0; d < 3; d++) {
+            q.lo[d] = boxes[l].lo[d];
+            q.n[d] = boxes[l].n[d];
+        }
+        P.push_back(q);
+    }
+    return P;
+}
+
+std::vector<PatchDef> patches_from(int npatches, const BssnPatch* patches) {
+    std::vector<PatchDef> P;
+    if (npatches < 1 || npatches > 64 || !patches) return P;
+    for (int p = 0; p < npatches; p++) {
+        PatchDef q;
+        q.level = patches[p].level;
+        q.parent = patches[p].parent;
+        for (int d = 0; d < 3; d++) {
+            q.lo[d] = patches[p].lo[d];
+            q.n[d] = patches[p].n[d];
+        }
+        P.push_back(q);
+    }
+    return P;
+}
+
+int levels_generate(const std::vector<PatchDef>& P, const int32_t M0[3], double xmin, double h0,
+                    BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes) {
     if (!nblocks || !n_nodes || !(h0 > 0.0)) return BSSN_EINVAL;
-    int st = check_boxes(nlevels, M0, boxes);
+    int st = check_patches(P, M0);
     if (st) return st;
     int64_t nodes = 0;
-    for (int l = 0; l < nlevels; l++)
-        nodes += int64_t(OCT * boxes[l].n[0] + 1) * (OCT * boxes[l].n[1] + 1) * (OCT * boxes[l].n[2] + 1);
+    for (const PatchDef& q : P)
+        nodes += int64_t(OCT * q.n[0] + 1) * (OCT * q.n[1] + 1) * (OCT * q.n[2] + 1);
     if (nodes >= (int64_t(1) << 31)) return BSSN_ELIMIT;
     int count = 0;
     int64_t offset = 0;
-    for (int l = 0; l < nlevels; l++) {
+    for (int p = 0; p < (int)P.size(); p++) {
+        const int l = P[p].level;
         Tiler t;
         for (int d = 0; d < 3; d++) {
-            t.box.lo[d] = boxes[l].lo[d];
-            t.box.n[d] = boxes[l].n[d];
+            t.box.lo[d] = P[p].lo[d];
+            t.box.n[d] = P[p].n[d];
         }
-        t.child = child_box(nlevels, boxes, l);
-        t.has_child = l + 1 < nlevels;
+        t.kids = children_of(P, p);
         for (int32_t z = t.box.lo[2]; z < t.box.lo[2] + t.box.n[2]; z += 8)
             for (int32_t y = t.box.lo[1]; y < t.box.lo[1] + t.box.n[1]; y += 8)
                 for (int32_t x = t.box.lo[0]; x < t.box.lo[0] + t.box.n[0]; x += 8) {
@@ -161,12 +215,11 @@ int levels_generate(int nlevels, const int32_t M0[3], const BssnLevelBox* boxes,
 
 namespace {
 
+// Index arguments named l below are patch indices (one patch per level for
+// meshes described by a box per level).
 struct Builder {
-    const BssnBlockDesc* blocks;
-    int nblocks, L;
-    const BssnLevelBox* boxes;
     LevelMaps* out;
-    std::vector<std::vector<int32_t>> owner;  // per level: block of each octant of its box, -1 none
+    std::vector<std::vector<int32_t>> owner;  // per patch: block of each octant of its box, -1 none
 
     const LevelGrid& grid(int l) const { return out->grids[l]; }
     bool in_grid(int l, const int64_t q[3]) const {
@@ -188,9 +241,10 @@ struct Builder {
         const int64_t i = (t[0] - g.lo[0]) + int64_t(g.n[0]) * ((t[1] - g.lo[1]) + int64_t(g.n[1]) * (t[2] - g.lo[2]));
         return owner[l][i];
     }
-    // Source of level-l index q outside level l's box (l >= 1): the coarse
-    // node or an interpolation entry.  kBad when the coarse stencil would
-    // leave level l-1's grid (cannot happen for valid boxes).
+    // Source of patch l's level index q outside its box (level >= 1): the
+    // parent's coincident node or an interpolation entry.  kBad when the
+    // coarse stencil would leave the parent's grid (cannot happen for valid
+    // patches).
     static constexpr int64_t kBad = std::numeric_limits<int64_t>::min();
     int64_t coarse_source(int l, const int64_t q[3]) {
         int64_t c[3];
@@ -210,12 +264,13 @@ struct Builder {
         }
         int64_t hi[3];
         for (int d = 0; d < 3; d++) hi[d] = c[d] + (j[d] >= 0 ? OCT : 0);
-        if (!in_grid(l - 1, c) || !in_grid(l - 1, hi)) return kBad;
-        if (!odd) return node(l - 1, c);
+        const int pa = grid(l).parent;
+        if (pa < 0 || !in_grid(pa, c) || !in_grid(pa, hi)) return kBad;
+        if (!odd) return node(pa, c);
         InterpEntry e;
         std::memset(&e, 0, sizeof e);
-        e.base = node(l - 1, c);
-        const LevelGrid& g = grid(l - 1);
+        e.base = node(pa, c);
+        const LevelGrid& g = grid(pa);
         e.stride[0] = 1;
         e.stride[1] = g.dims[0];
         e.stride[2] = g.dims[0] * g.dims[1];
@@ -225,73 +280,94 @@ struct Builder {
     }
     int64_t padded_source(int l, const int64_t q[3]) {
         if (in_grid(l, q)) return node(l, q);
-        if (l == 0) return -1;  // outside the domain
+        if (grid(l).level == 0) return -1;  // outside the domain
         return coarse_source(l, q);
     }
 };
 
 }  // namespace
 
-int levels_build(const BssnBlockDesc* blocks, int nblocks, int nlevels, const int32_t M0[3],
-                 const BssnLevelBox* boxes, LevelMaps* out) {
+int levels_build(const BssnBlockDesc* blocks, int nblocks, const std::vector<PatchDef>& P,
+                 const int32_t M0[3], LevelMaps* out) {
     if (!blocks || nblocks <= 0 || !out) return BSSN_EINVAL;
-    int st = check_boxes(nlevels, M0, boxes);
+    int st = check_patches(P, M0);
     if (st) return st;
     *out = LevelMaps();
+    const int np = (int)P.size();
+    int maxlev = 0;
     int64_t off = 0;
-    for (int l = 0; l < nlevels; l++) {
+    for (int p = 0; p < np; p++) {
         LevelGrid g;
         for (int d = 0; d < 3; d++) {
-            g.lo[d] = boxes[l].lo[d];
-            g.n[d] = boxes[l].n[d];
+            g.lo[d] = P[p].lo[d];
+            g.n[d] = P[p].n[d];
             g.dims[d] = OCT * g.n[d] + 1;
         }
+        g.level = P[p].level;
+        g.parent = P[p].parent;
         g.offset = off;
         off += int64_t(g.dims[0]) * g.dims[1] * g.dims[2];
         out->grids.push_back(g);
+        maxlev = std::max(maxlev, g.level);
     }
     if (off >= (int64_t(1) << 31)) return BSSN_ELIMIT;
     out->n_nodes = off;
-    Builder B{blocks, nblocks, nlevels, boxes, out, {}};
-    B.owner.resize(nlevels);
-    for (int l = 0; l < nlevels; l++)
-        B.owner[l].assign(size_t(boxes[l].n[0]) * boxes[l].n[1] * boxes[l].n[2], -1);
+    Builder B{out, {}};
+    B.owner.resize(np);
+    std::vector<std::vector<Box>> kids(np);
+    for (int p = 0; p < np; p++) {
+        B.owner[p].assign(size_t(P[p].n[0]) * P[p].n[1] * P[p].n[2], -1);
+        kids[p] = children_of(P, p);
+    }
+    auto box_of = [&](int p) {
+        Box b;
+        for (int d = 0; d < 3; d++) {
+            b.lo[d] = P[p].lo[d];
+            b.n[d] = P[p].n[d];
+        }
+        return b;
+    };
+    // each block belongs to the patch of its level that holds its octants
+    std::vector<int> patch_of(nblocks, -1);
     int64_t npad = 0;
     for (int b = 0; b < nblocks; b++) {
         const BssnBlockDesc& k = blocks[b];
         const int w = (k.sz - 7) / OCT;
-        if (k.level < 0 || k.level >= nlevels || k.sz != OCT * w + 7 || (w != 1 && w != 2 && w != 4 && w != 8) ||
+        if (k.level < 0 || k.level > maxlev || k.sz != OCT * w + 7 || (w != 1 && w != 2 && w != 4 && w != 8) ||
             k.offset < 0)
             return BSSN_EINVAL;
-        const Box child = child_box(nlevels, boxes, k.level);
         int32_t o[3];
         for (int d = 0; d < 3; d++) {
             if (k.g0[d] % OCT) return BSSN_EINVAL;
             o[d] = k.g0[d] / OCT;
         }
-        Box box{{boxes[k.level].lo[0], boxes[k.level].lo[1], boxes[k.level].lo[2]},
-                {boxes[k.level].n[0], boxes[k.level].n[1], boxes[k.level].n[2]}};
-        if (!box.contains_cell(o, w) || (k.level + 1 < nlevels && !child.disjoint_cell(o, w)))
-            return BSSN_EINVAL;
+        int p = -1;
+        for (int q = 0; q < np && p < 0; q++)
+            if (P[q].level == k.level && box_of(q).contains_cell(o, w)) p = q;
+        if (p < 0) return BSSN_EINVAL;
+        for (const Box& c : kids[p])
+            if (!c.disjoint_cell(o, w)) return BSSN_EINVAL;
+        patch_of[b] = p;
+        const Box box = box_of(p);
         for (int z = 0; z < w; z++)
             for (int y = 0; y < w; y++)
                 for (int x = 0; x < w; x++) {
                     const int64_t i = (o[0] + x - box.lo[0]) +
                                       int64_t(box.n[0]) * ((o[1] + y - box.lo[1]) + int64_t(box.n[1]) * (o[2] + z - box.lo[2]));
-                    if (B.owner[k.level][i] >= 0) return BSSN_EINVAL;  // overlapping blocks
-                    B.owner[k.level][i] = b;
+                    if (B.owner[p][i] >= 0) return BSSN_EINVAL;  // overlapping blocks
+                    B.owner[p][i] = b;
                 }
         npad = std::max<int64_t>(npad, k.offset + int64_t(k.sz) * k.sz * k.sz);
     }
-    // every octant of every level's region has a block
-    for (int l = 0; l < nlevels; l++) {
-        const Box child = child_box(nlevels, boxes, l);
-        for (int64_t i = 0; i < (int64_t)B.owner[l].size(); i++) {
-            const int32_t t[3] = {int32_t(boxes[l].lo[0] + i % boxes[l].n[0]),
-                                  int32_t(boxes[l].lo[1] + (i / boxes[l].n[0]) % boxes[l].n[1]),
-                                  int32_t(boxes[l].lo[2] + i / (int64_t(boxes[l].n[0]) * boxes[l].n[1]))};
-            const bool under = l + 1 < nlevels && child.contains_cell(t, 1);
-            if (under != (B.owner[l][i] < 0)) return BSSN_EINVAL;
+    // every octant of every patch's region has a block
+    for (int p = 0; p < np; p++) {
+        for (int64_t i = 0; i < (int64_t)B.owner[p].size(); i++) {
+            const int32_t t[3] = {int32_t(P[p].lo[0] + i % P[p].n[0]),
+                                  int32_t(P[p].lo[1] + (i / P[p].n[0]) % P[p].n[1]),
+                                  int32_t(P[p].lo[2] + i / (int64_t(P[p].n[0]) * P[p].n[1]))};
+            bool under = false;
+            for (const Box& c : kids[p]) under = under || c.contains_cell(t, 1);
+            if (under != (B.owner[p][i] < 0)) return BSSN_EINVAL;
         }
     }
     out->n_padded = npad;
@@ -304,37 +380,44 @@ int levels_build(const BssnBlockDesc* blocks, int nblocks, int nlevels, const in
             for (int r = 0; r < s; r++)
                 for (int a = 0; a < s; a++) {
                     const int64_t q[3] = {int64_t(k.g0[0]) + a - 3, int64_t(k.g0[1]) + r - 3, int64_t(k.g0[2]) + c - 3};
-                    const int64_t src = B.padded_source(k.level, q);
+                    const int64_t src = B.padded_source(patch_of[b], q);
                     if (src == Builder::kBad) return BSSN_EINVAL;
                     out->unzip_src[size_t(k.offset + a + int64_t(s) * (r + int64_t(s) * c))] = src;
                 }
     }
     // owners
     out->zip_src.assign(size_t(out->n_nodes), -1);
-    for (int l = 0; l < nlevels; l++) {
-        const LevelGrid& g = out->grids[l];
-        const Box child = child_box(nlevels, boxes, l);
-        const bool has_child = l + 1 < nlevels;
+    for (int p = 0; p < np; p++) {
+        const LevelGrid& g = out->grids[p];
         for (int64_t z = 0; z < g.dims[2]; z++)
             for (int64_t y = 0; y < g.dims[1]; y++)
                 for (int64_t x = 0; x < g.dims[0]; x++) {
                     const int64_t q[3] = {OCT * int64_t(g.lo[0]) + x, OCT * int64_t(g.lo[1]) + y,
                                           OCT * int64_t(g.lo[2]) + z};
                     const int64_t e[3] = {x, y, z};
-                    bool boundary = false, inside_child = has_child;
-                    for (int d = 0; d < 3; d++) {
-                        if (l > 0 && (e[d] == 0 || e[d] == g.dims[d] - 1)) boundary = true;
-                        if (has_child && !(q[d] > OCT * int64_t(child.lo[d]) && q[d] < OCT * int64_t(child.lo[d] + child.n[d])))
-                            inside_child = false;
+                    bool boundary = false;
+                    for (int d = 0; d < 3; d++)
+                        if (g.level > 0 && (e[d] == 0 || e[d] == g.dims[d] - 1)) boundary = true;
+                    bool inside_child = false;
+                    for (const Box& c : kids[p]) {
+                        bool in = true;
+                        for (int d = 0; d < 3; d++)
+                            in = in && q[d] > OCT * int64_t(c.lo[d]) && q[d] < OCT * int64_t(c.lo[d] + c.n[d]);
+                        inside_child = inside_child || in;
                     }
                     if (boundary || inside_child) continue;
                     int64_t t[3];
                     for (int d = 0; d < 3; d++) t[d] = std::min<int64_t>(q[d] / OCT, g.lo[d] + g.n[d] - 1);
-                    int32_t b = B.owner_of(l, t);
-                    if (b < 0 && has_child) {  // on the finer box's boundary: the octant below
-                        for (int d = 0; d < 3; d++)
-                            if (q[d] == OCT * int64_t(child.lo[d])) t[d] -= 1;
-                        b = B.owner_of(l, t);
+                    int32_t b = B.owner_of(p, t);
+                    if (b < 0) {  // on a finer patch's boundary: the octant below
+                        for (const Box& c : kids[p]) {
+                            const int32_t ti[3] = {int32_t(t[0]), int32_t(t[1]), int32_t(t[2])};
+                            if (!c.contains_cell(ti, 1)) continue;
+                            for (int d = 0; d < 3; d++)
+                                if (q[d] == OCT * int64_t(c.lo[d])) t[d] -= 1;
+                            break;
+                        }
+                        b = B.owner_of(p, t);
                     }
                     if (b < 0) return BSSN_EINVAL;
                     const BssnBlockDesc& k = blocks[b];
@@ -343,41 +426,47 @@ int levels_build(const BssnBlockDesc* blocks, int nblocks, int nlevels, const in
                         loc[d] = q[d] - k.g0[d] + 3;
                         if (loc[d] < 3 || loc[d] > k.sz - 4) return BSSN_EINVAL;
                     }
-                    out->zip_src[size_t(B.node(l, q))] =
+                    out->zip_src[size_t(B.node(p, q))] =
                         k.offset + loc[0] + int64_t(k.sz) * (loc[1] + int64_t(k.sz) * loc[2]);
                 }
     }
-    // restriction, finest level first
+    // restriction, finest level first (one segment per level)
     out->inject_first.push_back(0);
-    for (int l = nlevels - 1; l >= 1; l--) {
-        const LevelGrid& g = out->grids[l];
-        // level l's box in level l-1 node index: [3 lo, 3 (lo + n)]
-        for (int64_t z = 3 * int64_t(g.lo[2]) + 1; z < 3 * int64_t(g.lo[2] + g.n[2]); z++)
-            for (int64_t y = 3 * int64_t(g.lo[1]) + 1; y < 3 * int64_t(g.lo[1] + g.n[1]); y++)
-                for (int64_t x = 3 * int64_t(g.lo[0]) + 1; x < 3 * int64_t(g.lo[0] + g.n[0]); x++) {
-                    const int64_t c[3] = {x, y, z}, f[3] = {2 * x, 2 * y, 2 * z};
-                    out->inject_dst.push_back(B.node(l - 1, c));
-                    out->inject_src.push_back(B.node(l, f));
-                }
+    for (int lev = maxlev; lev >= 1; lev--) {
+        for (int p = 0; p < np; p++) {
+            if (P[p].level != lev) continue;
+            const LevelGrid& g = out->grids[p];
+            // the patch's box in its parent's node index: [3 lo, 3 (lo + n)]
+            for (int64_t z = 3 * int64_t(g.lo[2]) + 1; z < 3 * int64_t(g.lo[2] + g.n[2]); z++)
+                for (int64_t y = 3 * int64_t(g.lo[1]) + 1; y < 3 * int64_t(g.lo[1] + g.n[1]); y++)
+                    for (int64_t x = 3 * int64_t(g.lo[0]) + 1; x < 3 * int64_t(g.lo[0] + g.n[0]); x++) {
+                        const int64_t c[3] = {x, y, z}, f[3] = {2 * x, 2 * y, 2 * z};
+                        out->inject_dst.push_back(B.node(g.parent, c));
+                        out->inject_src.push_back(B.node(p, f));
+                    }
+        }
         out->inject_first.push_back((int)out->inject_dst.size());
     }
-    // prolongation of box boundaries, coarsest first
+    // prolongation of patch boundaries, coarsest level first
     out->prolong_first.push_back(0);
-    for (int l = 1; l < nlevels; l++) {
-        const LevelGrid& g = out->grids[l];
-        for (int64_t z = 0; z < g.dims[2]; z++)
-            for (int64_t y = 0; y < g.dims[1]; y++)
-                for (int64_t x = 0; x < g.dims[0]; x++) {
-                    const bool bd = x == 0 || y == 0 || z == 0 || x == g.dims[0] - 1 || y == g.dims[1] - 1 ||
-                                    z == g.dims[2] - 1;
-                    if (!bd) continue;
-                    const int64_t q[3] = {OCT * int64_t(g.lo[0]) + x, OCT * int64_t(g.lo[1]) + y,
-                                          OCT * int64_t(g.lo[2]) + z};
-                    const int64_t src = B.coarse_source(l, q);
-                    if (src == Builder::kBad) return BSSN_EINVAL;
-                    out->prolong_dst.push_back(B.node(l, q));
-                    out->prolong_src.push_back(src);
-                }
+    for (int lev = 1; lev <= maxlev; lev++) {
+        for (int p = 0; p < np; p++) {
+            if (P[p].level != lev) continue;
+            const LevelGrid& g = out->grids[p];
+            for (int64_t z = 0; z < g.dims[2]; z++)
+                for (int64_t y = 0; y < g.dims[1]; y++)
+                    for (int64_t x = 0; x < g.dims[0]; x++) {
+                        const bool bd = x == 0 || y == 0 || z == 0 || x == g.dims[0] - 1 || y == g.dims[1] - 1 ||
+                                        z == g.dims[2] - 1;
+                        if (!bd) continue;
+                        const int64_t q[3] = {OCT * int64_t(g.lo[0]) + x, OCT * int64_t(g.lo[1]) + y,
+                                              OCT * int64_t(g.lo[2]) + z};
+                        const int64_t src = B.coarse_source(p, q);
+                        if (src == Builder::kBad) return BSSN_EINVAL;
+                        out->prolong_dst.push_back(B.node(p, q));
+                        out->prolong_src.push_back(src);
+                    }
+        }
         out->prolong_first.push_back((int)out->prolong_dst.size());
     }
     return 0;
@@ -711,32 +800,36 @@ int levels_transfer(const LevelsDev& from, const double* const* U_old, const Lev
     // the new hierarchy's grids, for its coarse sources
     LevelMaps nm;
     nm.grids = to.grids;
-    Builder B{nullptr, 0, (int)to.grids.size(), nullptr, &nm, {}};
+    Builder B{&nm, {}};
     std::vector<int64_t> cdst, csrc, fdst, fsrc;
     std::vector<int> cfirst{0}, ffirst{0};
     for (int l = 0; l < (int)to.grids.size(); l++) {
         const LevelGrid& g = to.grids[l];
-        const bool has_old = l < (int)from.grids.size();
         for (int64_t z = 0; z < g.dims[2]; z++)
             for (int64_t y = 0; y < g.dims[1]; y++)
                 for (int64_t x = 0; x < g.dims[0]; x++) {
                     const int64_t q[3] = {OCT * int64_t(g.lo[0]) + x, OCT * int64_t(g.lo[1]) + y,
                                           OCT * int64_t(g.lo[2]) + z};
-                    bool in_old = has_old;
-                    if (has_old) {
-                        const LevelGrid& o = from.grids[l];
+                    // an old patch of the same level holding the node (patches
+                    // of one level are apart, so at most one does)
+                    int op = -1;
+                    for (int r = 0; r < (int)from.grids.size() && op < 0; r++) {
+                        const LevelGrid& o = from.grids[r];
+                        if (o.level != g.level) continue;
+                        bool in = true;
                         for (int d = 0; d < 3; d++)
-                            if (q[d] < OCT * int64_t(o.lo[d]) || q[d] > OCT * int64_t(o.lo[d] + o.n[d])) in_old = false;
+                            in = in && q[d] >= OCT * int64_t(o.lo[d]) && q[d] <= OCT * int64_t(o.lo[d] + o.n[d]);
+                        if (in) op = r;
                     }
                     const int64_t dst = B.node(l, q);
-                    if (in_old) {
-                        const LevelGrid& o = from.grids[l];
+                    if (op >= 0) {
+                        const LevelGrid& o = from.grids[op];
                         cdst.push_back(dst);
                         csrc.push_back(o.offset + (q[0] - OCT * int64_t(o.lo[0])) +
                                        int64_t(o.dims[0]) * ((q[1] - OCT * int64_t(o.lo[1])) +
                                                              int64_t(o.dims[1]) * (q[2] - OCT * int64_t(o.lo[2]))));
                     } else {
-                        if (l == 0) return BSSN_EINVAL;  // level 0 is the same grid
+                        if (g.level == 0) return BSSN_EINVAL;  // level 0 is the same grid
                         const int64_t src = B.coarse_source(l, q);
                         if (src == Builder::kBad) return BSSN_EINVAL;
                         fdst.push_back(dst);
@@ -778,20 +871,9 @@ int levels_transfer(const LevelsDev& from, const double* const* U_old, const Lev
 
 }  // namespace bssn
 
-extern "C" {
-
-int bssn_mesh_generate_levels(int nlevels, const int32_t M0[3], const BssnLevelBox* boxes, double xmin,
-                              double h0, BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes) {
-    return bssn::levels_generate(nlevels, M0, boxes, xmin, h0, blocks, nblocks, n_nodes);
-}
-
-int bssn_levels_maps(const BssnBlockDesc* blocks, int nblocks, int nlevels, const int32_t M0[3],
-                     const BssnLevelBox* boxes, int64_t sizes[5], int64_t* unzip_src, int64_t* zip_src,
-                     int64_t* inject, int64_t* prolong, int64_t* interp) {
-    if (!sizes) return BSSN_EINVAL;
-    bssn::LevelMaps m;
-    const int st = bssn::levels_build(blocks, nblocks, nlevels, M0, boxes, &m);
-    if (st) return st;
+// Host copies of the maps for the C ABI (bssn_levels_maps, bssn_patches_maps).
+static int export_maps(const bssn::LevelMaps& m, int64_t sizes[5], int64_t* unzip_src, int64_t* zip_src,
+                int64_t* inject, int64_t* prolong, int64_t* interp) {
     sizes[0] = m.n_padded;
     sizes[1] = m.n_nodes;
     sizes[2] = (int64_t)m.inject_dst.size();
@@ -820,6 +902,36 @@ int bssn_levels_maps(const BssnBlockDesc* blocks, int nblocks, int nlevels, cons
             }
         }
     return 0;
+}
+
+extern "C" {
+
+int bssn_mesh_generate_levels(int nlevels, const int32_t M0[3], const BssnLevelBox* boxes, double xmin,
+                              double h0, BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes) {
+    return bssn::levels_generate(bssn::chain_patches(nlevels, boxes), M0, xmin, h0, blocks, nblocks, n_nodes);
+}
+
+int bssn_mesh_generate_patches(int npatches, const int32_t M0[3], const BssnPatch* patches, double xmin,
+                               double h0, BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes) {
+    return bssn::levels_generate(bssn::patches_from(npatches, patches), M0, xmin, h0, blocks, nblocks, n_nodes);
+}
+
+int bssn_levels_maps(const BssnBlockDesc* blocks, int nblocks, int nlevels, const int32_t M0[3],
+                     const BssnLevelBox* boxes, int64_t sizes[5], int64_t* unzip_src, int64_t* zip_src,
+                     int64_t* inject, int64_t* prolong, int64_t* interp) {
+    if (!sizes) return BSSN_EINVAL;
+    bssn::LevelMaps m;
+    const int st = bssn::levels_build(blocks, nblocks, bssn::chain_patches(nlevels, boxes), M0, &m);
+    return st ? st : export_maps(m, sizes, unzip_src, zip_src, inject, prolong, interp);
+}
+
+int bssn_patches_maps(const BssnBlockDesc* blocks, int nblocks, int npatches, const int32_t M0[3],
+                      const BssnPatch* patches, int64_t sizes[5], int64_t* unzip_src, int64_t* zip_src,
+                      int64_t* inject, int64_t* prolong, int64_t* interp) {
+    if (!sizes) return BSSN_EINVAL;
+    bssn::LevelMaps m;
+    const int st = bssn::levels_build(blocks, nblocks, bssn::patches_from(npatches, patches), M0, &m);
+    return st ? st : export_maps(m, sizes, unzip_src, zip_src, inject, prolong, interp);
 }
 
 }  // extern "C"

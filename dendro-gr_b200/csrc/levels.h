@@ -20,6 +20,14 @@ struct LevelGrid {
     int32_t lo[3], n[3];
     int64_t offset;
     int32_t dims[3];
+    int32_t level = 0, parent = -1;  // the patch's level and parent patch
+};
+
+// One patch of the hierarchy (the public BssnPatch): a box of octants of
+// its level inside its parent patch.
+struct PatchDef {
+    int32_t level, parent;
+    int32_t lo[3], n[3];
 };
 
 // A point interpolated from the next coarser level: along every axis with
@@ -83,16 +91,19 @@ struct LevelsDev {
     std::vector<LevelGrid> grids;                  // host copy of the level grids
 };
 
-// Validates the boxes, tiles every level's region (its box minus the next
-// finer box) with blocks of 1, 2, 4 or 8 octants per axis, and lays them out
+// Validates the patches, tiles every patch's region (its box minus its
+// children's boxes) with blocks of 1, 2, 4 or 8 octants per axis, and lays them out
 // (offsets, sides 13/19/31/55, level, origin g0 in the level's node index,
 // ptmin / ptmax, physical-boundary flags on level 0).  blocks == NULL: count
 // only.  n_nodes: total zipped nodes over all levels.
-int levels_generate(int nlevels, const int32_t M0[3], const BssnLevelBox* boxes, double xmin,
-                    double h0, BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes);
+int levels_generate(const std::vector<PatchDef>& P, const int32_t M0[3], double xmin, double h0,
+                    BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes);
 // The maps of a generated mesh (host only).
-int levels_build(const BssnBlockDesc* blocks, int nblocks, int nlevels, const int32_t M0[3],
-                 const BssnLevelBox* boxes, LevelMaps* out);
+int levels_build(const BssnBlockDesc* blocks, int nblocks, const std::vector<PatchDef>& P,
+                 const int32_t M0[3], LevelMaps* out);
+// One patch per level from a box per level (patch l's parent is l - 1).
+std::vector<PatchDef> chain_patches(int nlevels, const BssnLevelBox* boxes);
+std::vector<PatchDef> patches_from(int npatches, const BssnPatch* patches);
 int levels_upload(const LevelMaps& m, LevelsDev* d);
 void levels_free(LevelsDev* d);
 

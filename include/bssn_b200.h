@@ -468,6 +468,30 @@ typedef struct BssnLevelBox {
     int32_t lo[3];          /* first octant, in level-l octants */
     int32_t n[3];           /* octants per axis */
 } BssnLevelBox;
+/* Several refined regions per level (octree-like refinement around
+ * separate sources, e.g. each puncture): a patch hierarchy.  Patch 0 is
+ * level 0 (the domain, parent -1); every other patch has a level >= 1, a
+ * parent patch of the level below listed before it, and a box of its own
+ * level's octants inside the parent's box with one parent octant of margin
+ * (even lo and n); patches of one level lie at least one parent octant apart.
+ * A patch's region is its box minus its children's boxes.  Every level rule
+ * above holds per patch (its own node grid; ghost fill from the patch or
+ * its parent; restriction into the parent; prolongation of its boundary
+ * from the parent).  A box per level is the chain of patches l, parent l-1. */
+typedef struct BssnPatch {
+    int32_t level;
+    int32_t parent;         /* patch index, -1 for patch 0 */
+    int32_t lo[3];
+    int32_t n[3];
+} BssnPatch;
+int bssn_mesh_generate_patches(int npatches, const int32_t M0[3], const BssnPatch* patches,
+                               double xmin, double h0, BssnBlockDesc* blocks, int* nblocks,
+                               int64_t* n_nodes);
+int bssn_mesh_create_patches(const BssnBlockDesc* blocks, int nblocks, int npatches,
+                             const int32_t M0[3], const BssnPatch* patches, bssn_mesh* out);
+int bssn_patches_maps(const BssnBlockDesc* blocks, int nblocks, int npatches, const int32_t M0[3],
+                      const BssnPatch* patches, int64_t sizes[5], int64_t* unzip_src,
+                      int64_t* zip_src, int64_t* inject, int64_t* prolong, int64_t* interp);
 /* Tiles the levels with blocks (sides 13/19/31/55, level, g0 = first
  * interior node in the level's global node index, ptmin/ptmax from
  * xmin + (g0 - 3) h_l, physical-boundary flags on level 0).  blocks == NULL

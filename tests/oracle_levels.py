@@ -37,11 +37,19 @@ def lagrange_half():
 
 
 class LevelOracle:
+    """Per patch (one per level for a box-per-level spec): its box, grid
+    offset, parent and children, derived from the spec's patch list; every
+    rule evaluated geometrically."""
+
     def __init__(self, spec, O):
         self.spec, self.O = spec, O
         self.W = lagrange_half()
-        self.boxes = [(np.array(lo, dtype=np.int64), np.array(n, dtype=np.int64)) for lo, n in spec.boxes]
-        self.L = len(self.boxes)
+        pl = spec.patch_list
+        self.level = [int(p[0]) for p in pl]
+        self.parent = [int(p[1]) for p in pl]
+        self.boxes = [(np.array(p[2], dtype=np.int64), np.array(p[3], dtype=np.int64)) for p in pl]
+        self.L = len(self.boxes)            # number of patches
+        self.kids = [[c for c in range(self.L) if self.parent[c] == q] for q in range(self.L)]
         self.offsets, self.dims = [], []
         off = 0
         for lo, n in self.boxes:
@@ -52,15 +60,19 @@ class LevelOracle:
         self.n_nodes = off
         bl = spec.as_numpy()
         self.blk = bl
-        # per level: block id of each octant of its box
+        # the patch of every block: its level's patch holding its octants
+        self.patch = np.full(spec.nblocks, -1, dtype=np.int64)
         self.octs = []
-        for l, (lo, n) in enumerate(self.boxes):
+        for q, (lo, n) in enumerate(self.boxes):
             t = -np.ones(tuple(n[::-1]), dtype=np.int64)
-            for b in np.nonzero(bl["level"] == l)[0]:
+            for b in np.nonzero(bl["level"] == self.level[q])[0]:
                 o = bl["g0"][b] // OCT - lo
                 w = (int(bl["sz"][b]) - 7) // OCT
-                t[o[2]:o[2] + w, o[1]:o[1] + w, o[0]:o[0] + w] = b
+                if np.all(o >= 0) and np.all(o + w <= n):
+                    t[o[2]:o[2] + w, o[1]:o[1] + w, o[0]:o[0] + w] = b
+                    self.patch[b] = q
             self.octs.append(t)
+        assert (self.patch >= 0).all()
         self.mo = MeshOracle(spec, O)
 
     # ---- geometry
@@ -75,8 +87,9 @@ class LevelOracle:
         return self.offsets[l] + r[..., 0] + d[0] * (r[..., 1] + d[1] * r[..., 2])
 
     def coarse_values(self, Z, l, q):
-        """(24, N) values at level-l points q (N, 3) from level l-1: the
+        """(24, N) values at patch-l points q (N, 3) from its parent: the
         coincident node, or the interpolation along every odd axis."""
+        pa = self.parent[l]
         out = np.zeros((NVARS, len(q)))
         odd = (q & 1) == 1
         c = np.where(odd, OCT * (((q - 1) // 2) // OCT), q // 2)
@@ -94,7 +107,7 @@ class LevelOracle:
                     tx = None
                     for aa in range(n[0]):
                         p = cs + np.array([aa, bb, cc])
-                        v = Z[:, self.node(l - 1, p)]
+                        v = Z[:, self.node(pa, p)]
                         t = wt[0][:, aa] * v
                         tx = t if aa == 0 else tx + t
                     t = wt[1][:, bb] * tx
@@ -108,14 +121,14 @@ class LevelOracle:
     def unzip(self, Z):
         P = np.zeros((NVARS, self.spec.n_unzip))
         for b in range(self.spec.nblocks):
-            s, l = int(self.blk["sz"][b]), int(self.blk["level"][b])
+            s, l = int(self.blk["sz"][b]), int(self.patch[b])
             i = np.arange(s)
             qz, qy, qx = np.meshgrid(i, i, i, indexing="ij")
             q = np.stack([qx.ravel(), qy.ravel(), qz.ravel()], axis=1) + self.blk["g0"][b] - 3
             vals = np.zeros((NVARS, len(q)))
             ins = self.in_grid(l, q)
             vals[:, ins] = Z[:, self.node(l, q[ins])]
-            if l > 0 and (~ins).any():
+            if self.level[l] > 0 and (~ins).any():
                 vals[:, ~ins] = self.coarse_values(Z, l, q[~ins])
             off = int(self.blk["offset"][b])
             P[:, off:off + s ** 3] = vals
@@ -130,19 +143,20 @@ class LevelOracle:
             e = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
             q = e + OCT * lo
             keep = np.ones(len(q), dtype=bool)
-            if l > 0:
+            if self.level[l] > 0:
                 keep &= ~np.any((e == 0) | (e == d - 1), axis=1)
-            if l + 1 < self.L:
-                clo, cn = self.boxes[l + 1][0] // 2, self.boxes[l + 1][1] // 2
+            for c in self.kids[l]:
+                clo, cn = self.boxes[c][0] // 2, self.boxes[c][1] // 2
                 keep &= ~np.all((q > OCT * clo) & (q < OCT * (clo + cn)), axis=1)
             q = q[keep]
             t = np.minimum(q // OCT, lo + n - 1)
             b = self.octs[l][t[:, 2] - lo[2], t[:, 1] - lo[1], t[:, 0] - lo[0]]
-            if l + 1 < self.L and (b < 0).any():
-                clo = self.boxes[l + 1][0] // 2
-                m = b < 0
-                t2 = t[m] - (q[m] == OCT * clo)
-                b[m] = self.octs[l][t2[:, 2] - lo[2], t2[:, 1] - lo[1], t2[:, 0] - lo[0]]
+            for c in self.kids[l]:  # on a finer patch's boundary: the octant below
+                clo, cn = self.boxes[c][0] // 2, self.boxes[c][1] // 2
+                m = (b < 0) & np.all((t >= clo) & (t < clo + cn), axis=1)
+                if m.any():
+                    t2 = t[m] - (q[m] == OCT * clo)
+                    b[m] = self.octs[l][t2[:, 2] - lo[2], t2[:, 1] - lo[1], t2[:, 0] - lo[0]]
             assert (b >= 0).all()
             sz = self.blk["sz"][b].astype(np.int64)
             loc = q - self.blk["g0"][b] + 3
@@ -150,13 +164,14 @@ class LevelOracle:
         return own
 
     def sync(self, Z):
-        for l in range(self.L - 1, 0, -1):  # restriction, finest first
+        order = sorted(range(1, self.L), key=lambda q: -self.level[q])
+        for l in order:  # restriction, finest first
             lo, n = self.boxes[l]
             r = [np.arange(3 * lo[k] + 1, 3 * (lo[k] + n[k])) for k in range(3)]
             z, y, x = np.meshgrid(r[2], r[1], r[0], indexing="ij")
             c = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
-            Z[:, self.node(l - 1, c)] = Z[:, self.node(l, 2 * c)]
-        for l in range(1, self.L):  # box boundaries, coarsest first
+            Z[:, self.node(self.parent[l], c)] = Z[:, self.node(l, 2 * c)]
+        for l in sorted(range(1, self.L), key=lambda q: self.level[q]):  # boundaries, coarsest first
             lo, n = self.boxes[l]
             d = self.dims[l]
             z, y, x = np.meshgrid(*[np.arange(k) for k in d[::-1]], indexing="ij")
@@ -172,7 +187,7 @@ class LevelOracle:
         Z = np.zeros((NVARS, self.n_nodes))
         b = (C.c_double * 6)(*bh)
         for l, (lo, n) in enumerate(self.boxes):
-            h = self.spec.h0 / 2 ** l
+            h = self.spec.h0 / 2 ** self.level[l]
             G = (C.c_int32 * 3)(*[int(x) for x in self.dims[l]])
             xm = (C.c_double * 3)(*[self.spec.xmin + OCT * int(lo[k]) * h for k in range(3)])
             ptr = (C.c_void_p * NVARS)(*[Z.ctypes.data + (v * self.n_nodes + self.offsets[l]) * 8
@@ -208,19 +223,24 @@ class LevelOracle:
 
 
 def transfer(LO_old, Z_old, LO_new):
-    """State on LO_new's hierarchy from Z_old on LO_old's: per new level,
-    in increasing order, the old same-level node where the old grid has it,
-    else the coincident node or interpolation from the new level below; then
+    """State on LO_new's hierarchy from Z_old on LO_old's: per new patch,
+    parents first, the node of an old patch of the same level where one has
+    it, else the coincident node or interpolation from the new parent; then
     the new hierarchy's sync."""
     Z = np.zeros((NVARS, LO_new.n_nodes))
     for l, (lo, n) in enumerate(LO_new.boxes):
         d = LO_new.dims[l]
         z, y, x = np.meshgrid(*[np.arange(k) for k in d[::-1]], indexing="ij")
         q = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1) + OCT * lo
-        old = LO_old.in_grid(l, q) if l < LO_old.L else np.zeros(len(q), dtype=bool)
-        if old.any():
-            Z[:, LO_new.node(l, q[old])] = Z_old[:, LO_old.node(l, q[old])]
-        if (~old).any():
-            assert l > 0
-            Z[:, LO_new.node(l, q[~old])] = LO_new.coarse_values(Z, l, q[~old])
+        done = np.zeros(len(q), dtype=bool)
+        for r in range(LO_old.L):  # the old patch of the same level holding the node
+            if LO_old.level[r] != LO_new.level[l]:
+                continue
+            m = ~done & LO_old.in_grid(r, q)
+            if m.any():
+                Z[:, LO_new.node(l, q[m])] = Z_old[:, LO_old.node(r, q[m])]
+                done |= m
+        if (~done).any():
+            assert LO_new.level[l] > 0
+            Z[:, LO_new.node(l, q[~done])] = LO_new.coarse_values(Z, l, q[~done])
     return LO_new.sync(Z)

@@ -143,3 +143,57 @@ def test_remesh_during_evolution(O):
     got = dV.cpu().numpy()
     assert np.isfinite(got).all()
     assert ol.rel_err(V, got).max() <= 1e-13
+
+
+PATCHES = ((8, 4, 4), [(1, 0, (2, 2, 2), (4, 4, 4)), (1, 0, (10, 2, 2), (4, 4, 4)),
+                       (2, 1, (6, 6, 6), (4, 4, 4))])
+
+
+def test_patches_ghost_fill_sync_and_steps(O):
+    """Two refined patches on level 1 (one refined again): ghost fill and
+    sync bit-exact, two RK4 steps (graph) within 1e-13 of the oracle."""
+    import bssn_b200 as B
+    from bssn_b200 import levels as LV
+    # origin off the node lattice of the punctures at (+-1, 0, 0), so no
+    # node sits on a puncture (Brill-Lindquist data is singular there)
+    spec = LV.generate_patches(*PATCHES, xmin=-8.25)
+    LO = LevelOracle(spec, O)
+    m = B.Mesh(spec)
+    rng = np.random.default_rng(4)
+    Z = rng.standard_normal((24, spec.n_nodes))
+    P = torch.zeros((24, m.n_unzip), dtype=torch.float64, device="cuda")
+    dZ = dev(Z)
+    m.unzip(P, dZ)
+    LV.sync(m, dZ)
+    torch.cuda.synchronize()
+    assert np.array_equal(P.cpu().numpy().view(np.uint64), LO.unzip(Z).view(np.uint64))
+    assert np.array_equal(dZ.cpu().numpy().view(np.uint64), LO.sync(Z.copy()).view(np.uint64))
+    Z0 = LO.initial_data(eps=1e-8)
+    dt = 0.25 * spec.h
+    dZ = dev(Z0)
+    plan = B.RK4Plan(m, B.default_params(), B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
+    Zr = Z0
+    for _ in range(2):
+        plan.step(dZ, dt)
+        Zr = LO.rk4_step(Zr, dt, ol.params())
+    torch.cuda.synchronize()
+    assert plan.violations() == 0
+    err = ol.rel_err(Zr, dZ.cpu().numpy())
+    assert err.max() <= 1e-13, err.max()
+
+
+def test_transfer_box_chain_to_patches(O):
+    """Transfer from a box-per-level hierarchy to a two-patch one, bit-exact
+    against the oracle's transfer."""
+    from oracle_levels import transfer as otransfer
+    import bssn_b200 as B
+    from bssn_b200 import levels as LV
+    old = LV.generate_levels((8, 4, 4), [((2, 2, 2), (12, 4, 4))])
+    LOo = LevelOracle(old, O)
+    Z = LOo.sync(np.random.default_rng(6).standard_normal((24, old.n_nodes)))
+    new = LV.generate_patches(*PATCHES)
+    mo, mn = B.Mesh(old), B.Mesh(new)
+    dV = torch.empty((24, new.n_nodes), dtype=torch.float64, device="cuda")
+    LV.transfer(mo, dev(Z), mn, dV)
+    ref = otransfer(LOo, Z, LevelOracle(new, O))
+    assert np.array_equal(dV.cpu().numpy().view(np.uint64), ref.view(np.uint64))

@@ -174,3 +174,53 @@ def test_regrid_policy():
     assert nb == [((2, 2, 2), (2, 2, 2))]
     for flags in (fine, corner, np.ones(spec.nblocks)):
         LV.generate_levels(M0, LV.regrid_boxes(spec, flags))
+
+
+PATCHES = ((8, 4, 4), [(1, 0, (2, 2, 2), (4, 4, 4)), (1, 0, (10, 2, 2), (4, 4, 4)),
+                       (2, 1, (6, 6, 6), (4, 4, 4))])
+
+
+def test_patch_maps_match_oracle(O):
+    """Two separate level-1 patches (one with a level-2 child): the
+    library's maps against the patch-aware oracle, bit for bit."""
+    spec = LV.generate_patches(*PATCHES)
+    LO = LevelOracle(spec, O)
+    maps = LV.level_maps(spec)
+    W = lagrange_half()
+    rng = np.random.default_rng(9)
+    Z = rng.standard_normal((3, spec.n_nodes))
+    Z24 = np.zeros((ol.NVARS, spec.n_nodes))
+    Z24[:3] = Z
+    value = eval_maps(maps, Z, W)
+    ref = LO.unzip(Z24)[:3]
+    assert np.array_equal(value(maps["unzip_src"]).view(np.uint64), ref.view(np.uint64))
+    assert np.array_equal(maps["zip_src"], LO.owners())
+    # sync through the maps: restriction by source level (finest first),
+    # then prolongation by level (coarsest first)
+    patch_of = lambda nodes: np.searchsorted(np.array(LO.offsets[1:]), nodes, side="right")  # noqa: E731
+    lev = np.array(LO.level)
+    S = Z.copy()
+    inj, pro = maps["inject"], maps["prolong"]
+    il = lev[patch_of(inj[:, 1])]
+    for l in sorted(set(il.tolist()), reverse=True):
+        m = il == l
+        S[:, inj[m, 0]] = S[:, inj[m, 1]]
+    pl = lev[patch_of(pro[:, 0])]
+    for l in sorted(set(pl.tolist())):
+        m = pl == l
+        S[:, pro[m, 0]] = eval_maps(maps, S, W)(pro[m, 1])
+    ref = LO.sync(Z24.copy())[:3]
+    assert np.array_equal(S.view(np.uint64), ref.view(np.uint64))
+
+
+def test_patch_rules():
+    """Invalid hierarchies are refused: patches of one level too close,
+    a child without margin, a parent of the wrong level."""
+    M0 = (8, 4, 4)
+    with pytest.raises(B.BssnError):  # level-1 patches touching (less than a parent octant apart)
+        LV.generate_patches(M0, [(1, 0, (2, 2, 2), (4, 4, 4)), (1, 0, (6, 2, 2), (4, 4, 4))])
+    LV.generate_patches(M0, [(1, 0, (2, 2, 2), (4, 4, 4)), (1, 0, (8, 2, 2), (4, 4, 4))])  # one apart: valid
+    with pytest.raises(B.BssnError):  # no margin inside the parent
+        LV.generate_patches(M0, [(1, 0, (0, 2, 2), (4, 4, 4))])
+    with pytest.raises(B.BssnError):  # parent of the wrong level
+        LV.generate_patches(M0, [(1, 0, (2, 2, 2), (4, 4, 4)), (1, 1, (6, 6, 6), (4, 4, 4))])
