@@ -255,16 +255,127 @@ def regrid_boxes(spec: LevelMeshSpec, flags, max_levels=None):
     return boxes
 
 
-def remesh(mesh, U, flags, max_levels=None, stream=None):
+def remesh(mesh, U, flags, max_levels=None, patches=False, stream=None):
     """Regrid a level mesh from refine flags and carry the state over:
     returns (spec, mesh, U) on the new hierarchy (the old mesh and state are
-    left as they are)."""
+    left as they are).  patches: one patch per cluster of refinement
+    (regrid_patches) instead of one box per level (regrid_boxes)."""
     import torch
     spec = mesh.spec
-    boxes = regrid_boxes(spec, flags.cpu().numpy() if hasattr(flags, "cpu") else flags, max_levels)
+    f = flags.cpu().numpy() if hasattr(flags, "cpu") else flags
     from . import Mesh
-    new = generate_levels(spec.M0, boxes, xmin=spec.xmin, L=spec.h0 * OCT * spec.M0[0])
+    L = spec.h0 * OCT * spec.M0[0]
+    if patches:
+        new = generate_patches(spec.M0, regrid_patches(spec, f, max_levels), xmin=spec.xmin, L=L)
+    else:
+        new = generate_levels(spec.M0, regrid_boxes(spec, f, max_levels), xmin=spec.xmin, L=L)
     nmesh = Mesh(new)
     V = torch.empty((NVARS, new.n_nodes), dtype=torch.float64, device=U.device)
     transfer(mesh, U, nmesh, V, stream)
     return new, nmesh, V
+
+
+def regrid_patches(spec: LevelMeshSpec, flags, max_levels=None):
+    """Patches (level, parent, lo, n) from per-block refine flags, one patch
+    per connected cluster of refinement, the multi-region form of
+    regrid_boxes (octree-like: separate sources get separate patches):
+
+    * level k needs the level-(k-1) octants of every flagged level-(k-1)
+      block, of every flagged level-k block (kept fine), and of every new
+      level-(k+1) patch (widened by one level-k octant, so it nests);
+    * flagged octants are widened by one parent octant, and all of them are
+      grouped into 26-connected clusters; each cluster's bounding box is a
+      patch, clamped to the region where level-k patches nest inside the
+      domain; patches closer than one parent octant are merged;
+    * levels are built finest first, so every patch lies inside the patch of
+      the level below that holds it; at most one level finer than the
+      current finest is added (max_levels caps the total).
+    Returns the patches after patch 0 (parents listed first)."""
+    flags = np.asarray(flags).astype(bool)
+    bl = spec.as_numpy()
+    L = spec.nlevels
+    top = L + 1 if max_levels is None else min(L + 1, max_levels)
+    M0 = np.asarray(spec.M0, dtype=np.int64)
+    # allowed [A, B) for level-k patch boxes, in level-(k-1) octants
+    A, Bnd = {1: np.ones(3, dtype=np.int64)}, {1: M0 - 1}
+    for k in range(2, top):
+        A[k], Bnd[k] = 2 * A[k - 1] + 1, 2 * Bnd[k - 1] - 1
+    per_level = {}          # level -> list of (lo, hi) in level-k octants
+    for k in range(top - 1, 0, -1):
+        cells = set()
+        for lev, scale in ((k - 1, 1), (k, 0)):
+            for b in np.nonzero(flags & (bl["level"] == lev))[0]:
+                o = np.asarray(bl["g0"][b], dtype=np.int64) // OCT
+                w = (int(bl["sz"][b]) - 7) // OCT
+                if scale == 0:  # level-k block -> its level-(k-1) octants
+                    lo, hi = o // 2, -(-(o + w) // 2)
+                else:
+                    lo, hi = o, o + w
+                lo, hi = lo - 1, hi + 1  # widened by one parent octant
+                for x in range(lo[0], hi[0]):
+                    for y in range(lo[1], hi[1]):
+                        for z in range(lo[2], hi[2]):
+                            cells.add((x, y, z))
+        for lo, hi in per_level.get(k + 1, []):  # finer patches, in level-(k-1) octants, widened
+            clo, chi = lo // 4 - 1, -(-hi // 4) + 1
+            for x in range(clo[0], chi[0]):
+                for y in range(clo[1], chi[1]):
+                    for z in range(clo[2], chi[2]):
+                        cells.add((x, y, z))
+        if not cells:
+            continue
+        # 26-connected clusters
+        boxes, seen = [], set()
+        for c in cells:
+            if c in seen:
+                continue
+            comp, stack = [], [c]
+            seen.add(c)
+            while stack:
+                u = stack.pop()
+                comp.append(u)
+                for dx in (-1, 0, 1):
+                    for dy in (-1, 0, 1):
+                        for dz in (-1, 0, 1):
+                            v = (u[0] + dx, u[1] + dy, u[2] + dz)
+                            if v in cells and v not in seen:
+                                seen.add(v)
+                                stack.append(v)
+            a = np.array(comp, dtype=np.int64)
+            lo = np.maximum(a.min(axis=0), A[k])
+            hi = np.minimum(a.max(axis=0) + 1, Bnd[k])
+            if np.all(hi > lo):
+                boxes.append([lo, hi])
+        # merge boxes closer than one parent octant (in level-(k-1) octants)
+        merged = True
+        while merged:
+            merged = False
+            for i in range(len(boxes)):
+                for j in range(i + 1, len(boxes)):
+                    (alo, ahi), (blo, bhi) = boxes[i], boxes[j]
+                    if np.all((alo < bhi + 1) & (blo < ahi + 1)):
+                        boxes[i] = [np.minimum(alo, blo), np.maximum(ahi, bhi)]
+                        del boxes[j]
+                        merged = True
+                        break
+                if merged:
+                    break
+        per_level[k] = [(2 * lo, 2 * hi) for lo, hi in boxes]  # level-k octants
+    out = []
+    index = {0: [(0, np.zeros(3, dtype=np.int64), 2 * M0)]}  # level -> [(patch, lo, hi) in next-level units]
+    for k in range(1, top):
+        if k not in per_level or not index.get(k - 1):
+            break
+        index[k] = []
+        for lo, hi in per_level[k]:
+            parent = None
+            for pi, plo, phi in index[k - 1]:
+                if np.all(lo >= plo) and np.all(hi <= phi):
+                    parent = pi
+                    break
+            if parent is None:
+                continue  # cannot nest (clamped away): dropped with its subtree
+            pid = len(out) + 1
+            out.append((k, parent, tuple(int(v) for v in lo), tuple(int(v) for v in hi - lo)))
+            index[k].append((pid, 2 * lo, 2 * hi))
+    return out

@@ -197,3 +197,46 @@ def test_transfer_box_chain_to_patches(O):
     LV.transfer(mo, dev(Z), mn, dV)
     ref = otransfer(LOo, Z, LevelOracle(new, O))
     assert np.array_equal(dV.cpu().numpy().view(np.uint64), ref.view(np.uint64))
+
+
+def test_remesh_into_patches_during_evolution(O):
+    """Two refined patches evolve, the wavelet test flags blocks, the flags
+    are clustered into new patches, the state is transferred and evolved on:
+    the GPU against the oracle fed the same flags."""
+    from oracle_levels import transfer as otransfer
+    import bssn_b200 as B
+    from bssn_b200 import levels as LV
+    spec = LV.generate_patches((12, 4, 4), [(1, 0, (2, 2, 2), (4, 4, 4)), (1, 0, (16, 2, 2), (4, 4, 4))],
+                               xmin=-8.25)
+    LO = LevelOracle(spec, O)
+    m = B.Mesh(spec)
+    prm = B.default_params()
+    dt = 0.25 * spec.h
+    Z = LO.initial_data(eps=1e-8)
+    dZ = dev(Z)
+    plan = B.RK4Plan(m, prm, B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
+    for _ in range(2):
+        plan.step(dZ, dt)
+        Z = LO.rk4_step(Z, dt, ol.params())
+    P = torch.zeros((24, m.n_unzip), dtype=torch.float64, device="cuda")
+    m.unzip(P, dZ)
+    _, ratio, _ = B.wavelet_scores(m, P, tol=1e-6)
+    r = ratio.cpu().numpy()
+    flags = (r >= np.quantile(r, 0.7)).astype(np.uint8)
+    new, nm, dV = LV.remesh(m, dZ, flags, patches=True)
+    LN = LevelOracle(new, O)
+    V = otransfer(LO, Z, LN)
+    assert ol.rel_err(V, dV.cpu().numpy()).max() <= 1e-13
+    plan2 = B.RK4Plan(nm, prm, B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
+    dt2 = 0.25 * new.h
+    for _ in range(2):
+        plan2.step(dV, dt2)
+        V = LN.rk4_step(V, dt2, ol.params())
+    torch.cuda.synchronize()
+    assert plan.violations() == 0 and plan2.violations() == 0
+    got = dV.cpu().numpy()
+    assert np.isfinite(got).all()
+    # relative to each variable's largest magnitude: the noise-level
+    # variables (|max| ~ 1e-6 on the finer patches) carry the rounding of
+    # the FP64 right-hand side (1e-12 of them, ~1e-18 absolute)
+    assert ol.rel_err(V, got).max() <= 1e-11

@@ -224,3 +224,30 @@ def test_patch_rules():
         LV.generate_patches(M0, [(1, 0, (0, 2, 2), (4, 4, 4))])
     with pytest.raises(B.BssnError):  # parent of the wrong level
         LV.generate_patches(M0, [(1, 0, (2, 2, 2), (4, 4, 4)), (1, 1, (6, 6, 6), (4, 4, 4))])
+
+
+def test_regrid_patches_clusters():
+    """Refinement in two separate places gives two patches per level (each
+    refined again where its fine blocks are flagged); nothing flagged gives
+    none; every result is a valid hierarchy."""
+    M0 = (12, 4, 4)
+    spec = LV.generate_patches(M0, [(1, 0, (2, 2, 2), (4, 4, 4)), (1, 0, (16, 2, 2), (4, 4, 4))])
+    bl = spec.as_numpy()
+    assert LV.regrid_patches(spec, np.zeros(spec.nblocks)) == []
+    pt = LV.regrid_patches(spec, (bl["level"] == 1).astype(np.uint8))
+    lev = [p[0] for p in pt]
+    assert lev.count(1) == 2 and lev.count(2) == 2
+    for k, par, lo, n in pt:  # children nest in their own parent
+        if k == 2:
+            plo, pn = np.array(pt[par - 1][2]), np.array(pt[par - 1][3])
+            assert np.all(np.array(lo) // 2 >= plo + 1) and np.all((np.array(lo) + n) // 2 <= plo + pn - 1)
+    LV.generate_patches(M0, pt)
+    # flags only on the level-0 blocks at the two ends: two level-1 patches
+    ends = np.zeros(spec.nblocks, dtype=np.uint8)
+    for b in np.nonzero(bl["level"] == 0)[0]:
+        o, w = bl["g0"][b] // 6, (int(bl["sz"][b]) - 7) // 6
+        if o[0] <= 1 < o[0] + w or o[0] <= 10 < o[0] + w:
+            ends[b] = 1
+    pt = LV.regrid_patches(spec, ends, max_levels=2)
+    assert [p[0] for p in pt] == [1, 1]
+    LV.generate_patches(M0, pt)
