@@ -74,6 +74,8 @@ def _sig():
     lib.bssn_rk4_plan_step.argtypes = [vp, vp, d, vp]
     lib.bssn_rk4_plan_diagnostics.argtypes = [vp, vp, P(d), d, P(d), P(d), vp, vp]
     lib.bssn_rk4_plan_step_diag.argtypes = [vp, vp, d, P(d), d, P(d), P(d), vp, vp]
+    lib.bssn_rk4_plan_diag_fields.argtypes = [vp, vp]
+    lib.bssn_rk4_plan_copy_diag_fields.argtypes = [vp, vp, i, vp]
     lib.bssn_rk4_plan_autotune.argtypes = [vp, vp, i, vp, P(C.c_float)]
     lib.bssn_rk4_plan_tile.argtypes = [vp, i]
     lib.bssn_rk4_plan_set_tile.argtypes = [vp, i, i]
@@ -314,6 +316,7 @@ PLAN_ENFORCE_STAGES = 1
 PLAN_GRAPH = 2
 PLAN_PER_BLOCK = 4
 PLAN_DIRECT = 8
+PLAN_DIAG_PSI4 = 16
 
 
 class RK4Plan:
@@ -350,6 +353,15 @@ class RK4Plan:
         xm, h, b, r, nd = self._diag_args(norms, bh, radii)
         check(lib.bssn_rk4_plan_step_diag(self.h, ptrs(U), dt, xm, h, b, r, nd, stream_ptr(stream)),
               "rk4_plan_step_diag")
+
+    def diag_fields(self, out, stream=None):
+        """Copy the plan's diagnostic fields into `out` ((4 or 6, n_nodes)
+        float64 CUDA tensor): ham, mom0..2 and, with PLAN_DIAG_PSI4, psi4
+        real and imaginary, as written by the last diagnostics call."""
+        nf = out.shape[0]
+        dst = (C.c_void_p * nf)(*[out[c].data_ptr() for c in range(nf)])
+        check(lib.bssn_rk4_plan_copy_diag_fields(self.h, dst, nf, stream_ptr(stream)), "copy_diag_fields")
+        return out
 
     def autotune(self, U, reps=3, stream=None):
         sides = sorted(set(self.mesh.spec.sides.tolist()))

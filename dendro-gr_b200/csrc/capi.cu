@@ -277,6 +277,30 @@ int bssn_rk4_plan_diagnostics(bssn_rk4_plan plan, double* const* u_dev, const do
     return st ? st : bssn::plan_diag(plan->p, u_dev, d, S(stream));
 }
 
+int bssn_rk4_plan_diag_fields(bssn_rk4_plan plan, double** fields_dev) {
+    if (!plan || !fields_dev) return BSSN_EINVAL;
+    bssn::Plan* p = plan->p;
+    if (!p->cons) return BSSN_ESTATE;
+    const int nf = (p->flags & BSSN_PLAN_DIAG_PSI4) ? 6 : 4;
+    for (int c = 0; c < 6; c++) fields_dev[c] = c < nf ? p->cons + (size_t)c * p->n_nodes : nullptr;
+    return 0;
+}
+
+int bssn_rk4_plan_copy_diag_fields(bssn_rk4_plan plan, double* const* dst_dev, int nfields,
+                                   bssn_stream_t stream) {
+    double* f[6];
+    int st = bssn_rk4_plan_diag_fields(plan, f);
+    if (st) return st;
+    if (!dst_dev || nfields < 1 || nfields > 6 || !f[nfields - 1]) return BSSN_EINVAL;
+    for (int c = 0; c < nfields; c++) {
+        if (!dst_dev[c]) return BSSN_EINVAL;
+        st = bssn::cuda_status(cudaMemcpyAsync(dst_dev[c], f[c], sizeof(double) * plan->p->n_nodes,
+                                               cudaMemcpyDeviceToDevice, S(stream)));
+        if (st) return st;
+    }
+    return 0;
+}
+
 int bssn_rk4_plan_step_diag(bssn_rk4_plan plan, double* const* u_dev, double dt,
                             const double xmin[3], double h, const double bh[6],
                             const double radii[2], double* norms_dev, bssn_stream_t stream) {

@@ -343,7 +343,8 @@ static int diag_prepare(Plan* p) {
     // needs the padded stage array and a single-level node grid
     if (p->direct || !p->P || p->mesh->lv) return BSSN_ESTATE;
     MeshState* m = p->mesh;
-    if (!p->cons && alloc(&p->cons, (size_t)4 * p->n_nodes)) return BSSN_ENOMEM;
+    const size_t nf = (p->flags & BSSN_PLAN_DIAG_PSI4) ? 6 : 4;  // ham, mom0..2 (, psi4 re, im)
+    if (!p->cons && alloc(&p->cons, nf * p->n_nodes)) return BSSN_ENOMEM;
     if (!m->d_partial &&
         cudaMalloc((void**)&m->d_partial, sizeof(double) * 5 * kNormPartials) != cudaSuccess) {
         cudaGetLastError();
@@ -358,9 +359,10 @@ static int enqueue_diag(Plan* p, double* const* u, const DiagArgs& d, cudaStream
     set_ptrs(p->P, m->unzip_size, Pp);
     int st = unzip_all(m, Pp, (const double* const*)u, s);
     if (st) return st;
-    double* cons[4];
-    for (int c = 0; c < 4; c++) cons[c] = p->cons + (size_t)c * p->n_nodes;
-    st = launch_constraints(m, (const double* const*)Pp, cons, s);
+    const bool psi4 = (p->flags & BSSN_PLAN_DIAG_PSI4) != 0;
+    double* cons[6];
+    for (int c = 0; c < (psi4 ? 6 : 4); c++) cons[c] = p->cons + (size_t)c * p->n_nodes;
+    st = launch_constraints(m, (const double* const*)Pp, cons, s, psi4);
     if (st) return st;
     return launch_l2_norms(m, (const double* const*)cons, 4, d.xmin, d.h, d.bh, d.radii, m->d_partial,
                            kNormPartials, d.norms, s);

@@ -320,6 +320,7 @@ int bssn_remesh_decide_f64(bssn_mesh mesh, const double* const* unzip_dev,
 #define BSSN_PLAN_GRAPH 2          /* capture / replay as a CUDA graph */
 #define BSSN_PLAN_PER_BLOCK 4      /* one RHS launch per block (plain path) */
 #define BSSN_PLAN_DIRECT 8         /* right-hand side on the zipped grid */
+#define BSSN_PLAN_DIAG_PSI4 16     /* diagnostics also compute psi4 */
 typedef struct bssn_rk4_plan_s* bssn_rk4_plan;
 int bssn_rk4_plan_create(bssn_mesh mesh, const BssnParams* params, int flags,
                          bssn_rk4_plan* out);
@@ -345,6 +346,15 @@ int bssn_rk4_plan_step_diag(bssn_rk4_plan plan, double* const* u_dev, double dt,
                             const double xmin[3], double h, const double bh[6],
                             const double radii[2], double* norms_dev,
                             bssn_stream_t stream);
+/* The plan's diagnostic fields (zipped, n_nodes doubles each) as written by
+ * its last diagnostics call: fields_dev[0..3] = ham, mom0..2 and, with
+ * BSSN_PLAN_DIAG_PSI4, fields_dev[4..5] = psi4 real, imaginary (ready for
+ * bssn_gw_extract_f64); BSSN_ESTATE before the first diagnostics call. */
+int bssn_rk4_plan_diag_fields(bssn_rk4_plan plan, double** fields_dev);
+/* Copies the first nfields of those fields into caller arrays (device to
+ * device, on `stream`). */
+int bssn_rk4_plan_copy_diag_fields(bssn_rk4_plan plan, double* const* dst_dev, int nfields,
+                                   bssn_stream_t stream);
 /* Autotuner: times every tile the plan can run (direct plans: split tiles
  * only) on every block-size bucket of the mesh with the state u_dev (best of
  * reps) and keeps the fastest per bucket in the mesh handle.  Blocking.

@@ -79,3 +79,32 @@ def test_constraint_norm_history_in_graph():
         ref = np.array([float.fromhex(x) for x in h["norms"]])
         worst = max(worst, (np.abs(got[h["step"] // 10] - ref) / np.abs(ref)).max())
     assert worst <= 1e-10, worst
+
+
+def test_psi4_in_diagnostics_graph():
+    """With PLAN_DIAG_PSI4 the graph-captured step + diagnostics also
+    writes psi4: the plan's fields equal bssn_constraints_psi4_f64 on the
+    ghost-filled new state (same kernel, bit for bit), and feed the
+    gravitational-wave extraction directly."""
+    import ctypes as C
+    import bssn_b200 as B
+    from bssn_b200 import gw
+    spec = B.generate_mesh(1, (2, 1, 1), seed=1, xmin=-8.25)
+    m = B.Mesh(spec)
+    U = torch.zeros((24, spec.n_nodes), dtype=torch.float64, device="cuda")
+    B.initial_data(U, spec)
+    plan = B.RK4Plan(m, B.default_params(), B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH | B.PLAN_DIAG_PSI4)
+    norms = torch.zeros(4, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        plan.step_diag(U, 0.25 * spec.h, norms)
+    fields = plan.diag_fields(torch.empty((6, spec.n_nodes), dtype=torch.float64, device="cuda"))
+    P = torch.zeros((24, m.n_unzip), dtype=torch.float64, device="cuda")
+    m.unzip(P, U)
+    ref = torch.zeros((6, spec.n_nodes), dtype=torch.float64, device="cuda")
+    cp = (C.c_void_p * 6)(*[ref[c].data_ptr() for c in range(6)])
+    B.lib.bssn_constraints_psi4_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    assert B.lib.bssn_constraints_psi4_f64(m.h, B.ptrs(P), cp, B.stream_ptr()) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(fields, ref)
+    md, coeff, l2 = gw.extract(fields[4].contiguous(), fields[5].contiguous(), spec, (3.0, 5.0), lmax=3)
+    assert np.isfinite(coeff).all() and (l2 > 0).all()
