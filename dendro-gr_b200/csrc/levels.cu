@@ -21,6 +21,7 @@
 
 #include "bssn_common.cuh"
 #include "levels.h"
+#include "rk4_stage.cuh"
 
 namespace bssn {
 
@@ -563,6 +564,38 @@ __global__ void __launch_bounds__(256) levels_zip_kernel(MutVars Rz, ConstVars R
     }
 }
 
+// One RK4 stage at every node (the node-wise stage kernel's algebra) with
+// the node's right-hand side read from the padded array at its owning zone
+// (0 for nodes no block owns; the level sync sets those).
+__global__ void __launch_bounds__(256) levels_stage_kernel(int stage, MutVars im, MutVars acc, MutVars u,
+                                                           ConstVars R, const int64_t* __restrict__ src,
+                                                           int64_t n, double dt, int enforce,
+                                                           double chi_floor, int* status) {
+    int bad = 0;
+    for (int64_t node = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; node < n;
+         node += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t sp = src[node];
+        double k[NVARS], v[NVARS], a[NVARS];
+#pragma unroll
+        for (int q = 0; q < NVARS; q++) {
+            k[q] = sp >= 0 ? __ldg(R.p[q] + sp) : 0.0;
+            v[q] = stage < 3 ? u.p[q][node] : 0.0;
+            a[q] = stage > 0 ? acc.p[q][node] : 0.0;
+        }
+        bad += stage_node(stage, dt, k, v, a, enforce, chi_floor);
+#pragma unroll
+        for (int q = 0; q < NVARS; q++) {
+            if (stage < 3) {
+                acc.p[q][node] = a[q];
+                im.p[q][node] = v[q];
+            } else {
+                u.p[q][node] = v[q];
+            }
+        }
+    }
+    if (status && bad) atomicAdd(status, bad);
+}
+
 // dst[i] <- source value of src[i]; the sources never overlap the
 // destinations of the same launch.
 __global__ void __launch_bounds__(256) levels_copy_kernel(MutVars U, int nvars,
@@ -747,6 +780,23 @@ int launch_levels_zip(const LevelsDev& d, double* const* Rz, const double* const
     if (!st) st = vars_in(R, nvars, &r);
     if (st || d.n_nodes == 0) return st;
     levels_zip_kernel<<<grid_for(d.n_nodes, 256), 256, 0, s>>>(z, r, nvars, d.zip_src, d.n_nodes);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_levels_stage(const LevelsDev& d, int stage, double* const* im, double* const* acc,
+                        double* const* u, const double* const* R, double dt, int enforce, double chi_floor,
+                        int* status, cudaStream_t s) {
+    MutVars I, A, U;
+    ConstVars Rr;
+    for (int q = 0; q < NVARS; q++) {
+        I.p[q] = im[q];
+        A.p[q] = acc[q];
+        U.p[q] = u[q];
+        Rr.p[q] = R[q];
+    }
+    if (d.n_nodes == 0) return 0;
+    levels_stage_kernel<<<grid_for(d.n_nodes, 256), 256, 0, s>>>(stage, I, A, U, Rr, d.zip_src, d.n_nodes, dt,
+                                                                  enforce, chi_floor, status);
     return cuda_status(cudaGetLastError());
 }
 

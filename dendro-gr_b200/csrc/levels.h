@@ -113,6 +113,11 @@ int launch_levels_unzip(const LevelsDev& d, double* const* P, const double* cons
 // Rz[node] <- R[owner zone of node], 0 for nodes no block owns.
 int launch_levels_zip(const LevelsDev& d, double* const* Rz, const double* const* R, int nvars,
                       cudaStream_t s);
+// One RK4 stage at every node (as launch_node_stage) with the right-hand
+// side gathered from the padded array R at each node's owning zone.
+int launch_levels_stage(const LevelsDev& d, int stage, double* const* im, double* const* acc,
+                        double* const* u, const double* const* R, double dt, int enforce, double chi_floor,
+                        int* status, cudaStream_t s);
 // Restriction (finest level first) then prolongation (coarsest first) on U.
 int launch_levels_sync(const LevelsDev& d, double* const* U, int nvars, cudaStream_t s);
 // Transfer of a state between two hierarchies on the same domain (after a

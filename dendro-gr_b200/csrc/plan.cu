@@ -248,16 +248,14 @@ int plan_enqueue_stage(Plan* p, double* const* u, double dt, int stage, cudaStre
     const double* const* src = stage == 0 ? (const double* const*)u : (const double* const*)Ip;
     if (m->lv) {
         // multi-level mesh: ghost fill through the level maps, right-hand
-        // side per block (each with its level's spacing), owner gather into
-        // the zipped right-hand side, node-wise stage, level sync of the state
-        // just written
-        double* Rz[NVARS];
-        set_ptrs(p->Rz, p->n_nodes, Rz);
+        // side per block (each with its level's spacing), node-wise stage
+        // reading each node's right-hand side at its owning zone, level sync
+        // of the state just written
         int st = launch_levels_unzip(*m->lv, Pp, src, NVARS, s);
         if (!st) st = plan_rhs(p, s, nullptr, nullptr);
-        if (!st) st = launch_levels_zip(*m->lv, Rz, (const double* const*)Rp, NVARS, s);
         if (!st)
-            st = launch_node_stage(stage, Ip, Ap, u, Rz, p->n_nodes, dt, enf, p->prm.chi_floor, p->status, s);
+            st = launch_levels_stage(*m->lv, stage, Ip, Ap, u, (const double* const*)Rp, dt, enf, p->prm.chi_floor,
+                                     p->status, s);
         if (!st) st = launch_levels_sync(*m->lv, stage < 3 ? Ip : u, NVARS, s);
         return st;
     }
@@ -582,11 +580,12 @@ int plan_launches_per_step(Plan* p) {
             rhs += rhs_launch_count(t, nt, m->scratch_zones);
         }
     }
-    if (m->lv) {  // ghost fill, owner gather, stage, one launch per non-empty sync segment
-        int sync = 0;
+    if (m->lv) {  // interpolation passes, ghost fill, stage, one launch per non-empty sync segment
+        int extra = 2;
+        for (int k = 0; k < 3; k++) extra += m->lv->n_task[k] > 0 ? 1 : 0;
         for (const auto* f : {&m->lv->inject_first, &m->lv->prolong_first})
-            for (size_t k = 0; k + 1 < f->size(); k++) sync += (*f)[k + 1] > (*f)[k] ? 1 : 0;
-        return 4 * (rhs + 3 + sync);
+            for (size_t k = 0; k + 1 < f->size(); k++) extra += (*f)[k + 1] > (*f)[k] ? 1 : 0;
+        return 4 * (rhs + extra);
     }
     return 4 * (rhs + (p->direct ? 1 : 2));
 }
