@@ -240,3 +240,36 @@ def test_remesh_into_patches_during_evolution(O):
     # variables (|max| ~ 1e-6 on the finer patches) carry the rounding of
     # the FP64 right-hand side (1e-12 of them, ~1e-18 absolute)
     assert ol.rel_err(V, got).max() <= 1e-11
+
+
+def test_learned_remesh_on_patch_mesh(O):
+    """The learned remesh decision on a patch hierarchy: with every block
+    deferred (lo = 0, hi = 1) it reproduces the exact wavelet test there;
+    its flags drive a remesh into patches, and the evolution goes on."""
+    import bssn_b200 as B
+    from bssn_b200 import levels as LV
+    spec = LV.generate_patches((12, 4, 4), [(1, 0, (2, 2, 2), (4, 4, 4)), (1, 0, (16, 2, 2), (4, 4, 4))],
+                               xmin=-8.25)
+    m = B.Mesh(spec)
+    U = torch.zeros((24, spec.n_nodes), dtype=torch.float64, device="cuda")
+    LV.initial_data_levels(U, spec, mesh=m)
+    plan = B.RK4Plan(m, B.default_params(), B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
+    plan.step(U, 0.25 * spec.h)
+    P = torch.zeros((24, m.n_unzip), dtype=torch.float64, device="cuda")
+    m.unzip(P, U)
+    net = B.RemeshMLP(seed=6)
+    net.lo, net.hi = 0.0, 1.0
+    flags, stats = B.remesh_decide(m, P, net, tol=1e-6, audit_frac=0.05)
+    _, _, exact = B.wavelet_scores(m, P, tol=1e-6)
+    torch.cuda.synchronize()
+    assert torch.equal(flags, exact)
+    net.lo, net.hi = 0.02, 0.98
+    flags, stats = B.remesh_decide(m, P, net, tol=1e-6, audit_frac=0.05)
+    torch.cuda.synchronize()
+    if int(flags.sum()) == 0:
+        flags[0] = 1  # a decision that refines somewhere, to exercise the remesh
+    new, nm, V = LV.remesh(m, U, flags, patches=True)
+    plan2 = B.RK4Plan(nm, B.default_params(), B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
+    plan2.step(V, 0.25 * new.h)
+    torch.cuda.synchronize()
+    assert bool(torch.isfinite(V).all()) and plan2.violations() == 0
