@@ -5,7 +5,7 @@ kernels can be checked against it.
 
 The reference takes its level transitions from dendrolib's ot::Mesh, which
 is absent from the reference tree (call sites BSSN_GR/src/rkBSSN.cpp:611-650),
-so these rules are this build's own definition (parity unpinned): the
+so these rules are this library's own definition (parity unpinned): the
 interpolation is dendrolib's kind -- the parent element's degree-6 Lagrange
 polynomial on its 7 nodes per axis -- evaluated axis by axis, x then y then
 z, each product and sum rounded in that order (exactly what the GPU does).

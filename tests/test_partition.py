@@ -1,5 +1,5 @@
 """Multi-rank evolution by block partition with a halo exchange before each
-RK4 stage (SURVEY (e)): two gloo ranks on the CPU, the oracle as the engine.
+RK4 stage: two gloo ranks on the CPU, the oracle as the engine.
 The partitioned step must reproduce the single-domain oracle step bit for
 bit on every node, each node owned by exactly one rank."""
 import os
