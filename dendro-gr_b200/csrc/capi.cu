@@ -363,7 +363,6 @@ int bssn_rk4_plan_destroy(bssn_rk4_plan plan) {
 int bssn_constraints_f64(bssn_mesh mesh, const double* const* unzip_dev, double* const* cons_dev,
                          bssn_stream_t stream) {
     if (!mesh || !unzip_dev || !cons_dev) return BSSN_EINVAL;
-    if (mesh->st->lv) return BSSN_ESTATE;  // single-level node grids only
     for (int c = 0; c < 4; c++)
         if (!cons_dev[c]) return BSSN_EINVAL;
     for (int v = 0; v < bssn::NVARS; v++)
@@ -374,7 +373,6 @@ int bssn_constraints_f64(bssn_mesh mesh, const double* const* unzip_dev, double*
 int bssn_constraints_psi4_f64(bssn_mesh mesh, const double* const* unzip_dev, double* const* cons_dev,
                               bssn_stream_t stream) {
     if (!mesh || !unzip_dev || !cons_dev) return BSSN_EINVAL;
-    if (mesh->st->lv) return BSSN_ESTATE;  // single-level node grids only
     for (int c = 0; c < 6; c++)
         if (!cons_dev[c]) return BSSN_EINVAL;
     for (int v = 0; v < bssn::NVARS; v++)

@@ -14,6 +14,8 @@
 // in the reference's order (d/dy(d/dx), d/dz(d/dx), d/dz(d/dy)).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "bssn_common.cuh"
 #include "constraints.h"
 #include "kernels.cuh"
@@ -100,13 +102,13 @@ __device__ __forceinline__ double Dmix(const Blk& b, const double* u, int inner,
 // and P4 the (At r) and d chi products of the definition.
 template <bool PSI4>
 __device__ void constraints_node(const ConstVars& P, const MutVars& out, const BssnBlockDesc& bd,
-                                 int64_t q, int gx, int gy, int gz) {
+                                 int64_t q, int gx, int gy, int gz, int64_t node_at = -1) {
     const int s = bd.sz, N = s - 6;
     const int i = (int)(q % N), j = (int)((q / N) % N), k = (int)(q / ((int64_t)N * N));
     const int64_t x = bd.g0[0] + i, y = bd.g0[1] + j, z = bd.g0[2] + k;
     const bool own = (i < N - 1 || x == gx - 1) && (j < N - 1 || y == gy - 1) &&
                      (k < N - 1 || z == gz - 1);
-    if (!own) return;
+    if (node_at < 0 && !own) return;
     Blk b;
     b.s = s;
     b.a[0] = i + 3;
@@ -226,7 +228,7 @@ __device__ void constraints_node(const ConstVars& P, const MutVars& out, const B
         ham += w * chi * ig[c] * R[c];
         sqrA += w * A[c] * AUU[c];
     }
-    const int64_t node = x + (int64_t)gx * (y + (int64_t)gy * z);
+    const int64_t node = node_at >= 0 ? node_at : x + (int64_t)gx * (y + (int64_t)gy * z);
     out.p[0][node] = ham - sqrA + 2.0 / 3.0 * K * K;
     double dK[3];
     for (int d = 0; d < 3; d++) dK[d] = D1(b, V(U_K), d);
@@ -338,6 +340,42 @@ __global__ void __launch_bounds__(256) constraints_kernel(ConstVars P, MutVars o
         constraints_node<PSI4>(P, out, bd, ck.start + r, gx, gy, gz);
 }
 
+// Multi-level meshes: node n of the zipped state (the level grids back to
+// back) takes the constraints at the zone that owns it, zip_src[n] (a padded
+// index); nodes filled from another level (zip_src -1: patch-boundary nodes
+// and coarse nodes under a finer patch) get 0.  The owning block is the last
+// one whose offset is <= the padded index (offsets ascend).
+template <bool PSI4>
+__global__ void __launch_bounds__(256) constraints_levels_kernel(ConstVars P, MutVars out,
+                                                                 const BssnBlockDesc* __restrict__ blocks,
+                                                                 int nblocks,
+                                                                 const int64_t* __restrict__ zip_src,
+                                                                 int64_t n_nodes) {
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < n_nodes;
+         n += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = zip_src[n];
+        int lo = 0, hi = nblocks - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (blocks[mid].offset <= p) lo = mid;
+            else hi = mid - 1;
+        }
+        const BssnBlockDesc bd = blocks[lo];
+        const int s = bd.sz;
+        const int64_t a = p - bd.offset;
+        const int ax = (int)(a % s), ay = (int)((a / s) % s), az = (int)(a / ((int64_t)s * s));
+        const bool ok = p >= 0 && a >= 0 && a < (int64_t)s * s * s && ax >= 3 && ax < s - 3 && ay >= 3 &&
+                        ay < s - 3 && az >= 3 && az < s - 3;
+        if (!ok) {
+            for (int c = 0; c < (PSI4 ? 6 : 4); c++) out.p[c][n] = 0.0;
+            continue;
+        }
+        const int N = s - 6;
+        const int64_t q = (ax - 3) + (int64_t)N * ((ay - 3) + (int64_t)N * (az - 3));
+        constraints_node<PSI4>(P, out, bd, q, 0, 0, 0, n);
+    }
+}
+
 }  // namespace
 
 // Per-CTA partial sums of c^2 and node counts over nodes outside both
@@ -396,6 +434,17 @@ int launch_constraints(const MeshState* m, const double* const* P, double* const
     MutVars o = {};
     for (int v = 0; v < NVARS; v++) p.p[v] = P[v];
     for (int c = 0; c < (psi4 ? 6 : 4); c++) o.p[c] = out[c];
+    if (m->lv) {
+        const int nb = (int)m->blocks.size();
+        const int64_t nn = m->lv->n_nodes;
+        if (nb == 0 || nn == 0) return 0;
+        const int grid = (int)std::min<int64_t>((nn + 255) / 256, 148 * 16);
+        if (psi4)
+            constraints_levels_kernel<true><<<grid, 256, 0, s>>>(p, o, m->d_blocks, nb, m->lv->zip_src, nn);
+        else
+            constraints_levels_kernel<false><<<grid, 256, 0, s>>>(p, o, m->d_blocks, nb, m->lv->zip_src, nn);
+        return cuda_status(cudaGetLastError());
+    }
     if (m->n_int_chunks == 0) return 0;
     if (psi4)
         constraints_kernel<true><<<m->n_int_chunks, 256, 0, s>>>(p, o, m->d_blocks, m->d_int_chunks,

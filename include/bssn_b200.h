@@ -171,7 +171,11 @@ int bssn_initial_data_f64(double* const* u_dev, const int32_t G[3],
 /* Hamiltonian and momentum constraints (CodeGen/constraints.py:250-283,
  * per block as physical_constraints, BSSN_GR/src/physcon.cpp:12-89) from
  * the padded stage state of every block, written to the zipped node arrays
- * cons_dev[0..3] = ham, mom0, mom1, mom2 (owned nodes only). */
+ * cons_dev[0..3] = ham, mom0, mom1, mom2 (owned nodes only).  On a
+ * multi-level mesh every zipped node (the level grids back to back) takes
+ * the value at the zone that owns it; nodes filled from another level
+ * (patch-boundary nodes, coarse nodes under a finer patch) are set to 0, so
+ * each physical point carries its value once. */
 int bssn_constraints_f64(bssn_mesh mesh, const double* const* unzip_dev,
                          double* const* cons_dev, bssn_stream_t stream);
 /* The same constraints plus the Weyl scalar psi4 for gravitational-wave

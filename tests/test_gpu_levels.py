@@ -273,3 +273,43 @@ def test_learned_remesh_on_patch_mesh(O):
     plan2.step(V, 0.25 * new.h)
     torch.cuda.synchronize()
     assert bool(torch.isfinite(V).all()) and plan2.violations() == 0
+
+
+@pytest.mark.parametrize("name", sorted(MESHES))
+def test_constraints_on_level_mesh(name, O):
+    """Hamiltonian and momentum constraints on a level mesh after one RK4
+    step: every node owned by a zone carries the oracle's
+    orc_physical_constraints (physcon.cpp:12-89 restated) of that zone's
+    block, nodes filled from another level are 0 (within 1e-12 of each
+    field's largest value, as the single-level constraint tests)."""
+    import ctypes as C
+    B, LV, spec, LO = setup(name, O)
+    m = B.Mesh(spec)
+    dZ = torch.zeros((24, spec.n_nodes), dtype=torch.float64, device="cuda")
+    LV.initial_data_levels(dZ, spec, mesh=m)
+    plan = B.RK4Plan(m, B.default_params(), B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
+    plan.step(dZ, 0.25 * spec.h)
+    P = torch.zeros((24, m.n_unzip), dtype=torch.float64, device="cuda")
+    m.unzip(P, dZ)
+    cons = torch.full((4, spec.n_nodes), np.nan, dtype=torch.float64, device="cuda")
+    B.constraints(m, cons, P)
+    torch.cuda.synchronize()
+    plan.close()
+    Uz = P.cpu().numpy()
+    Cz = np.zeros((24, m.n_unzip))
+    ws = np.zeros(288 * 55 ** 3)
+    for b in range(spec.nblocks):
+        blk = spec.blocks[b]
+        s = int(blk.sz)
+        pm, px = np.array(blk.ptmin[:]), np.array(blk.ptmax[:])
+        O.lib.orc_physical_constraints(ol.rows(Cz), ol.rows(Uz), C.c_uint(int(blk.offset)), ol.P(pm), ol.P(px),
+                                       (C.c_uint * 3)(s, s, s), C.c_uint(int(blk.bflag)), ol.P(ws))
+    zs = LV.level_maps(spec)["zip_src"]
+    own = zs >= 0
+    ref = np.zeros((4, spec.n_nodes))
+    ref[:, own] = Cz[:4, zs[own]]
+    got = cons.cpu().numpy()
+    assert np.isfinite(got).all()
+    assert not got[:, ~own].any()
+    err = ol.rel_err(ref, got)
+    assert err.max() <= 1e-12, err
