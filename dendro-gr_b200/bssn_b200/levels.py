@@ -204,7 +204,7 @@ def transfer(mesh_from, U_old, mesh_to, U_new, stream=None):
                                    stream_ptr(stream)), "levels_transfer")
 
 
-def regrid_boxes(spec: LevelMeshSpec, flags, max_levels=None):
+def regrid_boxes(spec: LevelMeshSpec, flags, max_levels=None, keep=None, max_n=None):
     """New level boxes (levels 1.., level-l octants) from per-block refine
     flags, the box-hierarchy form of the reference's remesh (refine where
     the test flags a block, coarsen where nothing asks for the level):
@@ -218,17 +218,25 @@ def regrid_boxes(spec: LevelMeshSpec, flags, max_levels=None):
       covered only as far as the clamp allows);
     * a level nothing asks for is dropped with every finer one; at most one
       level finer than the current finest is added (max_levels caps the
-      total).
+      total);
+    * keep (optional): blocks that hold their level without refining (the
+      reference's coarsening hysteresis: a block coarsens only when its
+      wavelet score is below BSSN_DENDRO_AMR_FAC * tol, BSSN_GR/src/
+      dataUtils.cpp:413-480); level l must cover its kept blocks too;
+    * max_n (optional, even): at most max_n own octants per axis and level,
+      the box shrunk about its centre (the size cap that the reference's
+      maximum depth gives an octree).
     Returns [(lo, n)] for levels 1.. (empty: a single-level mesh)."""
     flags = np.asarray(flags).astype(bool)
+    held = flags if keep is None else flags | np.asarray(keep).astype(bool)
     bl = spec.as_numpy()
     L = spec.nlevels
     top = L + 1 if max_levels is None else min(L + 1, max_levels)
     req = [None] * (top + 1)   # req[l]: (lo, hi) of level l in level-l octants, hi exclusive
     for l in range(top - 1, 0, -1):
         parts = []
-        for lev, scale in ((l - 1, 2), (l, 1)):
-            for b in np.nonzero(flags & (bl["level"] == lev))[0]:
+        for lev, scale, fl in ((l - 1, 2, flags), (l, 1, held)):
+            for b in np.nonzero(fl & (bl["level"] == lev))[0]:
                 o = np.asarray(bl["g0"][b], dtype=np.int64) // OCT
                 w = (int(bl["sz"][b]) - 7) // OCT
                 parts.append((o * scale, (o + w) * scale))
@@ -248,6 +256,11 @@ def regrid_boxes(spec: LevelMeshSpec, flags, max_levels=None):
         lo, hi = req[l]
         lo = np.maximum(lo, 2 * (plo + 1))
         hi = np.minimum(hi, 2 * (plo + pn - 1))
+        if max_n is not None:
+            over = hi - lo > max_n
+            c = ((lo + hi) // 4) * 2
+            lo = np.where(over, np.maximum(c - max_n // 2, 2 * (plo + 1)), lo)
+            hi = np.where(over, np.minimum(lo + max_n, 2 * (plo + pn - 1)), hi)
         if np.any(hi - lo < 2):
             break
         boxes.append((tuple(int(x) for x in lo), tuple(int(x) for x in hi - lo)))
@@ -255,11 +268,12 @@ def regrid_boxes(spec: LevelMeshSpec, flags, max_levels=None):
     return boxes
 
 
-def remesh(mesh, U, flags, max_levels=None, patches=False, stream=None):
+def remesh(mesh, U, flags, max_levels=None, patches=False, stream=None, keep=None, max_n=None):
     """Regrid a level mesh from refine flags and carry the state over:
     returns (spec, mesh, U) on the new hierarchy (the old mesh and state are
     left as they are).  patches: one patch per cluster of refinement
-    (regrid_patches) instead of one box per level (regrid_boxes)."""
+    (regrid_patches) instead of one box per level (regrid_boxes, which also
+    takes the blocks that keep their level)."""
     import torch
     spec = mesh.spec
     f = flags.cpu().numpy() if hasattr(flags, "cpu") else flags
@@ -268,7 +282,7 @@ def remesh(mesh, U, flags, max_levels=None, patches=False, stream=None):
     if patches:
         new = generate_patches(spec.M0, regrid_patches(spec, f, max_levels), xmin=spec.xmin, L=L)
     else:
-        new = generate_levels(spec.M0, regrid_boxes(spec, f, max_levels), xmin=spec.xmin, L=L)
+        new = generate_levels(spec.M0, regrid_boxes(spec, f, max_levels, keep=keep, max_n=max_n), xmin=spec.xmin, L=L)
     nmesh = Mesh(new)
     V = torch.empty((NVARS, new.n_nodes), dtype=torch.float64, device=U.device)
     transfer(mesh, U, nmesh, V, stream)

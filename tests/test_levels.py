@@ -174,6 +174,12 @@ def test_regrid_policy():
     assert nb == [((2, 2, 2), (2, 2, 2))]
     for flags in (fine, corner, np.ones(spec.nblocks)):
         LV.generate_levels(M0, LV.regrid_boxes(spec, flags))
+    # coarsening hysteresis: kept finest blocks hold their level (the box
+    # stays) without adding a finer one; kept flags on level 0 change nothing
+    none = np.zeros(spec.nblocks, dtype=np.uint8)
+    assert LV.regrid_boxes(spec, none, keep=fine) == [((2, 2, 2), (4, 4, 4))]
+    assert LV.regrid_boxes(spec, none, keep=(bl["level"] == 0)) == []
+    assert LV.regrid_boxes(spec, fine, keep=fine) == LV.regrid_boxes(spec, fine)
 
 
 PATCHES = ((8, 4, 4), [(1, 0, (2, 2, 2), (4, 4, 4)), (1, 0, (10, 2, 2), (4, 4, 4)),
@@ -251,3 +257,29 @@ def test_regrid_patches_clusters():
     pt = LV.regrid_patches(spec, ends, max_levels=2)
     assert [p[0] for p in pt] == [1, 1]
     LV.generate_patches(M0, pt)
+
+
+def test_evolve_norm_mask_counts_each_point_once():
+    """The full-evolution driver's constraint-norm mask: with no puncture
+    radii it holds every independent point of a level mesh exactly once (the
+    zone-owned nodes; patch-boundary nodes are filled from the coarser level
+    and counted there where they coincide with a coarse node), and its boxes
+    are the nested centred boxes."""
+    torch = pytest.importorskip("torch")
+    from bssn_b200 import evolve as EV
+    from bssn_b200 import levels as LV
+    assert EV.nested_boxes(24, 3) == [((12,) * 3, (24,) * 3), ((36,) * 3, (24,) * 3)]
+    spec = LV.generate_levels((4, 4, 4), EV.nested_boxes(4, 3), xmin=-8.0, L=16.0)
+    m = EV.norm_mask(spec, radii=(0.0, 0.0))
+    pts = set()
+    for g in spec.grids():
+        nx, ny, nz = g["dims"]
+        for k in range(nz):
+            for j in range(ny):
+                for i in range(nx):
+                    if g["level"] > 0 and (min(i, j, k) == 0 or i == nx - 1 or j == ny - 1 or k == nz - 1):
+                        continue
+                    pts.add(tuple(round((g["origin"][d] + e * g["h"]) * 1024) for d, e in enumerate((i, j, k))))
+    assert int(m.sum()) == len(pts)
+    m2 = EV.norm_mask(spec)
+    assert 0 < int(m2.sum()) < int(m.sum())
