@@ -313,3 +313,20 @@ def test_constraints_on_level_mesh(name, O):
     assert not got[:, ~own].any()
     err = ol.rel_err(ref, got)
     assert err.max() <= 1e-12, err
+
+
+def test_full_evolution_driver_small():
+    """The full-evolution driver on a small 3-level mesh: the exact run and
+    the learned run (two networks trained on the exact run's refine and keep
+    labels) both evolve 20 steps with a remesh test every 5, stay finite with
+    no enforcement violation, and report four constraint-norm entries plus
+    the final one, and the decision counters."""
+    from bssn_b200 import evolve as EV
+    res = EV.main(["--M0", "8", "--levels", "3", "--max-levels", "3", "--steps", "20", "--remesh-every", "5",
+                   "--diag-every", "5", "--train-steps", "50"])
+    for r in (res["exact"], res["learned"]):
+        assert r["finite"] and r["violations"] == 0
+        assert r["tests"] == 3 and len(r["history"]) == 5
+        assert all(np.isfinite(h[2:]).all() and h[2] > 0 for h in map(np.asarray, r["history"]))
+    assert res["exact"]["exact_refinements"] > 0 and res["exact"]["exact_keeps"] > 0
+    assert res["compare"]["exact_refinements_learned_run"] > 0
