@@ -283,3 +283,17 @@ def test_evolve_norm_mask_counts_each_point_once():
     assert int(m.sum()) == len(pts)
     m2 = EV.norm_mask(spec)
     assert 0 < int(m2.sum()) < int(m.sum())
+
+
+def test_evolve_remesh_rule():
+    """The driver rebuilds the mesh only when the regrid asks for a level
+    more or less, a box reaching outside the current one, or a current box
+    more than twice the volume asked for."""
+    from bssn_b200 import evolve as EV
+    cur = [((2, 2, 2), (8, 8, 8)), ((6, 6, 6), (8, 8, 8))]
+    assert not EV.needs_remesh(cur, cur)
+    assert not EV.needs_remesh(cur, [((2, 2, 2), (8, 8, 6)), ((6, 6, 6), (8, 8, 8))])
+    assert EV.needs_remesh(cur, cur[:1])
+    assert EV.needs_remesh(cur, [((0, 2, 2), (8, 8, 8)), ((6, 6, 6), (8, 8, 8))])
+    assert EV.needs_remesh(cur, [((2, 2, 2), (8, 8, 10)), ((6, 6, 6), (8, 8, 8))])
+    assert EV.needs_remesh(cur, [((2, 2, 2), (4, 8, 6)), ((6, 6, 6), (8, 8, 8))])
