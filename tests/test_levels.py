@@ -297,3 +297,20 @@ def test_evolve_remesh_rule():
     assert EV.needs_remesh(cur, [((0, 2, 2), (8, 8, 8)), ((6, 6, 6), (8, 8, 8))])
     assert EV.needs_remesh(cur, [((2, 2, 2), (8, 8, 10)), ((6, 6, 6), (8, 8, 8))])
     assert EV.needs_remesh(cur, [((2, 2, 2), (4, 8, 6)), ((6, 6, 6), (8, 8, 8))])
+
+
+def test_remesh_decision_thresholds():
+    """The learned decision's thresholds (host logic): at most half the
+    missed-refinement budget of the validation positives lies at or below lo,
+    at most the false-refinement budget of the negatives at or above hi, and
+    lo <= hi."""
+    from bssn_b200.remesh_train import pick_thresholds
+    rng = np.random.default_rng(4)
+    y = (rng.random(40000) < 0.3).astype(np.float32)
+    p = np.clip(np.where(y > 0.5, rng.beta(8, 2, y.size), rng.beta(2, 8, y.size)), 0, 1).astype(np.float32)
+    for fn, fp in ((1e-3, 1e-3), (2e-4, 1e-2)):
+        lo, hi = pick_thresholds(p, y, fn_target=fn, fp_target=fp)
+        pos, neg = p[y > 0.5], p[y < 0.5]
+        assert lo <= hi
+        assert (pos <= lo).mean() <= fn / 2
+        assert (neg >= hi).mean() <= fp
