@@ -68,4 +68,10 @@ __host__ __device__ inline AxisCoef axis_coef(double h) {
 
 inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? 0 : -(int)e; }
 
+// Raises a kernel's dynamic shared-memory limit to `bytes` on the current
+// device, once per (kernel, device) pair.  The attribute belongs to the
+// device, so a process that launches on several devices needs it set on each
+// of them; calls from several host threads are serialised.
+int set_smem_limit(const void* kernel, int bytes);
+
 }  // namespace bssn

@@ -5,6 +5,9 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <mutex>
+#include <set>
+#include <utility>
 #include <vector>
 
 #include "bssn_b200.h"
@@ -538,3 +541,21 @@ int bssn_tile_info(int tile, int info[4]) {
 }
 
 }  // extern "C"
+
+namespace bssn {
+
+int set_smem_limit(const void* kernel, int bytes) {
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;  // (kernel, device)
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e);
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.count({kernel, dev})) return 0;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return cuda_status(e);
+    done.insert({kernel, dev});
+    return 0;
+}
+
+}  // namespace bssn

@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "bssn_b200.h"
@@ -154,6 +155,43 @@ int enforce_bssn_constraints(double** u, unsigned begin, unsigned end, double ch
     if ((r = st(cudaMemcpyAsync(&bad, status, sizeof(int), cudaMemcpyDeviceToHost, s)))) return r;
     if ((r = st(cudaStreamSynchronize(s)))) return r;
     return -bad;
+}
+
+// ---- reference-signature forms ---------------------------------------------
+namespace {
+std::mutex g_cfg_mu;
+BssnParams g_params = {0.4, {1, 1, 1, 1}, {1.0, 0.0}, 2.0, 2.0, 40.0, 0, 0.99, 0.3, 1e-4};
+Domain g_domain = {{-1.0, -1.0, -1.0}, {1.0, 1.0, 1.0}, {0u, 0u, 0u}, {1u, 1u, 1u}};
+thread_local int t_last_status = 0;
+}  // namespace
+
+void set_params(const BssnParams& p) {
+    std::lock_guard<std::mutex> lock(g_cfg_mu);
+    g_params = p;
+}
+BssnParams get_params() {
+    std::lock_guard<std::mutex> lock(g_cfg_mu);
+    return g_params;
+}
+void set_domain(const Domain& d) {
+    std::lock_guard<std::mutex> lock(g_cfg_mu);
+    g_domain = d;
+}
+Domain get_domain() {
+    std::lock_guard<std::mutex> lock(g_cfg_mu);
+    return g_domain;
+}
+int last_status() { return t_last_status; }
+void set_last_status(int status) { t_last_status = status; }
+
+void bssnrhs(double** rhs, const double** u, const unsigned int& offset, const double* ptmin,
+             const double* ptmax, const unsigned int* sz, const unsigned int& bflag, const double t,
+             const double** cons) {
+    t_last_status = bssnrhs(rhs, u, offset, ptmin, ptmax, sz, bflag, get_params(), t, cons);
+}
+
+void enforce_bssn_constraints(double** u, unsigned int node) {
+    t_last_status = enforce_bssn_constraints(u, node, node + 1, get_params().chi_floor);
 }
 
 }  // namespace dendro_b200

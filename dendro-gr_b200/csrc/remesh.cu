@@ -473,12 +473,8 @@ int launch_mlp_grad(const void* wq, const float* norm, const float* X, const flo
     float* gpart = scratch;
     float* lpart = gpart + (size_t)parts * MLP_NPARAM;
     const size_t smem = sizeof(float) * (MLP_NPARAM + MLP_THREADS * (IN + 4 * HID + 2));
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return cuda_status(e);
-        attr = true;
-    }
+    const int st = set_smem_limit((const void*)mlp_grad_kernel, (int)smem);
+    if (st) return st;
     mlp_grad_kernel<<<parts, MLP_THREADS, smem, s>>>((const __nv_bfloat16*)wq, norm, X, Y, C, n, gpart, lpart);
     mlp_reduce_kernel<<<(MLP_NPARAM + MLP_THREADS - 1) / MLP_THREADS, MLP_THREADS, 0, s>>>(gpart, parts, grad);
     if (loss) mlp_loss_reduce_kernel<<<1, 32, 0, s>>>(lpart, parts, loss);

@@ -145,16 +145,7 @@ const TileEntry* tile_table(int* count) {
 
 int prepare(const TileEntry& t) {
     if (t.mode == 1) return prepare_split(t.shape);
-    static bool done[16] = {false};
-    int count;
-    const TileEntry* base = tile_table(&count);
-    const int id = (int)(&t - base);
-    if (!done[id]) {
-        cudaError_t e1 = cudaFuncSetAttribute(t.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem);
-        if (e1 != cudaSuccess) return cuda_status(e1);
-        done[id] = true;
-    }
-    return 0;
+    return set_smem_limit((const void*)t.kern, (int)t.smem);
 }
 }  // namespace
 

@@ -319,23 +319,13 @@ int split_zone_count(int shape) {
 }
 
 int prepare_split(int shape) {
-    static bool done[8] = {false};
     int c;
     const SplitEntry* t = split_table(&c);
     if (shape < 0 || shape >= c) return BSSN_EINVAL;
-    if (!done[shape]) {
-        cudaError_t e = cudaFuncSetAttribute(t[shape].deriv, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)t[shape].smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(t[shape].deriv_zip, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)t[shape].smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(t[shape].eq, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)eq_smem_bytes());
-        if (e != cudaSuccess) return cuda_status(e);
-        done[shape] = true;
-    }
-    return 0;
+    int st = set_smem_limit((const void*)t[shape].deriv, (int)t[shape].smem);
+    if (!st) st = set_smem_limit((const void*)t[shape].deriv_zip, (int)t[shape].smem);
+    if (!st) st = set_smem_limit((const void*)t[shape].eq, (int)eq_smem_bytes());
+    return st;
 }
 
 int launch_rhs_split(int shape, const RhsArgs& A, const BssnBlockDesc* blocks_dev,

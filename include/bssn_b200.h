@@ -276,7 +276,9 @@ int bssn_remesh_mlp_bwd_bf16(const void* wq_dev, const float* norm_dev,
  * up the array's device address (cudaGetSymbolAddress) with that device
  * current; make that first call before any stream capture.  All calls on a
  * device share the array, so calls whose kernels overlap on the GPU (for
- * example issued on two streams) race on it; serialise them. */
+ * example issued on two streams) race on it; serialise them.  The address is
+ * kept for the life of the process: a device reset (cudaDeviceReset) is not
+ * supported between calls. */
 int bssn_remesh_mlp_bwd_noalloc_bf16(const void* wq_dev, const float* norm_dev,
                                      const float* x_dev, const float* y_dev,
                                      const float* c_dev, int n, float* grad_dev,

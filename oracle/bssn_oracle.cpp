@@ -804,18 +804,22 @@ void orc_zip(double** zip, const double** unzip, const OrcBlock* blks,
     }
 }
 
-int64_t orc_rk4_step(double** u, const OrcBlock* blks, int nblk,
-                     const int32_t* G, int64_t n_unzip, double dt,
-                     const OrcParams* prm, double chi_floor,
-                     int enforce_stages, int nthreads) {
+int64_t orc_rk4_step_ws(double** u, const OrcBlock* blks, int nblk, const int32_t* G,
+                        int64_t n_unzip, double dt, const OrcParams* prm, double chi_floor,
+                        int enforce_stages, int nthreads, orc_rhs_fn rhs, double* ws) {
     static const double RK4_C[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
     static const double RK4_U[4] = {0.0, 1.0 / 2.0, 1.0 / 2.0, 1.0};
     const int64_t N = (int64_t)G[0] * G[1] * G[2];
-    std::vector<double> prev(NVARS * N), im(NVARS * N), kst(4 * NVARS * N);
-    std::vector<double> uz(NVARS * n_unzip, 0.0), rz(NVARS * n_unzip, 0.0);
+    if (!rhs) rhs = orc_bssnRHS;
+    double* prev = ws;
+    double* im = prev + NVARS * N;
+    double* kst = im + NVARS * N;
+    double* uz = kst + 4 * NVARS * N;
+    double* rz = uz + NVARS * n_unzip;
     double *pu[NVARS], *pim[NVARS], *puz[NVARS], *prz[NVARS];
+#pragma omp parallel for
+    for (int v = 0; v < NVARS; v++) std::memcpy(&prev[v * N], u[v], N * sizeof(double));
     for (int v = 0; v < NVARS; v++) {
-        std::memcpy(&prev[v * N], u[v], N * sizeof(double));
         pu[v] = u[v];
         pim[v] = &im[v * N];
         puz[v] = &uz[v * n_unzip];
@@ -825,7 +829,7 @@ int64_t orc_rk4_step(double** u, const OrcBlock* blks, int nblk,
     for (int stage = 0; stage < 4; stage++) {
         double** cur = stage == 0 ? pu : pim;
         orc_unzip(puz, (const double**)cur, blks, nblk, G, NVARS);
-        orc_bssnRHS(prz, (const double**)puz, blks, nblk, prm, nthreads);
+        rhs(prz, (const double**)puz, blks, nblk, prm, nthreads);
         double* ks[NVARS];
         for (int v = 0; v < NVARS; v++) ks[v] = &kst[(stage * NVARS + v) * N];
         orc_zip(ks, (const double**)prz, blks, nblk, G, NVARS);
@@ -850,6 +854,126 @@ int64_t orc_rk4_step(double** u, const OrcBlock* blks, int nblk,
         bad += enforce_node(pu, node, chi_floor);
     }
     return bad;
+}
+
+int64_t orc_rk4_ws_doubles(const int32_t* G, int64_t n_unzip) {
+    const int64_t N = (int64_t)G[0] * G[1] * G[2];
+    return NVARS * (6 * N + 2 * n_unzip);
+}
+
+int64_t orc_rk4_step(double** u, const OrcBlock* blks, int nblk,
+                     const int32_t* G, int64_t n_unzip, double dt,
+                     const OrcParams* prm, double chi_floor,
+                     int enforce_stages, int nthreads) {
+    std::vector<double> ws((size_t)orc_rk4_ws_doubles(G, n_unzip), 0.0);
+    return orc_rk4_step_ws(u, blks, nblk, G, n_unzip, dt, prm, chi_floor, enforce_stages,
+                           nthreads, orc_bssnRHS, ws.data());
+}
+
+// ---------------------------------------------------------------------------
+// Synthetic single-level octree meshes (the workloads' block lists), restated
+// from the definition the product library's generator documents: mode 0 = a
+// uniform dims[0]^3 grid of single-octant blocks (13^3); mode 1 = dims
+// super-cells of 8^3 octants, visited in a seeded order, each split top-down
+// (children in Morton order) where a uniform draw is not below the
+// probability of staying whole, which follows from the target block-count
+// fractions p = {p13, p19, p31, p55}.  Block b of w octants per side has
+// padded side 6w + 7, its first interior node at 6 * octant origin, and its
+// padded array at the running offset, each array rounded up to an even
+// number of doubles.
+// ---------------------------------------------------------------------------
+namespace {
+struct MeshRng {
+    uint64_t s;
+    uint64_t next() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ULL);  // splitmix64
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        return z ^ (z >> 31);
+    }
+    double uniform() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); }
+};
+struct Oct {
+    int o[3];
+    int w;
+};
+void split_oct(const Oct& c, const double stay[4], MeshRng& r, std::vector<Oct>& out) {
+    const int lvl = c.w == 8 ? 3 : (c.w == 4 ? 2 : (c.w == 2 ? 1 : 0));
+    if (c.w == 1 || r.uniform() < stay[lvl]) {
+        out.push_back(c);
+        return;
+    }
+    const int h = c.w / 2;
+    for (int m = 0; m < 8; m++)
+        split_oct(Oct{{c.o[0] + (m & 1) * h, c.o[1] + ((m >> 1) & 1) * h, c.o[2] + ((m >> 2) & 1) * h}, h},
+                  stay, r, out);
+}
+}  // namespace
+
+int orc_mesh_generate(int mode, const int32_t* dims, const double* p, uint64_t seed, double xmin,
+                      double L, OrcBlock* blks, int* nblk, int32_t* G, double* h_out) {
+    std::vector<Oct> cubes;
+    int M[3];
+    if (mode == 0) {
+        const int n = dims[0];
+        if (n < 1) return 1;
+        M[0] = M[1] = M[2] = n;
+        for (int z = 0; z < n; z++)
+            for (int y = 0; y < n; y++)
+                for (int x = 0; x < n; x++) cubes.push_back(Oct{{x, y, z}, 1});
+    } else if (mode == 1) {
+        for (int d = 0; d < 3; d++) {
+            if (dims[d] < 1) return 1;
+            M[d] = 8 * dims[d];
+        }
+        if (p[0] <= 0 || p[1] <= 0 || p[2] <= 0 || p[3] <= 0) return 1;
+        // expected blocks per super-cell: a, 8(1-a)b, 64(1-a)(1-b)c,
+        // 512(1-a)(1-b)(1-c) for sides 55, 31, 19, 13 (a, b, c = probability
+        // of staying whole at widths 8, 4, 2), solved for the fractions p
+        const double c = 8.0 / (8.0 + p[0] / p[1]);
+        const double b = 8.0 * c / (8.0 * c + p[1] / p[2]);
+        const double a = 8.0 * b / (8.0 * b + p[2] / p[3]);
+        const double stay[4] = {1.0, c, b, a};
+        MeshRng r{seed};
+        const int ns = dims[0] * dims[1] * dims[2];
+        std::vector<int> order(ns);
+        for (int i = 0; i < ns; i++) order[i] = i;
+        for (int i = ns - 1; i > 0; i--) std::swap(order[i], order[(int)(r.next() % (uint64_t)(i + 1))]);
+        for (int t = 0; t < ns; t++) {
+            const int id = order[t];
+            const int sx = id % dims[0], sy = (id / dims[0]) % dims[1], sz = id / (dims[0] * dims[1]);
+            split_oct(Oct{{8 * sx, 8 * sy, 8 * sz}, 8}, stay, r, cubes);
+        }
+    } else {
+        return 1;
+    }
+    for (int d = 0; d < 3; d++) G[d] = 6 * M[d] + 1;
+    const int Mmax = std::max(M[0], std::max(M[1], M[2]));
+    const double h = L / Mmax / 6.0;
+    *h_out = h;
+    *nblk = (int)cubes.size();
+    if (!blks) return 0;
+    int64_t off = 0;
+    for (size_t b = 0; b < cubes.size(); b++) {
+        const Oct& c = cubes[b];
+        OrcBlock d;
+        std::memset(&d, 0, sizeof(d));
+        const int s = 6 * c.w + 7;
+        d.offset = off;
+        d.sz = s;
+        for (int k = 0; k < 3; k++) {
+            d.g0[k] = 6 * c.o[k];
+            if (c.o[k] == 0) d.bflag |= 1u << (2 * k);
+            if (c.o[k] + c.w == M[k]) d.bflag |= 1u << (2 * k + 1);
+            d.ptmin[k] = xmin + (double)(d.g0[k] - 3) * h;
+            d.ptmax[k] = xmin + (double)(d.g0[k] - 3 + s - 1) * h;
+        }
+        d.level = c.w == 1 ? 3 : (c.w == 2 ? 2 : (c.w == 4 ? 1 : 0));
+        blks[b] = d;
+        const int64_t npts = (int64_t)s * s * s;
+        off += (npts + 1) / 2 * 2;
+    }
+    return 0;
 }
 
 // Hamiltonian and momentum constraints (CodeGen/constraints.py:250-283):

@@ -104,6 +104,23 @@ int64_t orc_rk4_step(double** u, const OrcBlock* blks, int nblk,
                      const int32_t* G, int64_t n_unzip, double dt,
                      const OrcParams* prm, double chi_floor,
                      int enforce_stages, int nthreads);
+/* The same step with a caller-provided workspace of orc_rk4_ws_doubles()
+ * doubles and the block-loop right-hand side as a parameter: orc_bssnRHS
+ * (NULL) or any function of the same form -- the reference's own compiled
+ * block loop (ref_bssnRHS_blocks in oracle/_ref, same block and parameter
+ * layouts) turns this into the reference CPU RK4 step. */
+typedef void (*orc_rhs_fn)(double** rhs, const double** u, const OrcBlock* blks, int nblk,
+                           const OrcParams* prm, int nthreads);
+int64_t orc_rk4_ws_doubles(const int32_t* G, int64_t n_unzip);
+int64_t orc_rk4_step_ws(double** u, const OrcBlock* blks, int nblk, const int32_t* G,
+                        int64_t n_unzip, double dt, const OrcParams* prm, double chi_floor,
+                        int enforce_stages, int nthreads, orc_rhs_fn rhs, double* ws);
+
+/* --- the workloads' synthetic single-level octree meshes (block lists; see
+ * bssn_oracle.cpp).  blks NULL: only *nblk, G and *h are set.  0 = ok. */
+int orc_mesh_generate(int mode, const int32_t* dims, const double* p, uint64_t seed,
+                      double xmin, double L, OrcBlock* blks, int* nblk, int32_t* G,
+                      double* h);
 
 /* --- Hamiltonian and momentum constraints (BSSN_GR/src/physcon.cpp:12-89,
  * equations from CodeGen/constraints.py) on a block's interior, and the

@@ -99,10 +99,58 @@ class Oracle:
                                                    C.c_uint(bflag), C.byref(prm), P(ws))
         return R
 
+    def enforce(self, U, chi_floor=1e-4):
+        """enforce_bssn_constraints on every column of a (24, n) array, in
+        place; returns the number of violating nodes."""
+        self.lib.orc_enforce.restype = C.c_int64
+        return self.lib.orc_enforce(rows(U), C.c_int64(U.shape[1]), C.c_double(chi_floor))
+
 
 def oracle():
     build_oracle()
     return Oracle()
+
+
+class OrcBlock(C.Structure):
+    _fields_ = [("offset", C.c_int64), ("sz", C.c_int32), ("bflag", C.c_uint32),
+                ("g0", C.c_int32 * 3), ("level", C.c_int32),
+                ("ptmin", C.c_double * 3), ("ptmax", C.c_double * 3)]
+
+
+class OracleMeshSpec:
+    """A workload mesh built by the oracle's own generator (no product
+    library involved): the same attributes MeshOracle reads from the
+    library's MeshSpec."""
+
+    def __init__(self, mode, dims, p=(0.7, 0.2, 0.08, 0.02), seed=0, xmin=-8.0, L=16.0, lib=None):
+        lib = (lib or oracle()).lib
+        d = (C.c_int32 * 3)(*dims)
+        pp = (C.c_double * 4)(*p)
+        n = C.c_int(0)
+        G = (C.c_int32 * 3)()
+        h = C.c_double(0)
+        lib.orc_mesh_generate.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_uint64, C.c_double,
+                                          C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        for blocks in (None, True):
+            if blocks:
+                blocks = (OrcBlock * n.value)()
+            rc = lib.orc_mesh_generate(mode, d, pp, seed, xmin, L, blocks, C.byref(n), G, C.byref(h))
+            assert rc == 0, rc
+        self.blocks, self.nblocks = blocks, n.value
+        self.G, self.h, self.xmin = tuple(G), h.value, xmin
+        self.sides = np.array([blocks[b].sz for b in range(n.value)], dtype=np.int32)
+
+    @property
+    def n_nodes(self):
+        return int(self.G[0]) * int(self.G[1]) * int(self.G[2])
+
+    @property
+    def n_unzip(self):
+        b = self.blocks[self.nblocks - 1]
+        return int(b.offset) + int(b.sz) ** 3
+
+    def zones(self):
+        return int(sum((int(s) - 6) ** 3 for s in self.sides))
 
 
 def reference():
@@ -154,6 +202,25 @@ class MeshOracle:
                                   C.c_double(m2), C.c_double(chi_floor), C.c_double(eps),
                                   C.c_uint64(seed))
         return Z
+
+    def rk4_workspace(self):
+        self.lib.orc_rk4_ws_doubles.restype = C.c_int64
+        n = self.lib.orc_rk4_ws_doubles(self.G, C.c_int64(self.spec.n_unzip))
+        return np.zeros(n)
+
+    def rk4_step_ws(self, Z, dt, prm, ws, rhs_fn=None, chi_floor=1e-4, enforce_stages=True,
+                    nthreads=0):
+        """One RK4 step in a persistent workspace (rk4_workspace()); rhs_fn:
+        the block-loop right-hand side (a ctypes function pointer, e.g. the
+        reference's own ref_bssnRHS_blocks) or None for the oracle's."""
+        self.lib.orc_rk4_step_ws.restype = C.c_int64
+        self.lib.orc_rk4_step_ws.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int64,
+                                             C.c_double, C.c_void_p, C.c_double, C.c_int, C.c_int,
+                                             C.c_void_p, C.c_void_p]
+        fn = C.cast(rhs_fn, C.c_void_p) if rhs_fn is not None else None
+        return self.lib.orc_rk4_step_ws(rows(Z), self.spec.blocks, self.spec.nblocks, self.G,
+                                        self.spec.n_unzip, dt, C.byref(prm), chi_floor,
+                                        int(enforce_stages), nthreads, fn, P(ws))
 
     def rk4_step(self, Z, dt, prm, chi_floor=1e-4, enforce_stages=True, nthreads=0):
         self.lib.orc_rk4_step.restype = C.c_int64

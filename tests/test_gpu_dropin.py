@@ -56,3 +56,27 @@ def test_dropin_stencils_bit_exact(exe, tmp_path):
             got = np.fromfile(fout)
             ref = O.stencil(kind, u, 0.3, (side, side, side), bflag)
             assert np.array_equal(got.view(np.uint64), ref.view(np.uint64)), (kind, bflag)
+
+
+def test_dropin_reference_signatures(exe, tmp_path):
+    """The reference's own argument lists (rhs.h:28-36 with t and
+    uZipConstVars, bssn_constraints.h:15 per node): bssnrhs and the
+    block-list bssnRHS over a stand-in ot::Block agree bit for bit, match the
+    oracle at 1e-12, and per-node enforcement matches the oracle's."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_golden as mg
+    side, bflag = 13, 21
+    U, _, _ = mg.golden_input(side, 0.25, (-1.0, -0.8, -1.1), 1e-8, 91)
+    fin, frhs, fenf = (str(tmp_path / f) for f in ("u.bin", "r.bin", "e.bin"))
+    U.tofile(fin)
+    subprocess.run([exe, "refsig", str(side), str(bflag), fin, frhs, fenf], check=True)
+    raw = np.fromfile(frhs)
+    R, pmin, pmax = raw[:-6].reshape(24, -1), raw[-6:-3], raw[-3:]
+    ref = ol.oracle().bssnrhs(U, 0, pmin, pmax, side, bflag, ol.params())
+    err = ol.rel_err(mg.interior(ref, side), mg.interior(R, side))
+    assert err.max() <= 1e-12, err.max()
+    E = np.fromfile(fenf).reshape(24, -1)
+    want = U.copy()
+    assert ol.oracle().enforce(want, 1e-4) == 0
+    assert ol.rel_err(want, E).max() <= 1e-14
