@@ -67,6 +67,8 @@ FLOP_PER_ZONE_STAGE = 6535.0  # 6,439 RHS + 96 RK axpy (per zone, per stage)
 
 
 SPLIT_SLOTS = 162  # scratch doubles per zone of the split right-hand side
+KIND_NAMES = {"fused": "bssn::rhs_kernel / bssn::onchip_kernel (one-kernel right-hand side)",
+              "deriv": "bssn::deriv_kernel (derivative pass)", "eq": "bssn::eq_kernel (equation pass)"}
 
 
 def tile_pins(arg):
@@ -78,56 +80,49 @@ def tile_pins(arg):
     return {int(a): int(b) for a, b in (kv.split(":") for kv in arg.split(","))}
 
 
-def kernel_bytes(sides, chosen, modes, n_nodes, direct):
-    """Algorithmic HBM bytes of one right-hand-side pass per kernel kind, as
-    the plan's timing call runs it.
-    Direct form: the derivative pass reads the 24 zipped variables once and
-    writes 162 derivative doubles per node; the equation pass reads them and
-    the node's 24 variables and writes its 24 right-hand sides.
-    Every bucket split (zipped right-hand side): the derivative pass reads
-    the 24 padded variables once (192 B per padded point) and writes 162
-    doubles per node, from the zone owning it; the equation pass reads those
-    and the node's 24 variables and writes its 24 right-hand sides.
-    Otherwise, per block by the tile chosen for its side: fused reads the 24
-    padded variables and writes the 24 interior right-hand sides; split
-    writes / reads 162 derivative doubles per interior zone in between."""
-    out = {"fused": 0, "deriv": 0, "eq": 0}
-    n_nodes = int(n_nodes)
-    if direct:
-        out["deriv"] = 8 * (24 + SPLIT_SLOTS) * n_nodes
-        out["eq"] = 8 * (SPLIT_SLOTS + 24 + 24) * n_nodes
-        return out
-    if all(modes[chosen[int(s)]] == 1 for s in sides):
-        out["deriv"] = 8 * (24 * sum(int(s) ** 3 for s in sides) + SPLIT_SLOTS * n_nodes)
-        out["eq"] = 8 * (SPLIT_SLOTS + 24 + 24) * n_nodes
-        return out
+def kernel_bytes(sides, chosen, modes):
+    """Algorithmic HBM bytes of one right-hand-side pass per kernel kind, by
+    the compulsory-traffic rule of the hot-path contract (24 FP64 variables):
+    a one-kernel right-hand side (fused or on chip) reads each padded block
+    once and writes the interior: 192 (s^3 + (s-6)^3) per block; the split
+    path's derivative pass reads the padded block, 192 s^3, and its equation
+    pass reads and writes the zone's variables, 384 (s-6)^3.  The split
+    path's derivative scratch (162 doubles written and read per zone) is not
+    algorithmic: it is returned separately as overhead."""
+    out = {"fused": 0, "deriv": 0, "eq": 0, "overhead": 0}
     for s in sides:
         s = int(s)
         pad, inner = s ** 3, (s - 6) ** 3
-        if modes[chosen[s]] == 0:
-            out["fused"] += 8 * 24 * (pad + inner)
+        if modes[chosen[s]] == 1:
+            out["deriv"] += 192 * pad
+            out["eq"] += 384 * inner
+            out["overhead"] += 2 * 8 * SPLIT_SLOTS * inner
         else:
-            out["deriv"] += 8 * (24 * pad + SPLIT_SLOTS * inner)
-            out["eq"] += 8 * (SPLIT_SLOTS + 24 + 24) * inner
+            out["fused"] += 192 * (pad + inner)
     return out
 
 
-# DRAM traffic / algorithmic bytes of each kernel (dram__bytes_read.sum +
-# dram__bytes_write.sum of one launch over that launch's algorithmic bytes),
-# from ncu captures of the 7x7x7 split tile on the uniform 512-block workload
-# (13^3 blocks); scales a full pass's algorithmic bytes to its DRAM traffic.
-TRAFFIC_RATIO = {"deriv": 1.09, "eq": 1.35}
+# DRAM traffic / algorithmic bytes of one launch of each kernel kind, from ncu
+# captures on small workloads (dram__bytes_read.sum + dram__bytes_write.sum
+# over the launch's algorithmic bytes as kernel_bytes counts them): split
+# 7x7x7 on the uniform 512-block workload; the on-chip kernel on the small
+# mixed workload.  Scales a full pass's algorithmic bytes to DRAM traffic.
+# (uniform 512: deriv 257.0 + 143.4 MB against 192 * 2197 * 512 B; eq 249.3 +
+# 17.9 MB against 384 * 343 * 512 B -- the scratch round trip is the excess)
+TRAFFIC_RATIO = {"deriv": 400.4e6 / (192 * 2197 * 512), "eq": 267.2e6 / (384 * 343 * 512)}
 
 
-def step_bytes(sides, n_nodes):
-    """Compulsory HBM bytes of one RK stage of the padded plan: ghost fill
-    (read zipped, write padded), right-hand side (read padded, write
-    interior), zip + update (read RHS, u, acc; write stage state and acc).
-    The split right-hand side's derivative round trip is not included."""
-    pad = sum(int(s) ** 3 for s in sides)
-    inner = sum((int(s) - 6) ** 3 for s in sides)
-    n_nodes = int(n_nodes)
-    return 8 * 24 * (n_nodes + pad + pad + inner + inner + 4 * n_nodes)
+def rhs_bytes(sides):
+    """The fused right-hand side's compulsory bytes per pass: 192 (s^3 + (s-6)^3) per block."""
+    return sum(192 * (int(s) ** 3 + (int(s) - 6) ** 3) for s in sides)
+
+
+def step_bytes(sides):
+    """Compulsory HBM bytes of one RK stage (the contract's full-stage rule):
+    192 (3 s^3 + 2 (s-6)^3) per block -- padded read by the right-hand side,
+    ghost fill write and read, stage-state, accumulator and next-state
+    traffic of the interior."""
+    return sum(192 * (3 * int(s) ** 3 + 2 * (int(s) - 6) ** 3) for s in sides)
 
 
 class Clocks:
@@ -211,100 +206,106 @@ def measured_peaks():
 
 
 # ---------------------------------------------------------------------------
-# reference arm: the reference's own CPU bssnrhs on the host cores
+# reference arm: the reference's own CPU RK4 step on the host cores
 # ---------------------------------------------------------------------------
-def cpu_reference_rate(sides_all, seconds=15.0, threads=0, target=2.5e6):
-    """Time the reference CPU right-hand side (oracle/_ref, compiled from the
-    reference sources; else the repository's CPU restatement) on a bounded,
-    size-stratified sample of the workload's blocks with all host threads.
-    Returns (zone-updates/s, info).  One RK4 zone-update = 4 RHS passes;
-    ghost fill, zip and the stage algebra are excluded (favours the CPU)."""
-    import numpy as np
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_lib as ol
+# The CPU step runs on a bounded sample of a workload: the same generator,
+# seed and size mix on fewer super-cells (3 x 3 x 3 of mix20k's 10 x 10 x 7:
+# 741 blocks, 3.35 M zones), so K steps finish within minutes on the host.
+REF_SAMPLE_DIMS = (3, 3, 3)
 
-    ref = ol.reference()
-    kind = "reference"
-    if ref is None:
-        ref = ol.oracle()
-        kind = "port"
-    rng = np.random.default_rng(1)
-    # stratified sample: keep the workload's size fractions, ~2.5M zones
-    sides_all = np.asarray(sides_all)
-    uniq, counts = np.unique(sides_all, return_counts=True)
-    zones_all = float(((sides_all - 6.0) ** 3).sum())
-    frac = min(1.0, target / zones_all)
-    sample = []
-    for s, c in zip(uniq, counts):
-        k = max(1, int(round(c * frac)))
-        sample += [int(s)] * k
-    # lay the sample out as independent blocks with BL-like data
-    offs, off = [], 0
-    for s in sample:
-        offs.append(off)
-        off += s ** 3
-    U = np.zeros((24, off))
-    U[[0, 1, 12, 15, 17]] = 1.0
-    U += 1e-8 * rng.uniform(-1, 1, U.shape)
-    blocks = []
-    for s, o in zip(sample, offs):
-        h = 0.05
-        pmin = rng.uniform(-6, 6, 3)
-        blocks.append((o, s, pmin, pmin + (s - 1) * h))
-    nthreads = threads or os.cpu_count()
 
-    class RB(C.Structure):
-        _fields_ = [("offset", C.c_int64), ("sz", C.c_int32), ("bflag", C.c_uint32),
-                    ("g0", C.c_int32 * 3), ("level", C.c_int32),
-                    ("ptmin", C.c_double * 3), ("ptmax", C.c_double * 3)]
-    arr = (RB * len(blocks))()
-    for i, (o, s, pm, px) in enumerate(blocks):
-        arr[i].offset, arr[i].sz, arr[i].bflag = o, s, 0
-        arr[i].ptmin[:] = list(pm)
-        arr[i].ptmax[:] = list(px)
-    R = np.zeros_like(U)
-    prm = ol.params()
-    fn = ref.lib.ref_bssnRHS_blocks if kind == "reference" else ref.lib.orc_bssnRHS
-    zones = float(sum((s - 6) ** 3 for s in sample))
-    t0 = time.perf_counter()
-    passes = 0
-    while True:
-        fn(ol.rows(R), ol.rows(U), arr, len(blocks), C.byref(prm), nthreads)
-        passes += 1
-        if time.perf_counter() - t0 > seconds and passes >= 4:
-            break
-    dt = time.perf_counter() - t0
-    rate = zones * passes / 4.0 / dt
-    return rate, {"kind": kind, "cores": nthreads,
-                  "sample": f"{len(sample)} blocks ({zones:.3g} zones) drawn with the "
-                            f"workload's size fractions; {passes} RHS passes in {dt:.1f} s; "
-                            "RHS only (ghost fill / zip / RK algebra excluded)"}
+def ref_sample(wl):
+    """(mode, dims, name) of the CPU sample of workload wl."""
+    mode, dims, _ = WORKLOADS[wl]
+    if mode == 0:
+        return mode, dims, wl
+    sd = tuple(min(a, b) for a, b in zip(dims, REF_SAMPLE_DIMS))
+    if sd == tuple(dims):
+        return mode, dims, wl
+    return mode, sd, f"{wl}-sample-{sd[0]}x{sd[1]}x{sd[2]}"
+
+
+class CpuRK4:
+    """The reference CPU RK4 step (ghost fill, the block-loop right-hand side,
+    zip, stage algebra and constraint enforcement of the oracle's restatement
+    of rkBSSN.cpp:764-860) with the right-hand side the reference's own
+    compiled bssnrhs (oracle/_ref, kind "reference"; the oracle's
+    restatement, kind "port", where that library is absent), on a mesh built
+    by the oracle's generator: the product library is not loaded."""
+
+    def __init__(self, mode, dims, threads=0):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib as ol
+        self.ol = ol
+        self.spec = ol.OracleMeshSpec(mode, dims, MIX, seed=SEED_MESH)
+        O = ol.oracle()
+        ref = ol.reference()
+        self.kind = "reference" if ref is not None else "port"
+        self.fn = ref.lib.ref_bssnRHS_blocks if ref is not None else None
+        self.mo = ol.MeshOracle(self.spec, O)
+        self.Z = self.mo.initial_data(eps=1e-8)
+        self.ws = self.mo.rk4_workspace()
+        self.dt = 0.25 * self.spec.h
+        self.prm = ol.params()
+        self.threads = threads or os.cpu_count()
+
+    def step(self):
+        t0 = time.perf_counter()
+        bad = self.mo.rk4_step_ws(self.Z, self.dt, self.prm, self.ws, rhs_fn=self.fn,
+                                  nthreads=self.threads)
+        assert bad == 0, f"{bad} enforcement violations"
+        return time.perf_counter() - t0
+
+
+def cpu_baseline(wl, steps=3, threads=0):
+    """Timed CPU RK4 steps on the workload's sample: (zone-updates/s, info)."""
+    mode, dims, name = ref_sample(wl)
+    c = CpuRK4(mode, dims, threads)
+    c.step()  # warm-up (page faults of the workspace)
+    ts = [c.step() for _ in range(steps)]
+    zones = c.spec.zones()
+    rate = zones * steps / sum(ts)
+    return rate, {"kind": c.kind, "cores": c.threads,
+                  "sample": f"{name}: {c.spec.nblocks} blocks, {zones} zones; {steps} full RK4 steps "
+                            f"(ghost fill, bssnrhs block loop, zip, stage algebra, enforcement), "
+                            f"{sum(ts):.1f} s"}
 
 
 def run_reference(args, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import bssn_b200 as B
     mode, dims, desc = WORKLOADS[wl]
-    spec = workload_spec(B, wl)
-    rates = []
+    if mode == 2:
+        print(json.dumps({"impl": "reference", "unavailable": "the CPU oracle has no multi-level "
+                          "ghost fill outside the test harness; run the single-level workloads"}))
+        return
+    smode, sdims, name = ref_sample(wl)
+    c = CpuRK4(smode, sdims)
     for _ in range(args.warmup):
-        cpu_reference_rate(spec.sides, seconds=2.0)
-    for _ in range(args.steps):
-        r, info = cpu_reference_rate(spec.sides, seconds=6.0)
-        rates.append(r)
-    rate = statistics.median(rates)
-    ms = spec.zones() / rate * 1e3
+        c.step()
+    ts = [c.step() for _ in range(args.steps)]
+    total = sum(ts)
+    zones = c.spec.zones()
+    rate = zones * args.steps / total
+    info = {"kind": c.kind, "cores": c.threads,
+            "sample": f"{name}: the workload's generator, seed and size mix on "
+                      f"{sdims[0]}x{sdims[1]}x{sdims[2]} super-cells ({c.spec.nblocks} blocks, {zones} zones); "
+                      "each step one full RK4 step"}
     out = {"metric": "BSSN RK4 zone-updates/s FP64 on 1 B200, batched vs plain; % HBM roofline",
            "impl": "reference", "value": rate, "unit": "zone-updates/s",
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": wl, "description": desc, "blocks": spec.nblocks},
-           "cpu_baseline": dict(info, value=rate, unit="zone-updates/s"),
+           "config": {"workload": name, "sampled_from": wl, "description": desc,
+                      "blocks": c.spec.nblocks, "zones": zones, "nodes": c.spec.n_nodes,
+                      "path": "reference CPU RK4 step: oracle ghost fill + the reference's compiled "
+                              "bssnrhs block loop (OpenMP over blocks) + zip + stage algebra + "
+                              "enforce_bssn_constraints"},
+           "cpu_baseline": dict(info, value=rate, unit="zone-updates/s", cpu_model=cpu_model()),
            "e2e": {"value": rate, "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
-                   "d2h_bytes_per_step": 0}}
+                   "d2h_bytes_per_step": 0},
+           "step_seconds": ts}
     print(json.dumps(out, default=_plain))
 
 
@@ -597,21 +598,20 @@ def main():
     peaks, peak_src = measured_peaks()
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     modes = [B.tile_mode(t) for t in range(len(B.tiles()))]
-    kb = kernel_bytes(spec.sides, chosen, modes, spec.n_nodes, direct=False)
-    names = {"fused": "bssn::rhs_kernel (fused RHS)", "deriv": "bssn::deriv_kernel (derivative pass)",
-             "eq": "bssn::eq_kernel (equation pass)"}
+    kb = kernel_bytes(spec.sides, chosen, modes)
     kernels = {}
     for k, key in enumerate(("fused", "deriv", "eq")):
         ms, n = kt[k], kt[3 + k]
         if n <= 0:
             continue
         gbs = kb[key] / (ms * 1e-3) / 1e9
-        kernels[key] = {"kernel": names[key], "ms_per_pass": ms, "launches_per_pass": n,
+        kernels[key] = {"kernel": KIND_NAMES[key], "ms_per_pass": ms, "launches_per_pass": n,
                         "bytes_per_pass": kb[key], "achieved_gbs": gbs, "frac": gbs / hbm_peak}
     dom = max(kernels, key=lambda k: kernels[k]["ms_per_pass"])
     d = kernels[dom]
     ratio = TRAFFIC_RATIO.get(dom)
     flops_rhs = zones * FLOP_PER_ZONE_STAGE
+    rb = rhs_bytes(spec.sides)
     roofline = {"bound": "hbm", "kernel": d["kernel"],
                 "achieved": d["achieved_gbs"], "peak": hbm_peak, "unit": "GB/s",
                 "frac": d["frac"], "peak_source": peak_src,
@@ -619,12 +619,15 @@ def main():
                 "launch_ms": d["ms_per_pass"] / d["launches_per_pass"],
                 "bytes_per_launch": d["bytes_per_pass"] / d["launches_per_pass"],
                 "kernels": kernels,
-                "rhs_pass_ms": rhs_ms.value,
+                "split_scratch_overhead_bytes_per_pass": kb["overhead"],
+                "rhs_pass": {"ms": rhs_ms.value, "algorithmic_bytes": rb,
+                             "achieved_gbs": rb / (rhs_ms.value * 1e-3) / 1e9,
+                             "frac": rb / (rhs_ms.value * 1e-3) / 1e9 / hbm_peak},
                 "fp64": {"achieved_tflops": flops_rhs / (rhs_ms.value * 1e-3) / 1e12,
                          "peak_tflops": fp64.value, "peak_source": "measured FMA probe",
                          "frac": flops_rhs / (rhs_ms.value * 1e-3) / 1e12 / fp64.value,
-                         "scope": "whole right-hand-side pass"}}
-    sb = step_bytes(spec.sides, spec.n_nodes) * 4
+                         "scope": "whole right-hand-side pass, 6,535 FP64 operations per zone"}}
+    sb = step_bytes(spec.sides) * 4
     out = {"metric": "BSSN RK4 zone-updates/s FP64 on 1 B200, batched vs plain; % HBM roofline",
            "value": value, "unit": "zone-updates/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
@@ -639,18 +642,20 @@ def main():
                                  if getattr(spec, "boxes", None) else None)},
            "roofline": roofline,
            "step_hbm": {"bytes_per_step": sb, "achieved_gbs": sb / (ms_step * 1e-3) / 1e9,
-                        "frac": sb / (ms_step * 1e-3) / 1e9 / hbm_peak},
+                        "frac": sb / (ms_step * 1e-3) / 1e9 / hbm_peak,
+                        "rule": "192 (3 s^3 + 2 (s-6)^3) bytes per block and RK stage"},
            "plain": plain, "batched_vs_plain": (value / plain["value"]) if plain else None,
            "e2e": e2e, "clocks": clk,
            "gpu_launches": args.steps * launches_per_step,
            "enforce_violations": violations, "state_finite": finite,
            "autotune_ms": {str(k): v for k, v in table.items()}}
     if not args.no_cpu:
-        rate, info = cpu_reference_rate(spec.sides, seconds=15.0)
-        rate1, info1 = cpu_reference_rate(spec.sides, seconds=5.0, threads=1, target=2.5e5)
+        rate, info = cpu_baseline(wl if mode != 2 else "mix20k", steps=2)
         out["cpu_baseline"] = dict(info, value=rate, unit="zone-updates/s", cpu_model=cpu_model(),
-                                   nproc=os.cpu_count(),
-                                   one_thread={"value": rate1, "sample": info1["sample"]})
+                                   nproc=os.cpu_count())
+        if mode == 1:
+            rate1, info1 = cpu_baseline("small", steps=1, threads=1)
+            out["cpu_baseline"]["one_thread"] = {"value": rate1, "sample": info1["sample"]}
     print(json.dumps(out, default=_plain))
     if dist is not None:
         dist.destroy_process_group()

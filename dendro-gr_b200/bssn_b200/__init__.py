@@ -176,9 +176,12 @@ class MeshSpec:
         return np.ctypeslib.as_array(self.blocks, shape=(self.nblocks,)).copy()
 
 
-def generate_mesh(mode, dims, p=(0.7, 0.2, 0.08, 0.02), seed=0, xmin=-8.0, L=16.0):
+def generate_mesh(mode, dims, p=(0.7, 0.2, 0.08, 0.02), seed=0, xmin=-8.0, L=16.0, origin=None):
     """mode 0: uniform 13^3 blocks on a dims[0]^3 octant box; mode 1: seeded
-    mix of 13/19/31/55 blocks on a dims super-cell box (8^3 octants each)."""
+    mix of 13/19/31/55 blocks on a dims super-cell box (8^3 octants each).
+    The longest axis spans L; node (0,0,0) sits at xmin on every axis, or at
+    `origin` (per axis) when given -- e.g. to centre a non-cubic box on the
+    coordinate origin, where the Sommerfeld condition measures r from."""
     d = (C.c_int32 * 3)(*dims)
     pp = (C.c_double * 4)(*p)
     n = C.c_int(0)
@@ -188,7 +191,20 @@ def generate_mesh(mode, dims, p=(0.7, 0.2, 0.08, 0.02), seed=0, xmin=-8.0, L=16.
     blocks = (BssnBlockDesc * n.value)()
     check(lib.bssn_mesh_generate(mode, d, pp, seed, xmin, L, blocks, C.byref(n), G, C.byref(h)), "mesh_generate")
     sides = np.array([blocks[b].sz for b in range(n.value)], dtype=np.int32)
+    if origin is not None:
+        reorigin_blocks(blocks, n.value, origin, h.value)
+        return MeshSpec(blocks, n.value, tuple(G), h.value, float(origin[0]), sides, tuple(origin))
     return MeshSpec(blocks, n.value, tuple(G), h.value, xmin, sides)
+
+
+def reorigin_blocks(blocks, nblocks, origin, h):
+    """Block corners for node (0,0,0) at `origin`: ptmin = origin + (g0 - 3) h,
+    ptmax = origin + (g0 - 3 + s - 1) h per axis (the generator's formula)."""
+    for b in range(nblocks):
+        blk = blocks[b]
+        for k in range(3):
+            blk.ptmin[k] = origin[k] + float(blk.g0[k] - 3) * h
+            blk.ptmax[k] = origin[k] + float(blk.g0[k] - 3 + blk.sz - 1) * h
 
 
 class Mesh:
@@ -411,7 +427,7 @@ def constraint_norms(mesh: Mesh, cons, norms, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0)
     """Masked L2 norms sqrt(sum c^2 / N) of the 4 zipped constraint fields
     into the CUDA tensor `norms` (>= ncons doubles)."""
     spec = mesh.spec
-    xm = (C.c_double * 3)(spec.xmin, spec.xmin, spec.xmin)
+    xm = (C.c_double * 3)(*spec.origin3)
     b = (C.c_double * 6)(*bh)
     r = (C.c_double * 2)(*radii)
     check(lib.bssn_constraint_norms_f64(mesh.h, _cons_ptrs(cons), ncons, xm, spec.h, b, r,

@@ -15,7 +15,10 @@ ghostExchangeStart / ghostExchangeRecvSync around its unzip
 order on both sides, so a send matches its receive element by element.
 
 Transport: torch.distributed point-to-point (NCCL between GPUs; with the
-gloo backend the buffers go through host memory).  Packing and unpacking run
+gloo backend the buffers go through host memory).  The global quantities
+are reductions over the ranks, as the reference's MPI reductions: the
+constraint L2 norms from summed squares and counts of owned nodes, the time
+step as a minimum, the remesh decision as a logical OR.  Packing and unpacking run
 on the GPU (bssn_halo_pack_f64 / bssn_halo_unpack_f64), or, for host arrays,
 as numpy gathers (the same lists).
 """
@@ -28,6 +31,9 @@ import numpy as np
 
 from . import (NVARS, BssnBlockDesc, Mesh, MeshSpec, RK4Plan, PLAN_ENFORCE_STAGES, PLAN_GRAPH,
                check, default_params, lib, ptrs, stream_ptr)
+
+lib.bssn_constraint_sums_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_double,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
 
 OCT = 6  # nodes per octant edge
 
@@ -213,6 +219,53 @@ class HaloExchange:
                 fields[:, ix] = buf.reshape(NVARS, -1)
 
 
+# ---------------------------------------------------------------------------
+# Reductions over the ranks (the reference's MPI reductions)
+# ---------------------------------------------------------------------------
+def allreduce_sum(t, group=None):
+    """Sum a float64 tensor over the ranks, in place (NCCL for device
+    tensors, gloo for host tensors)."""
+    import torch.distributed as dist
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t
+
+
+def norms_from_sums(sums):
+    """Constraint L2 norms sqrt(sum c^2 / N) from the 5 reduced sums
+    (bssn_constraint_sums_f64 layout: sums of squares, then the count)."""
+    s = np.asarray(sums, dtype=np.float64)
+    n = s[4]
+    return np.sqrt(s[:4] / n) if n > 0 else np.zeros(4)
+
+
+def dt_min(dt_local, group=None):
+    """The global time step: the minimum of the ranks' CFL time steps (the
+    reference reduces its dt with MPI_MIN, BSSN_GR/src/bssngr_main.cpp)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(dt_local)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MIN, group=group)
+    return float(t.item())
+
+
+def remesh_vote(flag_local, group=None):
+    """Whether any rank asks for a remesh: the reference's
+    MPI_Allreduce(..., MPI_LOR) after isReMeshWAMR
+    (BSSN_GR/src/dataUtils.cpp:833), as a MAX over 0/1."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([1 if flag_local else 0], dtype=torch.int32)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return bool(t.item())
+
+
+def owned_mask(sub: Subdomain):
+    """uint8 per node of the rank's box: 1 where the rank owns the node."""
+    m = np.zeros(sub.n_nodes, dtype=np.uint8)
+    m[sub.owned] = 1
+    return m
+
+
 class PartitionedRK4:
     """One rank's share of a partitioned RK4 evolution on its GPU: the
     rank's box mesh, an RK4 plan on it run stage by stage, and the halo
@@ -240,6 +293,32 @@ class PartitionedRK4:
         for stage in range(4):
             self.ex.run(u if stage == 0 else self.im)
             check(lib.bssn_rk4_plan_stage(self.plan.h, u, dt, stage, stream_ptr()), "plan_stage")
+
+    def constraint_norms(self, U, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0), radii=(0.5, 0.5)):
+        """Hamiltonian / momentum constraint L2 norms of the whole
+        partitioned state (every rank calls it): halo exchange of U, ghost
+        fill and constraints on the rank's box, sums of squares over the
+        nodes this rank owns outside the radii, summed over the ranks."""
+        import torch
+        from . import constraints
+        if not hasattr(self, "_diag"):
+            spec = self.sub.spec
+            self._diag = (torch.zeros((NVARS, self.mesh.n_unzip), dtype=torch.float64, device="cuda"),
+                          torch.zeros((4, spec.n_nodes), dtype=torch.float64, device="cuda"),
+                          torch.from_numpy(owned_mask(self.sub)).cuda(),
+                          torch.zeros(5, dtype=torch.float64, device="cuda"))
+        Pz, cons, mask, sums = self._diag
+        self.ex.run(ptrs(U))
+        self.mesh.unzip(Pz, U)
+        constraints(self.mesh, cons, Pz)
+        spec = self.sub.spec
+        cp = (C.c_void_p * 4)(*[cons[c].data_ptr() for c in range(4)])
+        check(lib.bssn_constraint_sums_f64(self.mesh.h, cp, 4, (C.c_double * 3)(*spec.origin3), spec.h,
+                                           (C.c_double * 6)(*bh), (C.c_double * 2)(*radii),
+                                           C.c_void_p(mask.data_ptr()), C.c_void_p(sums.data_ptr()),
+                                           stream_ptr()), "constraint_sums")
+        allreduce_sum(sums, self.ex.group)
+        return norms_from_sums(sums.cpu().numpy())
 
     def close(self):
         self.plan.close()

@@ -403,6 +403,25 @@ int bssn_constraint_norms_f64(bssn_mesh mesh, const double* const* cons_dev, int
                                  norms_dev, S(stream));
 }
 
+int bssn_constraint_sums_f64(bssn_mesh mesh, const double* const* cons_dev, int ncons,
+                             const double xmin[3], double h, const double bh[6],
+                             const double radii[2], const uint8_t* mask_dev, double* sums_dev,
+                             bssn_stream_t stream) {
+    if (!mesh || !cons_dev || ncons < 1 || ncons > 4 || !xmin || !bh || !radii || !sums_dev)
+        return BSSN_EINVAL;
+    if (mesh->st->lv) return BSSN_ESTATE;
+    for (int c = 0; c < ncons; c++)
+        if (!cons_dev[c]) return BSSN_EINVAL;
+    bssn::MeshState* m = mesh->st;
+    const int npartial = bssn::kNormPartials;
+    if (!m->d_partial) {
+        if (cudaMalloc((void**)&m->d_partial, sizeof(double) * 5 * npartial) != cudaSuccess)
+            return BSSN_ENOMEM;
+    }
+    return bssn::launch_l2_norms(m, cons_dev, ncons, xmin, h, bh, radii, m->d_partial, npartial,
+                                 sums_dev, S(stream), mask_dev, true);
+}
+
 int64_t bssn_mesh_num_elements(bssn_mesh mesh) {
     if (!mesh) return -1;
     int64_t n = 0;

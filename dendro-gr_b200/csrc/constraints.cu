@@ -381,10 +381,12 @@ __global__ void __launch_bounds__(256) constraints_levels_kernel(ConstVars P, Mu
 // Per-CTA partial sums of c^2 and node counts over nodes outside both
 // puncture radii, then one thread sums the partials in CTA order: a fixed
 // grid and a fixed order, so the result is deterministic.
+// mask (optional): only nodes with mask[node] != 0 count (the nodes one rank
+// of a partition owns).
 __global__ void __launch_bounds__(256) l2_partial_kernel(ConstVars C, int nc, int64_t n, int gx, int gy, double x0,
                                   double y0, double z0, double h, double b0, double b1, double b2,
                                   double b3, double b4, double b5, double r1, double r2,
-                                  double* partial) {
+                                  const uint8_t* __restrict__ mask, double* partial) {
     __shared__ double red[256][5];
     double acc[4] = {0, 0, 0, 0};
     double cnt = 0;
@@ -402,6 +404,7 @@ __global__ void __launch_bounds__(256) l2_partial_kernel(ConstVars C, int nc, in
         const double d1 = dist(__dsub_rn(x, b0), __dsub_rn(y, b1), __dsub_rn(z, b2));
         const double d2 = dist(__dsub_rn(x, b3), __dsub_rn(y, b4), __dsub_rn(z, b5));
         if (d1 < r1 || d2 < r2) continue;
+        if (mask && !mask[node]) continue;
         for (int c = 0; c < nc; c++) {
             const double v = C.p[c][node];
             acc[c] += v * v;
@@ -420,11 +423,18 @@ __global__ void __launch_bounds__(256) l2_partial_kernel(ConstVars C, int nc, in
         for (int c = 0; c < 5; c++) partial[blockIdx.x * 5 + c] = red[0][c];
 }
 
-__global__ void l2_final_kernel(const double* partial, int nblocks, int nc, double* norms) {
+// sums: write the raw sums of squares (out[0..nc-1]) and the node count
+// (out[4]) for a reduction over ranks instead of the norms
+__global__ void l2_final_kernel(const double* partial, int nblocks, int nc, double* norms, bool sums) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double s[5] = {0, 0, 0, 0, 0};
     for (int b = 0; b < nblocks; b++)
         for (int c = 0; c < 5; c++) s[c] += partial[b * 5 + c];
+    if (sums) {
+        for (int c = 0; c < nc; c++) norms[c] = s[c];
+        norms[4] = s[4];
+        return;
+    }
     for (int c = 0; c < nc; c++) norms[c] = s[4] > 0 ? sqrt(s[c] / s[4]) : 0.0;
 }
 
@@ -457,15 +467,15 @@ int launch_constraints(const MeshState* m, const double* const* P, double* const
 
 int launch_l2_norms(const MeshState* m, const double* const* C, int nc, const double xmin[3],
                     double h, const double bh[6], const double radii[2], double* partial,
-                    int npartial, double* norms, cudaStream_t s) {
+                    int npartial, double* norms, cudaStream_t s, const uint8_t* mask, bool sums) {
     if (nc < 1 || nc > 4 || npartial < 1) return BSSN_EINVAL;
     ConstVars c = {};
     for (int q = 0; q < nc; q++) c.p[q] = C[q];
     const int64_t n = (int64_t)m->G[0] * m->G[1] * m->G[2];
     l2_partial_kernel<<<npartial, 256, 0, s>>>(c, nc, n, m->G[0], m->G[1], xmin[0], xmin[1],
                                                xmin[2], h, bh[0], bh[1], bh[2], bh[3], bh[4],
-                                               bh[5], radii[0], radii[1], partial);
-    l2_final_kernel<<<1, 32, 0, s>>>(partial, npartial, nc, norms);
+                                               bh[5], radii[0], radii[1], mask, partial);
+    l2_final_kernel<<<1, 32, 0, s>>>(partial, npartial, nc, norms, sums);
     return cuda_status(cudaGetLastError());
 }
 

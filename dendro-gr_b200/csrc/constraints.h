@@ -11,5 +11,6 @@ int launch_constraints(const MeshState* m, const double* const* P, double* const
                        cudaStream_t s, bool psi4 = false);
 int launch_l2_norms(const MeshState* m, const double* const* C, int nc, const double xmin[3],
                     double h, const double bh[6], const double radii[2], double* partial,
-                    int npartial, double* norms, cudaStream_t s);
+                    int npartial, double* norms, cudaStream_t s,
+                    const uint8_t* mask = nullptr, bool sums = false);
 }  // namespace bssn

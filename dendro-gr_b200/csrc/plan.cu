@@ -81,7 +81,7 @@ int plan_create(MeshState* m, const BssnParams& prm, int flags, Plan** out) {
     std::vector<int> keys = p->direct ? std::vector<int>{kAllZOrder} : p->sides;
     for (int key : keys) {
         for (int t = 0; t < tile_count(); t++) {
-            if (p->direct && tile_mode(t) != 1) continue;
+            if (p->direct && !tile_zipped(tile_mode(t))) continue;
             const BrickTask* tk;
             int nt;
             st = mesh_tasks_side(m, t, key, &tk, &nt);
@@ -142,14 +142,14 @@ void plan_destroy(Plan* p) {
 int plan_tile(const Plan* p, int side) {
     auto it = p->mesh->tuned.find(p->direct ? kAllZOrder : side);
     const int t = it == p->mesh->tuned.end() ? -1 : it->second;
-    if (p->direct) return (t >= 0 && tile_mode(t) == 1) ? t : default_split_tile();
+    if (p->direct) return (t >= 0 && tile_zipped(tile_mode(t))) ? t : default_split_tile();
     return t >= 0 ? t : default_split_tile();
 }
 
 int plan_set_tile(Plan* p, int side, int tile) {
     if (tile < 0 || tile >= tile_count()) return BSSN_EINVAL;
     if (p->direct) {
-        if (tile_mode(tile) != 1) return BSSN_EINVAL;
+        if (!tile_zipped(tile_mode(tile))) return BSSN_EINVAL;
         p->mesh->tuned[kAllZOrder] = tile;
     } else if (side == 0) {
         for (int sd : p->sides) p->mesh->tuned[sd] = tile;
@@ -166,7 +166,7 @@ int plan_set_tile(Plan* p, int side, int tile) {
 bool plan_zipped_rhs(const Plan* p) {
     if (p->direct || !p->Rz || (p->flags & BSSN_PLAN_PER_BLOCK) || p->mesh->lv) return false;
     for (int side : p->sides)
-        if (tile_mode(plan_tile(p, side)) != 1) return false;
+        if (!tile_zipped(tile_mode(plan_tile(p, side)))) return false;
     return true;
 }
 
@@ -206,8 +206,27 @@ int plan_rhs(Plan* p, cudaStream_t s, KernelTimer* tm, const double* const* src)
         A.rhs.p[v] = Rp[v];
     }
     if (p->flags & BSSN_PLAN_PER_BLOCK) {
+        // the reference's block loop (rhs.cpp:10-73): blocks in mesh order,
+        // each with its own launch(es) of the kernel the batched plan runs
+        // for its side (split tiles: the block's bricks of the bucket's task
+        // list, derivative + equation launch; the others: one launch)
+        std::map<int, int> seen;  // blocks of each side visited so far
         for (auto& b : m->blocks) {
-            int st = launch_rhs_single(plan_tile(p, b.sz), A, b, s);
+            const int t = plan_tile(p, b.sz);
+            const int j = seen[b.sz]++;
+            int st;
+            if (tile_mode(t) == 1) {
+                const BrickTask* tk;
+                int nt;
+                st = mesh_tasks_side(m, t, b.sz, &tk, &nt);
+                const int per = bricks_per_block(t, b.sz);
+                if (!st && (j + 1) * per > nt) st = BSSN_ESTATE;
+                if (!st)
+                    st = launch_rhs_tasks(t, A, m->d_blocks, tk + (size_t)j * per, per, s, m->d_scratch,
+                                          m->scratch_zones, tm);
+            } else {
+                st = launch_rhs_single(t, A, b, s);
+            }
             if (st) return st;
         }
         return 0;
@@ -437,7 +456,7 @@ int plan_autotune(Plan* p, double* const* u, int reps, cudaStream_t s, float* ti
         int best_t = default_split_tile();
         std::vector<float> tt(nt, 1e30f);
         for (int t = 0; t < nt && !st; t++) {
-            if (tile_mode(t) != 1) continue;
+            if (!tile_zipped(tile_mode(t))) continue;
             const BrickTask* tk;
             int ntask;
             st = mesh_tasks_side(m, t, kAllZOrder, &tk, &ntask);
@@ -564,7 +583,7 @@ int plan_launches_per_step(Plan* p) {
     MeshState* m = p->mesh;
     int rhs = 0;
     if (p->flags & BSSN_PLAN_PER_BLOCK) {
-        rhs = (int)m->blocks.size();
+        for (auto& b : m->blocks) rhs += tile_mode(plan_tile(p, b.sz)) == 1 ? 2 : 1;
     } else if (p->direct) {
         const int t = plan_tile(p, kAllZOrder);
         const BrickTask* tk;

@@ -411,6 +411,82 @@ __device__ __forceinline__ void zone_dirs(const ZoneCtx& z, const double* tile, 
     }
 }
 
+// The interior stencils of zone_dirs (d1_in / d2_in / ko_in along x, y, z)
+// advanced one tap at a time across all nine chains: every chain keeps the
+// reference's left-to-right order of rounded products and sums, but the
+// chains' operations alternate, so each tap step offers nine independent
+// FP64 chains to hide latency with few warps per SM.  Closures as in
+// zone_dirs.
+template <bool SECOND, class Bk>
+__device__ __forceinline__ void zone_dirs_il(const ZoneCtx& z, const double* tile, Dir3 r[3]) {
+    const double* t = tile + z.tc;
+    constexpr int ST[3] = {1, Bk::TX, Bk::TX * Bk::TY};
+    double a1[3], a2[3], ak[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {  // tap -3
+        const double v = t[-3 * ST[d]];
+        a1[d] = -v;
+        a2[d] = SECOND ? __dmul_rn(2.0, v) : 0.0;
+        ak[d] = -v;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {  // tap -2
+        const double v = t[-2 * ST[d]];
+        a1[d] = __dadd_rn(a1[d], __dmul_rn(9.0, v));
+        if (SECOND) a2[d] = __dadd_rn(a2[d], __dmul_rn(-27.0, v));
+        ak[d] = __dadd_rn(ak[d], __dmul_rn(6.0, v));
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {  // tap -1
+        const double v = t[-ST[d]];
+        a1[d] = __dadd_rn(a1[d], __dmul_rn(-45.0, v));
+        if (SECOND) a2[d] = __dadd_rn(a2[d], __dmul_rn(270.0, v));
+        ak[d] = __dadd_rn(ak[d], __dmul_rn(-15.0, v));
+    }
+    {  // tap 0 (not in the first derivative)
+        const double v = t[0];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            if (SECOND) a2[d] = __dadd_rn(a2[d], __dmul_rn(-490.0, v));
+            ak[d] = __dadd_rn(ak[d], __dmul_rn(20.0, v));
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {  // tap 1
+        const double v = t[ST[d]];
+        a1[d] = __dadd_rn(a1[d], __dmul_rn(45.0, v));
+        if (SECOND) a2[d] = __dadd_rn(a2[d], __dmul_rn(270.0, v));
+        ak[d] = __dadd_rn(ak[d], __dmul_rn(-15.0, v));
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {  // tap 2
+        const double v = t[2 * ST[d]];
+        a1[d] = __dadd_rn(a1[d], __dmul_rn(-9.0, v));
+        if (SECOND) a2[d] = __dadd_rn(a2[d], __dmul_rn(-27.0, v));
+        ak[d] = __dadd_rn(ak[d], __dmul_rn(6.0, v));
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {  // tap 3
+        const double v = t[3 * ST[d]];
+        a1[d] = __dadd_rn(a1[d], v);
+        if (SECOND) a2[d] = __dadd_rn(a2[d], __dmul_rn(2.0, v));
+        ak[d] = __dadd_rn(ak[d], -v);
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        r[d].d1 = __dmul_rn(a1[d], z.cf[d].ih60);
+        r[d].d2 = SECOND ? __dmul_rn(a2[d], z.cf[d].ih2_180) : 0.0;
+        r[d].ko = __dmul_rn(z.cf[d].ko_pre, ak[d]);
+    }
+    if (z.bflag) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const bool lo = z.bflag & (1u << (2 * d)), hi = z.bflag & (2u << (2 * d));
+            if (near_face(z.a[d], z.s, lo, hi)) r[d] = closure3(t, z.st[d], z.a[d], z.s, lo, z.cf[d], SECOND);
+        }
+    }
+}
+
 // The halo part of the mixed scratch: d/dx on the 6 halo rows in y (mxj) and
 // d/dx, d/dy on the 6 halo planes in z (mxk, myk); the brick part is written
 // by the zones themselves from their own gradient.  Halo row / plane h in

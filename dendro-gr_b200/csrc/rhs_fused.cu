@@ -120,10 +120,17 @@ TileEntry make_split_tile(int shape, int fused) {
     using Bk = Brick<BX, BY, BZ>;
     return TileEntry{BX, BY, BZ, Bk::THREADS, Bk::SMEM_BYTES, nullptr, 1, shape, fused};
 }
+template <int BX, int BY, int BZ>
+TileEntry make_onchip_tile(int shape) {
+    using Bk = Brick<BX, BY, BZ>;
+    return TileEntry{BX, BY, BZ, Bk::THREADS, 0, nullptr, 2, shape, -1};
+}
 
 // tiles 0..2: fused; 3..5: the same shapes split; 6..9: split-only shapes
 // (13x5x5 and 9x9x5 fit the 25-zone interiors of 31^3 blocks with few idle
-// threads)
+// threads); 10..13: on chip (128-zone bricks, every extent >= 3 for every
+// block side, as the one-sided closures need; 10, 11 at two CTAs per SM,
+// 12, 13 the same shapes at three)
 // (rhs_split.cu's shape order).  `fused` is the tile a single-block launch
 // of the shape runs (the nearest fused shape for split-only ones).
 const TileEntry* tile_table(int* count) {
@@ -138,6 +145,10 @@ const TileEntry* tile_table(int* count) {
         make_split_tile<8, 8, 8>(4, 0),
         make_split_tile<13, 5, 5>(5, 1),
         make_split_tile<9, 9, 5>(6, 1),
+        make_onchip_tile<5, 5, 5>(0),
+        make_onchip_tile<7, 4, 4>(1),
+        make_onchip_tile<5, 5, 5>(2),
+        make_onchip_tile<7, 4, 4>(3),
     };
     *count = (int)(sizeof(table) / sizeof(table[0]));
     return table;
@@ -145,6 +156,7 @@ const TileEntry* tile_table(int* count) {
 
 int prepare(const TileEntry& t) {
     if (t.mode == 1) return prepare_split(t.shape);
+    if (t.mode == 2) return prepare_onchip(t.shape);
     return set_smem_limit((const void*)t.kern, (int)t.smem);
 }
 }  // namespace
@@ -212,6 +224,19 @@ long check_tile_shape() {
     const int B[3] = {BX, BY, BZ};
     const int T[3] = {Bk::TX, Bk::TY, Bk::TZ};
     long bad = 0;
+    // the splitter's brick extents for every block side: at least 3 (a
+    // one-sided closure at a physical face reads up to 5 points inward, which
+    // a thinner brick's tile of brick + 3 halo points does not hold) and at
+    // most the shape
+    for (int side : {13, 19, 31, 55})
+        for (int d = 0; d < 3; d++) {
+            const int n = side - 2 * PW, nb = (n + B[d] - 1) / B[d];
+            for (int q = 0; q < nb; q++) {
+                int o, e;
+                split1(n, B[d], q, o, e);
+                if (e < 3 || e > B[d]) bad++;
+            }
+        }
     for (int e0 = 3; e0 <= BX; e0++)
         for (int e1 = 3; e1 <= BY; e1++)
             for (int e2 = 3; e2 <= BZ; e2++)
@@ -258,6 +283,8 @@ long tile_selfcheck(int tile) {
     const int b[3] = {tab[tile].bx, tab[tile].by, tab[tile].bz};
     auto is = [&](int x, int y, int z) { return b[0] == x && b[1] == y && b[2] == z; };
     if (is(8, 8, 4)) return check_tile_shape<8, 8, 4>();
+    if (is(5, 5, 5)) return check_tile_shape<5, 5, 5>();
+    if (is(7, 4, 4)) return check_tile_shape<7, 4, 4>();
     if (is(7, 7, 4)) return check_tile_shape<7, 7, 4>();
     if (is(8, 4, 4)) return check_tile_shape<8, 4, 4>();
     if (is(7, 7, 7)) return check_tile_shape<7, 7, 7>();
@@ -318,6 +345,8 @@ int launch_rhs_tasks(int tile, const RhsArgs& A, const BssnBlockDesc* blocks_dev
     if (t.mode == 1)
         return launch_rhs_split(t.shape, A, blocks_dev, tasks_dev, ntasks, scratch, scratch_zones,
                                 s, tm, zip_grid, zip_in);
+    if (t.mode == 2)
+        return launch_rhs_onchip(t.shape, A, blocks_dev, tasks_dev, ntasks, s, tm, zip_grid, zip_in);
     if (zip_grid) return BSSN_EINVAL;  // the fused kernel writes padded right-hand sides only
     int st = prepare(t);
     if (!st && tm) st = tm->start(KernelTimer::FUSED, s);
@@ -326,6 +355,15 @@ int launch_rhs_tasks(int tile, const RhsArgs& A, const BssnBlockDesc* blocks_dev
     st = cuda_status(cudaGetLastError());
     if (!st && tm) st = tm->stop(s);
     return st;
+}
+
+int bricks_per_block(int tile, int side) {
+    int c;
+    const TileEntry* tab = tile_table(&c);
+    if (tile < 0 || tile >= c) return 0;
+    const TileEntry& t = tab[tile];
+    const int n = side - 2 * PW;
+    return ((n + t.bx - 1) / t.bx) * ((n + t.by - 1) / t.by) * ((n + t.bz - 1) / t.bz);
 }
 
 int rhs_launch_count(int tile, int ntasks, int64_t scratch_zones) {
@@ -340,6 +378,7 @@ int launch_rhs_single(int tile, const RhsArgs& A, const BssnBlockDesc& blk,
     int c;
     const TileEntry* tab = tile_table(&c);
     if (tile < 0 || tile >= c) return BSSN_EINVAL;
+    if (tab[tile].mode == 2) return launch_rhs_onchip_single(tab[tile].shape, A, blk, s);
     const TileEntry& t = tab[tab[tile].fused];
     int st = prepare(t);
     if (st) return st;

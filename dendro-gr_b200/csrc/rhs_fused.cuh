@@ -23,15 +23,19 @@ struct BrickTask {
     int16_t e[3];
 };
 
-// Tiles: a brick shape run either fused (one kernel) or split (derivative
-// pass + equation pass through a scratch of kSplitSlots doubles per zone).
+// Tiles: a brick shape run fused (one kernel, rhs_kernel), split (derivative
+// pass + equation pass through a scratch of kSplitSlots doubles per zone) or
+// on chip (one kernel, derivatives handed to the equations in registers,
+// rhs_onchip.cu).
 constexpr int kSplitSlots = 11 * 10 + 13 * 4;
 // Largest scratch the mesh allocates for the split path (zones); longer task
 // lists are processed in chunks.
 constexpr int64_t kSplitScratchZonesMax = int64_t(6) << 20;
 
 int tile_count();
-int tile_mode(int tile);   // 0 fused, 1 split, -1 unknown
+int tile_mode(int tile);   // 0 fused, 1 split, 2 on chip, -1 unknown
+// whether a tile's kernels can write zipped right-hand sides (split, on chip)
+inline bool tile_zipped(int mode) { return mode == 1 || mode == 2; }
 int default_split_tile();  // the split tile used before autotuning
 int tile_zones(int tile);  // zones per brick (BX*BY*BZ)
 long tile_selfcheck(int tile);
@@ -89,11 +93,23 @@ int launch_rhs_tasks(int tile, const RhsArgs& A, const BssnBlockDesc* blocks_dev
                      const BrickTask* tasks_dev, int ntasks, cudaStream_t s,
                      double* scratch, int64_t scratch_zones, KernelTimer* tm = nullptr,
                      const int32_t* zip_grid = nullptr, bool zip_in = true);
+// bricks of one block of padded side `side` under a tile (build_tasks keeps
+// a block's bricks together, blocks in mesh order)
+int bricks_per_block(int tile, int side);
 // kernel launches launch_rhs_tasks makes for a task list of ntasks bricks
 int rhs_launch_count(int tile, int ntasks, int64_t scratch_zones);
 // one block; a split tile runs its shape fused
 int launch_rhs_single(int tile, const RhsArgs& A, const BssnBlockDesc& blk,
                       cudaStream_t s);
+
+// on-chip path (rhs_onchip.cu); shape = index among the on-chip shapes
+int onchip_shape_count();
+int onchip_shape(int shape, int b[3]);
+int prepare_onchip(int shape);
+int launch_rhs_onchip(int shape, const RhsArgs& A, const BssnBlockDesc* blocks_dev,
+                      const BrickTask* tasks_dev, int ntasks, cudaStream_t s, KernelTimer* tm,
+                      const int32_t* zip_grid, bool zip_in);
+int launch_rhs_onchip_single(int shape, const RhsArgs& A, const BssnBlockDesc& blk, cudaStream_t s);
 
 // split path (rhs_split.cu); shape = index among the split shapes
 int split_shape_count();

@@ -220,6 +220,18 @@ int bssn_constraint_norms_f64(bssn_mesh mesh, const double* const* cons_dev,
                               int ncons, const double xmin[3], double h,
                               const double bh[6], const double radii[2],
                               double* norms_dev, bssn_stream_t stream);
+/* The pieces of those norms for a reduction over the ranks of a partition
+ * (the reference's par::Mpi_Reduce of the local sums,
+ * BSSN_GR/include/grUtils.tcc:31): sums_dev[c] = sum of cons_c^2 over the
+ * counted nodes (c < ncons), sums_dev[4] = their number; counted are the
+ * nodes outside both radii with mask_dev[node] != 0 (mask_dev NULL: every
+ * node).  Same fixed reduction order as bssn_constraint_norms_f64.  After
+ * summing sums_dev over the ranks, norm_c = sqrt(sum_c / count). */
+int bssn_constraint_sums_f64(bssn_mesh mesh, const double* const* cons_dev,
+                             int ncons, const double xmin[3], double h,
+                             const double bh[6], const double radii[2],
+                             const uint8_t* mask_dev, double* sums_dev,
+                             bssn_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
 /* Remesh decision.  The reference scores each element with dendrolib's

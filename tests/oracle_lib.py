@@ -122,7 +122,8 @@ class OracleMeshSpec:
     library involved): the same attributes MeshOracle reads from the
     library's MeshSpec."""
 
-    def __init__(self, mode, dims, p=(0.7, 0.2, 0.08, 0.02), seed=0, xmin=-8.0, L=16.0, lib=None):
+    def __init__(self, mode, dims, p=(0.7, 0.2, 0.08, 0.02), seed=0, xmin=-8.0, L=16.0, lib=None,
+                 origin=None):
         lib = (lib or oracle()).lib
         d = (C.c_int32 * 3)(*dims)
         pp = (C.c_double * 4)(*p)
@@ -136,9 +137,20 @@ class OracleMeshSpec:
                 blocks = (OrcBlock * n.value)()
             rc = lib.orc_mesh_generate(mode, d, pp, seed, xmin, L, blocks, C.byref(n), G, C.byref(h))
             assert rc == 0, rc
+        if origin is not None:  # node (0,0,0) at origin per axis, the generator's corner formula
+            for b in range(n.value):
+                for k in range(3):
+                    blocks[b].ptmin[k] = origin[k] + float(blocks[b].g0[k] - 3) * h.value
+                    blocks[b].ptmax[k] = origin[k] + float(blocks[b].g0[k] - 3 + blocks[b].sz - 1) * h.value
+            xmin = float(origin[0])
+        self.origin = tuple(origin) if origin is not None else None
         self.blocks, self.nblocks = blocks, n.value
         self.G, self.h, self.xmin = tuple(G), h.value, xmin
         self.sides = np.array([blocks[b].sz for b in range(n.value)], dtype=np.int32)
+
+    @property
+    def origin3(self):
+        return self.origin if self.origin is not None else (self.xmin,) * 3
 
     @property
     def n_nodes(self):
@@ -196,7 +208,8 @@ class MeshOracle:
     def initial_data(self, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0), m1=0.5, m2=0.5, chi_floor=1e-4,
                      eps=1e-8, seed=20261203):
         Z = np.zeros((NVARS, self.spec.n_nodes))
-        xm = (C.c_double * 3)(self.spec.xmin, self.spec.xmin, self.spec.xmin)
+        org = getattr(self.spec, "origin3", (self.spec.xmin,) * 3)
+        xm = (C.c_double * 3)(*org)
         b = (C.c_double * 6)(*bh)
         self.lib.orc_initial_data(rows(Z), self.G, xm, C.c_double(self.spec.h), b, C.c_double(m1),
                                   C.c_double(m2), C.c_double(chi_floor), C.c_double(eps),
@@ -248,21 +261,32 @@ def rel_err(ref, got):
     return np.where(den > 0, num / np.where(den > 0, den, 1), num)
 
 
-def oracle_constraints(spec, Uz, lib=None):
+def oracle_constraints(spec, Uz, lib=None, threads=1):
     """ham, mom0..2 on every zipped node from the padded state Uz, by
     orc_physical_constraints per block (physcon.cpp:12-89 restated) and the
-    oracle's zip."""
+    oracle's zip; blocks spread over `threads` host threads (each block
+    writes only its own interior)."""
     O = lib or oracle()
     Cz = np.zeros((NVARS, spec.n_unzip))
-    ws = np.zeros(288 * 55 ** 3)
-    for b in range(spec.nblocks):
-        blk = spec.blocks[b]
-        s = int(blk.sz)
-        pm = np.array(blk.ptmin[:])
-        px = np.array(blk.ptmax[:])
-        sz = (C.c_uint * 3)(s, s, s)
-        O.lib.orc_physical_constraints(rows(Cz), rows(Uz), C.c_uint(int(blk.offset)), P(pm), P(px), sz,
-                                       C.c_uint(int(blk.bflag)), P(ws))
+    rc, ru = rows(Cz), rows(Uz)
+
+    def run(bs):
+        ws = np.zeros(288 * 55 ** 3)
+        for b in bs:
+            blk = spec.blocks[b]
+            s = int(blk.sz)
+            pm = np.array(blk.ptmin[:])
+            px = np.array(blk.ptmax[:])
+            sz = (C.c_uint * 3)(s, s, s)
+            O.lib.orc_physical_constraints(rc, ru, C.c_uint(int(blk.offset)), P(pm), P(px), sz,
+                                           C.c_uint(int(blk.bflag)), P(ws))
+
+    if threads <= 1:
+        run(range(spec.nblocks))
+    else:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(threads) as ex:
+            list(ex.map(run, [range(t, spec.nblocks, threads) for t in range(threads)]))
     return MeshOracle(spec, O).zip(Cz, nvars=4)[:4]
 
 
@@ -288,10 +312,11 @@ def l2_norms(spec, Cn, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0), radii=(0.5, 0.5)):
     """sqrt(sum c^2 / N) over nodes outside both puncture radii
     (grUtils.tcc:36-134)."""
     G = spec.G
+    o = getattr(spec, "origin3", (spec.xmin,) * 3)
     g = np.arange(spec.n_nodes)
-    x = spec.xmin + (g % G[0]) * spec.h
-    y = spec.xmin + ((g // G[0]) % G[1]) * spec.h
-    z = spec.xmin + (g // (G[0] * G[1])) * spec.h
+    x = o[0] + (g % G[0]) * spec.h
+    y = o[1] + ((g // G[0]) % G[1]) * spec.h
+    z = o[2] + (g // (G[0] * G[1])) * spec.h
     d1 = np.sqrt((x - bh[0]) ** 2 + (y - bh[1]) ** 2 + (z - bh[2]) ** 2)
     d2 = np.sqrt((x - bh[3]) ** 2 + (y - bh[4]) ** 2 + (z - bh[5]) ** 2)
     keep = ~((d1 < radii[0]) | (d2 < radii[1]))

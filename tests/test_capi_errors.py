@@ -105,4 +105,4 @@ def test_tile_queries():
     lib.bssn_tile_selfcheck.restype = C.c_long
     assert lib.bssn_tile_selfcheck(99) == -1
     modes = [lib.bssn_tile_mode(t) for t in range(lib.bssn_tile_count())]
-    assert set(modes) == {0, 1}
+    assert set(modes) == {0, 1, 2}  # fused, split, on chip

@@ -26,7 +26,7 @@ def dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-@pytest.mark.parametrize("side", [13, 19, 31])
+@pytest.mark.parametrize("side", [13, 19, 31, 55])
 def test_stencils_bit_exact(B, O, side):
     rng = np.random.default_rng(side)
     u = rng.standard_normal(side ** 3)
@@ -39,6 +39,37 @@ def test_stencils_bit_exact(B, O, side):
             torch.cuda.synchronize()
             got = D.cpu().numpy()
             assert np.array_equal(ref.view(np.uint64), got.view(np.uint64)), (kind, bflag)
+
+
+@pytest.mark.parametrize("side", [13, 55])
+def test_deriv644adv_bit_exact(B, O, side):
+    """deriv644adv_{x,y,z} (derivs.cpp:3313-3347) against the reference's own
+    compiled functions (oracle/_ref) where that library is present, else the
+    oracle's centred stencil -- the reference wires the advective forms to
+    the centred one, so the shift vector must not change the result."""
+    import ctypes as C
+    rng = np.random.default_rng(100 + side)
+    n = side ** 3
+    u = 1.0 + 1e-8 * rng.standard_normal(n)
+    beta = rng.standard_normal(n)
+    du, dbeta = dev(u), dev(beta)
+    ref_lib = ol.reference()
+    sz = (C.c_uint * 3)(side, side, side)
+    for kind, name in enumerate(("x", "y", "z")):
+        for bflag in (0, 63, 21, 42, 9):
+            if ref_lib is not None:
+                ref = np.zeros(n)
+                getattr(ref_lib.lib, "ref_deriv644adv_" + name)(ol.P(ref), ol.P(u), C.c_double(0.29), sz,
+                                                                ol.P(beta), C.c_uint(bflag))
+            else:
+                ref = O.stencil(kind, u, 0.29, (side, side, side), bflag)
+            D = torch.zeros(n, dtype=torch.float64, device="cuda")
+            rc = B.lib.bssn_deriv644adv_f64(kind, C.c_void_p(D.data_ptr()), C.c_void_p(du.data_ptr()), 0.29, sz,
+                                            C.c_void_p(dbeta.data_ptr()), bflag, B.stream_ptr())
+            assert rc == 0
+            torch.cuda.synchronize()
+            got = D.cpu().numpy()
+            assert np.array_equal(ref.view(np.uint64), got.view(np.uint64)), (name, bflag)
 
 
 def bl_block(side, bflag_seed, h=1.0 / 3.0, shift=(0.0, -1.0, -1.0), noise=1e-6, seed=0):
@@ -204,6 +235,59 @@ def test_rk4_step_vs_oracle(B, O, path, mesh):
         d_ref = Z1[v] - Z0[v]
         d_got = got[v] - Z0[v]
         assert np.abs(d_got - d_ref).max() <= 1e-10 * np.abs(d_ref).max(), v
+
+
+def onchip_tiles(B, variant=0):
+    """side -> on-chip tile: 7x4x4 bricks for 13^3 blocks, 5x5x5 for the rest;
+    variant 0 = the first tile of each shape in the table (two CTAs per SM),
+    1 = the second (three CTAs per SM)."""
+    pick = {}
+    for t, shape in enumerate(B.tiles()):
+        if B.tile_mode(t) == 2:
+            pick.setdefault(shape[:3], []).append(t)
+    return {13: pick[(7, 4, 4)][variant], 19: pick[(5, 5, 5)][variant],
+            31: pick[(5, 5, 5)][variant], 55: pick[(5, 5, 5)][variant]}
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("path", ["graph", "per_block", "direct"])
+@pytest.mark.parametrize("mesh", ["uniform", "mix"])
+def test_rk4_step_onchip_tiles(B, O, path, mesh, variant):
+    """One RK4 step with the on-chip right-hand side (derivatives handed to
+    the equations in registers) on every bucket: graph-replayed plan (zipped
+    right-hand side, 55^3 tiles staged from the zipped state), the plain
+    per-block path (the same kernel, one launch per block) and the direct
+    form, against the oracle's step."""
+    spec = B.generate_mesh(0, (4, 4, 4)) if mesh == "uniform" else B.generate_mesh(1, (2, 1, 1), seed=1, xmin=-8.25)
+    mo = ol.MeshOracle(spec, O)
+    Z0 = mo.initial_data(eps=1e-8)
+    dt = 0.25 * spec.h
+    Z1 = Z0.copy()
+    assert mo.rk4_step(Z1, dt, ol.params()) == 0
+    m = B.Mesh(spec)
+    dZ = dev(Z0)
+    flags = B.PLAN_ENFORCE_STAGES | {"graph": B.PLAN_GRAPH, "per_block": B.PLAN_PER_BLOCK,
+                                     "direct": B.PLAN_DIRECT}[path]
+    plan = B.RK4Plan(m, B.default_params(), flags)
+    if path == "direct":
+        plan.set_tile(onchip_tiles(B, variant)[55])
+    else:
+        for side, t in onchip_tiles(B, variant).items():
+            if side in set(spec.sides.tolist()):
+                plan.set_tile(t, side)
+    plan.step(dZ, dt)
+    torch.cuda.synchronize()
+    assert plan.violations() == 0
+    plan.close()
+    err = ol.rel_err(Z1, dZ.cpu().numpy())
+    # The on-chip right-hand side agrees with the oracle to ~2e-15 per call
+    # (test_mesh_rhs_mixed_sizes).  Its equations contract multiply-adds in
+    # places other than the split path's, and those last-bit differences
+    # (~3e-16 after stage 1) grow through stages 2 and 3 for the variables
+    # that sit at the 1e-8 noise level (Gt, B): 2.9e-13 of their largest
+    # magnitude after the step (split path: 2.4e-14).  The bar is the
+    # per-call 1e-12 of the contract.
+    assert err.max() <= 1e-12, (err.max(), int(err.argmax()))
 
 
 def test_graph_replay_matches_eager(B):

@@ -73,3 +73,33 @@ def test_partitioned_step_matches_single_domain(kind, world, steps):
     assert len(all_ids) == spec.n_nodes and len(np.unique(all_ids)) == spec.n_nodes
     for i, v in zip(ids, vals):
         assert np.array_equal(v, Zref[:, i])
+
+
+@pytest.mark.parametrize("kind,world", [("mix", 2), ("uniform", 3)])
+def test_partitioned_reductions_match_single_domain(kind, world):
+    """The global quantities of a partitioned run after one step: constraint
+    L2 norms from the ranks' owned-node sums reduced over the ranks equal the
+    single-domain norms; every block's exact wavelet flag equals its flag in
+    the single domain; the remesh OR-vote and the time-step minimum are the
+    same on every rank."""
+    spec, Z = reference_step(kind, 1)
+    O = ol.oracle()
+    mo = ol.MeshOracle(spec, O)
+    U = mo.unzip(Z)
+    ref_norms = ol.l2_norms(spec, ol.oracle_constraints(spec, U, O))
+    ref_flags = pr.block_flags(spec, U, O)
+    with tempfile.TemporaryDirectory() as d:
+        run_ranks(pr.cpu_diag_rank, world, kind, 1, d)
+        norms = [np.load(os.path.join(d, f"norms{r}.npy")) for r in range(world)]
+        flags = [np.load(os.path.join(d, f"flags{r}.npy")) for r in range(world)]
+        votes = [np.load(os.path.join(d, f"vote{r}.npy")) for r in range(world)]
+        dts = [np.load(os.path.join(d, f"dt{r}.npy"))[0] for r in range(world)]
+    for n in norms:
+        assert np.allclose(n, ref_norms, rtol=1e-12, atol=0), (n, ref_norms)
+    got = np.full(spec.nblocks, -1)
+    for f in flags:
+        got[f[0]] = f[1]
+    assert np.array_equal(got, ref_flags.astype(np.int64))
+    for v in votes:
+        assert list(v) == [bool(ref_flags.any()), True, False]
+    assert dts == [0.25 * spec.h] * world
