@@ -530,3 +530,33 @@ def remesh_decide(mesh: Mesh, unz, net: RemeshMLP, tol=1e-6, audit_frac=0.05, se
                                      seed, tol, _vp(flags), _vp(stats), _vp(work), wb, stream_ptr(stream)),
           "remesh_decide")
     return flags, stats
+
+
+lib.bssn_remesh_decide2_work_bytes.argtypes = [C.c_void_p]
+lib.bssn_remesh_decide2_work_bytes.restype = C.c_size_t
+lib.bssn_remesh_decide2_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float,
+                                        C.c_float, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
+                                        C.c_double, C.c_uint64, C.c_double, C.c_double, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
+
+
+def remesh_decide2(mesh: Mesh, unz, net_refine: RemeshMLP, net_keep: RemeshMLP, tol=1e-6, keep_fac=0.1,
+                   audit_frac=0.05, seed=7, work=None, stream=None):
+    """Refine and keep flags (exact: block score above tol / above
+    keep_fac * tol) learned in one pass: one feature pass, both networks, one
+    exact-test pass over the blocks either network is unsure of and one
+    audit sample.  Returns (refine uint8[nblocks], keep uint8[nblocks],
+    stats int32[8])."""
+    import torch
+    nb = mesh.spec.nblocks
+    wb = lib.bssn_remesh_decide2_work_bytes(mesh.h)
+    if work is None or work.numel() < wb:
+        work = torch.empty(wb, dtype=torch.uint8, device="cuda")
+    refine = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    keep = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    stats = torch.zeros(8, dtype=torch.int32, device="cuda")
+    check(lib.bssn_remesh_decide2_f64(mesh.h, ptrs(unz), _vp(net_refine.wq), _vp(net_refine.norm), net_refine.lo,
+                                      net_refine.hi, _vp(net_keep.wq), _vp(net_keep.norm), net_keep.lo,
+                                      net_keep.hi, audit_frac, seed, tol, keep_fac, _vp(refine), _vp(keep),
+                                      _vp(stats), _vp(work), wb, stream_ptr(stream)), "remesh_decide2")
+    return refine, keep, stats

@@ -21,12 +21,15 @@ test and refines again at the one after.
 
 The learned run uses two networks of the same shape, one per threshold,
 trained on the labels the exact test gave during the exact run (features of
-every block at every remesh test), with the decision thresholds set on a
-held-out tenth of those samples; each decision defers its uncertain blocks
-and a seeded audit sample to the exact test at its own threshold.  In the
-learned run the exact test is also evaluated at every remesh test, outside
-the timed decision, to count the refine and keep flags the decision
-missed.
+every block at every remesh test).  Their decision thresholds are set on the
+samples of the exact run's last fifth of remesh tests, which the networks
+never saw in training (snapshots later in the evolution, on the meshes of
+that time), and lowered by a margin in logit units.  One decision pass
+serves both flags (bssn_remesh_decide2_f64): the features once, both
+networks, and one exact-test pass on the blocks either network is unsure of
+plus a seeded audit sample.  In the learned run the exact test is also
+evaluated at every remesh test, outside the timed decision, to count the
+refine and keep flags the decision missed.
 
     python -m bssn_b200.evolve --steps 1000 --remesh-every 10 --out run.json
 """
@@ -39,7 +42,7 @@ import time
 import numpy as np
 
 from . import (Mesh, NVARS, PLAN_ENFORCE_STAGES, PLAN_GRAPH, RemeshMLP, RK4Plan, block_features,
-               constraints, default_params, remesh_decide, wavelet_scores)
+               constraints, default_params, remesh_decide2, wavelet_scores)
 from . import levels as LV
 from .remesh_train import pick_thresholds, train
 
@@ -128,7 +131,8 @@ def run(indicator, a, nets=None, collect=False, log=print):
     refine and keep labels when collect)."""
     import torch
     params = default_params()
-    spec = LV.generate_levels((a.M0,) * 3, nested_boxes(a.M0, a.levels), xmin=-a.half, L=2 * a.half)
+    spec = LV.generate_levels((a.M0,) * 3, nested_boxes(a.M0, a.levels), xmin=-a.half, L=2 * a.half,
+                              max_w=a.max_block_octants)
     mesh = Mesh(spec)
     U = torch.zeros((NVARS, spec.n_nodes), dtype=torch.float64, device="cuda")
     LV.initial_data_levels(U, spec, mesh=mesh, bh=BH)
@@ -137,9 +141,8 @@ def run(indicator, a, nets=None, collect=False, log=print):
     rec = dict(indicator=indicator, evolve_ms=0.0, decide_ms=0.0, regrid_s=0.0, zone_updates=0.0,
                tests=0, remeshes=0, history=[], blocks=[spec.nblocks], levels=[spec.nlevels],
                missed=0, exact_refinements=0, keep_missed=0, exact_keeps=0,
-               decide_stats=[0, 0, 0, 0], keep_stats=[0, 0, 0, 0])
+               decide_stats=[0] * 8)
     X, Y, K = [], [], []
-    ktol = a.amr_fac * a.tol
     t, step = 0.0, 0
     torch.cuda.synchronize()
     wall0 = time.perf_counter()
@@ -163,9 +166,8 @@ def run(indicator, a, nets=None, collect=False, log=print):
                 _, ratio, flags = wavelet_scores(st.mesh, st.P, tol=a.tol)
                 keep = (ratio > a.amr_fac).to(torch.uint8)
             else:
-                flags, stats = remesh_decide(st.mesh, st.P, nets[0], tol=a.tol, audit_frac=a.audit, seed=step)
-                keep, kstats = remesh_decide(st.mesh, st.P, nets[1], tol=ktol, audit_frac=a.audit,
-                                             seed=step + 1)
+                flags, keep, stats = remesh_decide2(st.mesh, st.P, nets[0], nets[1], tol=a.tol,
+                                                    keep_fac=a.amr_fac, audit_frac=a.audit, seed=step)
             e1.record()
             e1.synchronize()
             rec["decide_ms"] += e0.elapsed_time(e1)
@@ -178,7 +180,6 @@ def run(indicator, a, nets=None, collect=False, log=print):
                 rec["keep_missed"] += int(((keep == 0) & ekeep).sum())
                 rec["exact_keeps"] += int(ekeep.sum())
                 rec["decide_stats"] = [x + y for x, y in zip(rec["decide_stats"], stats.cpu().tolist())]
-                rec["keep_stats"] = [x + y for x, y in zip(rec["keep_stats"], kstats.cpu().tolist())]
             else:
                 rec["exact_refinements"] += int(flags.sum())
                 rec["exact_keeps"] += int(keep.sum())
@@ -250,6 +251,9 @@ def main(argv=None):
     ap.add_argument("--max-levels", type=int, default=7)
     ap.add_argument("--half", type=float, default=400.0, help="domain [-half, half]^3")
     ap.add_argument("--max-box", type=int, default=None, help="octants per axis and level (default M0)")
+    ap.add_argument("--max-block-octants", type=int, default=8, choices=(1, 2, 4, 8),
+                    help="largest block in octants per axis (1: every block 13^3; M0 20 with 7 levels "
+                         "then gives 50,000 blocks)")
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--remesh-every", type=int, default=10)
     ap.add_argument("--diag-every", type=int, default=10)
@@ -258,6 +262,8 @@ def main(argv=None):
     ap.add_argument("--amr-fac", type=float, default=0.1, help="keep threshold / tol (BSSN_DENDRO_AMR_FAC)")
     ap.add_argument("--audit", type=float, default=0.05)
     ap.add_argument("--train-steps", type=int, default=2000)
+    ap.add_argument("--margin", type=float, default=1.0,
+                    help="lower threshold margin in logit units (remesh_train.pick_thresholds)")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     a.max_box = a.max_box or a.M0
@@ -265,20 +271,22 @@ def main(argv=None):
     ex, X, Y, K = run("exact", a, collect=True)
     print(json.dumps({k: v for k, v in ex.items() if k != "history"}), flush=True)
     t0 = time.perf_counter()
-    perm = np.random.default_rng(0).permutation(len(X))
-    nva = max(len(X) // 10, 1)
-    va, tr = perm[:nva], perm[nva:]
+    # samples in test order: train on the first four fifths of the tests,
+    # thresholds on the last fifth (later snapshots, unseen in training)
+    nva = max(len(X) // 5, 1)
+    tr, va = np.arange(len(X) - nva), np.arange(len(X) - nva, len(X))
     nets = []
     for seed, lab in ((0, Y), (1, K)):
         net = RemeshMLP(seed=seed)
         train(net, X[tr], lab[tr], steps=a.train_steps, log=lambda s: None)
         pv = torch.sigmoid(net.logits(torch.tensor(X[va], device="cuda"))).cpu().numpy()
-        net.lo, net.hi = pick_thresholds(pv, lab[va])
+        net.lo, net.hi = pick_thresholds(pv, lab[va], margin=a.margin)
         nets.append(net)
     train_s = time.perf_counter() - t0
     le = run("learned", a, nets=nets)
     res = {"config": {k: getattr(a, k) for k in ("M0", "levels", "max_levels", "half", "max_box", "steps", "remesh_every",
-                                                 "diag_every", "cfl", "tol", "amr_fac", "audit", "train_steps")},
+                                                 "diag_every", "cfl", "tol", "amr_fac", "audit", "train_steps",
+                                                 "margin", "max_block_octants")},
            "training": {"samples": int(len(tr)), "validation": int(nva), "refine_labels": int(Y.sum()),
                         "keep_labels": int(K.sum()), "thresholds": [[n.lo, n.hi] for n in nets],
                         "seconds": train_s},

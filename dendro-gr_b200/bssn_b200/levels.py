@@ -40,6 +40,9 @@ lib.bssn_levels_maps.argtypes = [C.POINTER(BssnBlockDesc), C.c_int, C.c_int, C.P
 lib.bssn_mesh_generate_patches.argtypes = [C.c_int, C.POINTER(C.c_int32), C.POINTER(BssnPatch), C.c_double,
                                            C.c_double, C.POINTER(BssnBlockDesc), C.POINTER(C.c_int),
                                            C.POINTER(C.c_int64)]
+lib.bssn_mesh_generate_patches_w.argtypes = [C.c_int, C.POINTER(C.c_int32), C.POINTER(BssnPatch), C.c_double,
+                                             C.c_double, C.c_int, C.POINTER(BssnBlockDesc), C.POINTER(C.c_int),
+                                             C.POINTER(C.c_int64)]
 lib.bssn_mesh_create_patches.argtypes = [C.POINTER(BssnBlockDesc), C.c_int, C.c_int, C.POINTER(C.c_int32),
                                          C.POINTER(BssnPatch), C.POINTER(C.c_void_p)]
 lib.bssn_patches_maps.argtypes = [C.POINTER(BssnBlockDesc), C.c_int, C.c_int, C.POINTER(C.c_int32),
@@ -56,6 +59,8 @@ class LevelMeshSpec(MeshSpec):
     # [(level, parent, lo, n)] per patch when a level holds several patches
     # (None: one patch per level, the boxes above)
     patches: list = None
+    # largest block, in octants per axis (8: sides up to 55)
+    max_w: int = 8
 
     @property
     def patch_list(self):
@@ -95,45 +100,48 @@ class LevelMeshSpec(MeshSpec):
         return out
 
 
-def generate_levels(M0, boxes, xmin=-8.0, L=16.0):
+def generate_levels(M0, boxes, xmin=-8.0, L=16.0, max_w=8):
     """Level 0 = the domain [xmin, xmin + L]^3 in M0 octants per axis; boxes
-    = [(lo, n)] of levels 1.. in their own octants."""
+    = [(lo, n)] of levels 1.. in their own octants; blocks of at most max_w
+    octants per axis."""
     allb = [((0, 0, 0), tuple(M0))] + [(tuple(lo), tuple(n)) for lo, n in boxes]
     h0 = L / (OCT * M0[0])
     spec = LevelMeshSpec(None, 0, (0, 1, 1), h0 / 2 ** (len(allb) - 1), xmin, None, None,
-                         tuple(M0), allb, h0)
-    cb = spec.c_boxes()
+                         tuple(M0), allb, h0, None, int(max_w))
+    cp = spec.c_patches()
     M = (C.c_int32 * 3)(*M0)
     n = C.c_int(0)
     nn = C.c_int64(0)
-    check(lib.bssn_mesh_generate_levels(len(allb), M, cb, xmin, h0, None, C.byref(n), C.byref(nn)),
+    check(lib.bssn_mesh_generate_patches_w(len(allb), M, cp, xmin, h0, int(max_w), None, C.byref(n), C.byref(nn)),
           "mesh_generate_levels")
     blocks = (BssnBlockDesc * n.value)()
-    check(lib.bssn_mesh_generate_levels(len(allb), M, cb, xmin, h0, blocks, C.byref(n), C.byref(nn)),
-          "mesh_generate_levels")
+    check(lib.bssn_mesh_generate_patches_w(len(allb), M, cp, xmin, h0, int(max_w), blocks, C.byref(n),
+                                           C.byref(nn)), "mesh_generate_levels")
     spec.blocks, spec.nblocks = blocks, n.value
     spec.G = (int(nn.value), 1, 1)
     spec.sides = np.array([blocks[b].sz for b in range(n.value)], dtype=np.int32)
     return spec
 
 
-def generate_patches(M0, patches, xmin=-8.0, L=16.0):
+def generate_patches(M0, patches, xmin=-8.0, L=16.0, max_w=8):
     """Patch 0 = the domain [xmin, xmin + L]^3 in M0 octants per axis;
     patches = [(level, parent, lo, n)] of patches 1.. (parents listed first,
-    boxes in their own level's octants)."""
+    boxes in their own level's octants); blocks of at most max_w octants per
+    axis."""
     allp = [(0, -1, (0, 0, 0), tuple(M0))] + [(int(a), int(b), tuple(lo), tuple(n)) for a, b, lo, n in patches]
     h0 = L / (OCT * M0[0])
     nlev = 1 + max(p[0] for p in allp)
-    spec = LevelMeshSpec(None, 0, (0, 1, 1), h0 / 2 ** (nlev - 1), xmin, None, None, tuple(M0), [], h0, allp)
+    spec = LevelMeshSpec(None, 0, (0, 1, 1), h0 / 2 ** (nlev - 1), xmin, None, None, tuple(M0), [], h0, allp,
+                         int(max_w))
     cp = spec.c_patches()
     M = (C.c_int32 * 3)(*M0)
     n = C.c_int(0)
     nn = C.c_int64(0)
-    check(lib.bssn_mesh_generate_patches(len(allp), M, cp, xmin, h0, None, C.byref(n), C.byref(nn)),
+    check(lib.bssn_mesh_generate_patches_w(len(allp), M, cp, xmin, h0, int(max_w), None, C.byref(n), C.byref(nn)),
           "mesh_generate_patches")
     blocks = (BssnBlockDesc * n.value)()
-    check(lib.bssn_mesh_generate_patches(len(allp), M, cp, xmin, h0, blocks, C.byref(n), C.byref(nn)),
-          "mesh_generate_patches")
+    check(lib.bssn_mesh_generate_patches_w(len(allp), M, cp, xmin, h0, int(max_w), blocks, C.byref(n),
+                                           C.byref(nn)), "mesh_generate_patches")
     spec.blocks, spec.nblocks = blocks, n.value
     spec.G = (int(nn.value), 1, 1)
     spec.sides = np.array([blocks[b].sz for b in range(n.value)], dtype=np.int32)
@@ -280,9 +288,10 @@ def remesh(mesh, U, flags, max_levels=None, patches=False, stream=None, keep=Non
     from . import Mesh
     L = spec.h0 * OCT * spec.M0[0]
     if patches:
-        new = generate_patches(spec.M0, regrid_patches(spec, f, max_levels), xmin=spec.xmin, L=L)
+        new = generate_patches(spec.M0, regrid_patches(spec, f, max_levels), xmin=spec.xmin, L=L, max_w=spec.max_w)
     else:
-        new = generate_levels(spec.M0, regrid_boxes(spec, f, max_levels, keep=keep, max_n=max_n), xmin=spec.xmin, L=L)
+        new = generate_levels(spec.M0, regrid_boxes(spec, f, max_levels, keep=keep, max_n=max_n), xmin=spec.xmin, L=L,
+                              max_w=spec.max_w)
     nmesh = Mesh(new)
     V = torch.empty((NVARS, new.n_nodes), dtype=torch.float64, device=U.device)
     transfer(mesh, U, nmesh, V, stream)

@@ -80,13 +80,19 @@ def train(net: RemeshMLP, X, Y, steps=3000, batch=16384, lr=3e-3, seed=0, log=pr
     return net
 
 
-def pick_thresholds(p, y, fn_target=1e-3, fp_target=1e-3):
+def pick_thresholds(p, y, fn_target=1e-3, fp_target=1e-3, margin=1.0):
     """lo: the largest threshold with (positives at p <= lo) / positives <=
-    fn_target / 2 (half the budget, for margin); hi: the smallest with
-    (negatives at p >= hi) / negatives <= fp_target."""
+    fn_target / 2 (half the budget, for margin), then lowered by `margin` in
+    logit units (margin > 0 keeps room for snapshots unlike the validation
+    ones: each unit widens the deferred band toward p = 0 by a factor of
+    about e); hi: the smallest with (negatives at p >= hi) / negatives <=
+    fp_target."""
     pos = p[y > 0.5]
     neg = p[y < 0.5]
     lo = float(np.quantile(pos, fn_target / 2, method="lower")) if len(pos) else 0.5
+    if margin > 0 and 0.0 < lo < 1.0:
+        z = np.log(lo / (1.0 - lo)) - margin
+        lo = float(1.0 / (1.0 + np.exp(-z)))
     lo = np.nextafter(np.float32(lo), np.float32(0)).item()
     hi = float(np.quantile(neg, 1 - fp_target, method="higher")) if len(neg) else 0.5
     hi = np.nextafter(np.float32(hi), np.float32(1)).item()

@@ -518,6 +518,60 @@ int bssn_remesh_decide_f64(bssn_mesh mesh, const double* const* unzip_dev, const
     return st;
 }
 
+size_t bssn_remesh_decide2_work_bytes(bssn_mesh mesh) {
+    if (!mesh) return 0;
+    const size_t nb = mesh->st->blocks.size();
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    return bssn_remesh_decide_work_bytes(mesh) + al(nb * sizeof(float)) + al(nb * sizeof(double));
+}
+
+int bssn_remesh_decide2_f64(bssn_mesh mesh, const double* const* unzip_dev, const void* wq_refine,
+                            const float* norm_refine, float lo_r, float hi_r, const void* wq_keep,
+                            const float* norm_keep, float lo_k, float hi_k, double audit_frac,
+                            uint64_t seed, double tol, double keep_fac, uint8_t* refine_dev,
+                            uint8_t* keep_dev, int* stats_dev, void* work_dev, size_t work_bytes,
+                            bssn_stream_t stream) {
+    if (!mesh || !unzip_dev || !wq_refine || !wq_keep || !refine_dev || !keep_dev || !stats_dev ||
+        !work_dev)
+        return BSSN_EINVAL;
+    if (!(lo_r <= hi_r) || !(lo_k <= hi_k) || audit_frac < 0 || audit_frac > 1 || !(tol > 0) ||
+        !(keep_fac > 0) || keep_fac > 1)
+        return BSSN_EINVAL;
+    if (work_bytes < bssn_remesh_decide2_work_bytes(mesh)) return BSSN_EINVAL;
+    bssn::MeshState* m = mesh->st;
+    const int nb = (int)m->blocks.size();
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    char* w = (char*)work_dev;
+    float* feats = (float*)w;
+    w += al((size_t)nb * 16 * sizeof(float));
+    float* lr = (float*)w;
+    w += al((size_t)nb * sizeof(float));
+    float* lk = (float*)w;
+    w += al((size_t)nb * sizeof(float));
+    uint8_t* need = (uint8_t*)w;
+    w += al(nb);
+    uint8_t* decided = (uint8_t*)w;
+    w += al(nb);
+    w += al(nb);  // (the one-flag decision's exact flags)
+    double* ratio = (double*)w;
+    w += al((size_t)nb * sizeof(double));
+    double* scores = (double*)w;
+    cudaStream_t s = S(stream);
+    int st = cudaMemsetAsync(stats_dev, 0, 8 * sizeof(int), s) == cudaSuccess ? 0 : BSSN_EINVAL;
+    if (!st) st = bssn::launch_features(m, unzip_dev, feats, s);
+    if (!st) st = bssn::launch_mlp_fwd(wq_refine, norm_refine, feats, nb, lr, s);
+    if (!st) st = bssn::launch_mlp_fwd(wq_keep, norm_keep, feats, nb, lk, s);
+    if (!st)
+        st = bssn::launch_remesh_select2(lr, lk, nb, lo_r, hi_r, lo_k, hi_k, audit_frac, seed, need,
+                                         decided, stats_dev, s);
+    if (!st) st = bssn::launch_wavelet_scores(m, unzip_dev, bssn::NVARS, scores, need, s);
+    if (!st) st = bssn::launch_block_flags(m, scores, bssn::NVARS, tol, ratio, nullptr, need, s);
+    if (!st)
+        st = bssn::launch_remesh_merge2(nb, need, decided, ratio, keep_fac, lr, lk, lo_r, lo_k,
+                                        stats_dev, refine_dev, keep_dev, s);
+    return st;
+}
+
 int bssn_mesh_partition(const BssnBlockDesc* blocks, int nblocks, int nparts, int32_t* part) {
     return bssn::mesh_partition(blocks, nblocks, nparts, part);
 }

@@ -162,8 +162,9 @@ std::vector<PatchDef> patches_from(int npatches, const BssnPatch* patches) {
 }
 
 int levels_generate(const std::vector<PatchDef>& P, const int32_t M0[3], double xmin, double h0,
-                    BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes) {
+                    BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes, int max_w) {
     if (!nblocks || !n_nodes || !(h0 > 0.0)) return BSSN_EINVAL;
+    if (max_w != 1 && max_w != 2 && max_w != 4 && max_w != 8) return BSSN_EINVAL;
     int st = check_patches(P, M0);
     if (st) return st;
     int64_t nodes = 0;
@@ -180,11 +181,13 @@ int levels_generate(const std::vector<PatchDef>& P, const int32_t M0[3], double 
             t.box.n[d] = P[p].n[d];
         }
         t.kids = children_of(P, p);
-        for (int32_t z = t.box.lo[2]; z < t.box.lo[2] + t.box.n[2]; z += 8)
-            for (int32_t y = t.box.lo[1]; y < t.box.lo[1] + t.box.n[1]; y += 8)
-                for (int32_t x = t.box.lo[0]; x < t.box.lo[0] + t.box.n[0]; x += 8) {
+        // cells of max_w octants per axis (blocks of side 6 max_w + 7), split
+        // where a box or a child box cuts them
+        for (int32_t z = t.box.lo[2]; z < t.box.lo[2] + t.box.n[2]; z += max_w)
+            for (int32_t y = t.box.lo[1]; y < t.box.lo[1] + t.box.n[1]; y += max_w)
+                for (int32_t x = t.box.lo[0]; x < t.box.lo[0] + t.box.n[0]; x += max_w) {
                     const int32_t o[3] = {x, y, z};
-                    t.tile(o, 8);
+                    t.tile(o, max_w);
                 }
         const double h = std::ldexp(h0, -l);
         for (auto& c : t.cells) {
@@ -958,12 +961,21 @@ extern "C" {
 
 int bssn_mesh_generate_levels(int nlevels, const int32_t M0[3], const BssnLevelBox* boxes, double xmin,
                               double h0, BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes) {
-    return bssn::levels_generate(bssn::chain_patches(nlevels, boxes), M0, xmin, h0, blocks, nblocks, n_nodes);
+    return bssn::levels_generate(bssn::chain_patches(nlevels, boxes), M0, xmin, h0, blocks, nblocks, n_nodes,
+                                 8);
 }
 
 int bssn_mesh_generate_patches(int npatches, const int32_t M0[3], const BssnPatch* patches, double xmin,
                                double h0, BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes) {
-    return bssn::levels_generate(bssn::patches_from(npatches, patches), M0, xmin, h0, blocks, nblocks, n_nodes);
+    return bssn::levels_generate(bssn::patches_from(npatches, patches), M0, xmin, h0, blocks, nblocks, n_nodes,
+                                 8);
+}
+
+int bssn_mesh_generate_patches_w(int npatches, const int32_t M0[3], const BssnPatch* patches, double xmin,
+                                 double h0, int max_w, BssnBlockDesc* blocks, int* nblocks,
+                                 int64_t* n_nodes) {
+    return bssn::levels_generate(bssn::patches_from(npatches, patches), M0, xmin, h0, blocks, nblocks, n_nodes,
+                                 max_w);
 }
 
 int bssn_levels_maps(const BssnBlockDesc* blocks, int nblocks, int nlevels, const int32_t M0[3],

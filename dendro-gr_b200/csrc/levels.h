@@ -97,7 +97,8 @@ struct LevelsDev {
 // ptmin / ptmax, physical-boundary flags on level 0).  blocks == NULL: count
 // only.  n_nodes: total zipped nodes over all levels.
 int levels_generate(const std::vector<PatchDef>& P, const int32_t M0[3], double xmin, double h0,
-                    BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes);
+                    BssnBlockDesc* blocks, int* nblocks, int64_t* n_nodes,
+                    int max_w = 8);
 // The maps of a generated mesh (host only).
 int levels_build(const BssnBlockDesc* blocks, int nblocks, const std::vector<PatchDef>& P,
                  const int32_t M0[3], LevelMaps* out);

@@ -402,7 +402,73 @@ __global__ void __launch_bounds__(256) remesh_merge_kernel(int nblk, const uint8
     }
 }
 
+// Two-flag decision (refine at tol, keep at keep_fac * tol) in one pass:
+// the exact test runs once on the union of both networks' uncertain blocks
+// and one seeded audit sample.  stats (8 ints): uncertain for refine,
+// uncertain for keep, extra audited blocks, audited refine misses, audited
+// exact refines, audited keep misses, audited exact keeps, 0.
+__global__ void __launch_bounds__(256) remesh_select2_kernel(const float* __restrict__ lr,
+                                                             const float* __restrict__ lk, int nblk,
+                                                             float lo_r, float hi_r, float lo_k,
+                                                             float hi_k, double audit_frac,
+                                                             uint64_t seed, uint8_t* need,
+                                                             uint8_t* decided, int* stats) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblk) return;
+    const float pr = 1.0f / (1.0f + expf(-lr[b])), pk = 1.0f / (1.0f + expf(-lk[b]));
+    const bool ur = pr > lo_r && pr < hi_r, uk = pk > lo_k && pk < hi_k;
+    const double u = (double)(hmix(seed + 0x9E3779B97F4A7C15ULL * (uint64_t)(b + 1)) >> 11) *
+                     (1.0 / 9007199254740992.0);
+    const bool audit = u < audit_frac;
+    need[b] = (ur || uk || audit) ? 1 : 0;
+    decided[b] = (pr >= hi_r ? 1 : 0) | (pk >= hi_k ? 2 : 0);
+    if (ur) atomicAdd(&stats[0], 1);
+    if (uk) atomicAdd(&stats[1], 1);
+    if (audit && !ur && !uk) atomicAdd(&stats[2], 1);
+}
+
+// Final flags: from the exact ratio (block max score / tol) where the exact
+// test ran, the networks' decisions elsewhere.
+__global__ void __launch_bounds__(256) remesh_merge2_kernel(int nblk, const uint8_t* need,
+                                                            const uint8_t* decided,
+                                                            const double* ratio, double keep_fac,
+                                                            const float* lr, const float* lk,
+                                                            float lo_r, float lo_k, int* stats,
+                                                            uint8_t* flags_r, uint8_t* flags_k) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblk) return;
+    if (need[b]) {
+        const uint8_t er = ratio[b] > 1.0 ? 1 : 0, ek = ratio[b] > keep_fac ? 1 : 0;
+        flags_r[b] = er;
+        flags_k[b] = ek;
+        const float pr = 1.0f / (1.0f + expf(-lr[b])), pk = 1.0f / (1.0f + expf(-lk[b]));
+        if (pr <= lo_r && er) atomicAdd(&stats[3], 1);
+        if (er) atomicAdd(&stats[4], 1);
+        if (pk <= lo_k && ek) atomicAdd(&stats[5], 1);
+        if (ek) atomicAdd(&stats[6], 1);
+    } else {
+        flags_r[b] = decided[b] & 1;
+        flags_k[b] = (decided[b] >> 1) & 1;
+    }
+}
+
 }  // namespace
+
+int launch_remesh_select2(const float* lr, const float* lk, int nblk, float lo_r, float hi_r,
+                          float lo_k, float hi_k, double audit_frac, uint64_t seed, uint8_t* need,
+                          uint8_t* decided, int* stats, cudaStream_t s) {
+    remesh_select2_kernel<<<(nblk + 255) / 256, 256, 0, s>>>(lr, lk, nblk, lo_r, hi_r, lo_k, hi_k,
+                                                             audit_frac, seed, need, decided, stats);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_remesh_merge2(int nblk, const uint8_t* need, const uint8_t* decided, const double* ratio,
+                         double keep_fac, const float* lr, const float* lk, float lo_r, float lo_k,
+                         int* stats, uint8_t* flags_r, uint8_t* flags_k, cudaStream_t s) {
+    remesh_merge2_kernel<<<(nblk + 255) / 256, 256, 0, s>>>(nblk, need, decided, ratio, keep_fac, lr,
+                                                            lk, lo_r, lo_k, stats, flags_r, flags_k);
+    return cuda_status(cudaGetLastError());
+}
 
 int remesh_elements(MeshState* m) {
     if (m->d_elems) return 0;

@@ -38,4 +38,11 @@ int launch_remesh_merge(int nblk, const uint8_t* need, const uint8_t* decided,
                         const uint8_t* exact, const float* logits, float lo, int* stats,
                         uint8_t* flags, cudaStream_t s);
 
+int launch_remesh_select2(const float* lr, const float* lk, int nblk, float lo_r, float hi_r,
+                          float lo_k, float hi_k, double audit_frac, uint64_t seed, uint8_t* need,
+                          uint8_t* decided, int* stats, cudaStream_t s);
+int launch_remesh_merge2(int nblk, const uint8_t* need, const uint8_t* decided, const double* ratio,
+                         double keep_fac, const float* lr, const float* lk, float lo_r, float lo_k,
+                         int* stats, uint8_t* flags_r, uint8_t* flags_k, cudaStream_t s);
+
 }  // namespace bssn

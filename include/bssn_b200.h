@@ -314,6 +314,27 @@ int bssn_remesh_decide_f64(bssn_mesh mesh, const double* const* unzip_dev,
                            void* work_dev, size_t work_bytes,
                            bssn_stream_t stream);
 
+/* Both flags of isReMeshWAMR (BSSN_GR/src/dataUtils.cpp:413-480) learned in
+ * one pass: refine (exact: block score > tol) from the network wq_refine
+ * with thresholds lo_r / hi_r, keep (exact: score > keep_fac * tol,
+ * BSSN_DENDRO_AMR_FAC) from wq_keep with lo_k / hi_k.  The features are
+ * computed once; the exact wavelet test runs once, on the blocks either
+ * network is unsure of plus one seeded audit sample (fraction audit_frac),
+ * and gives both flags there.  stats_dev (8 ints): blocks uncertain for
+ * refine, uncertain for keep, extra audited blocks, audited refine misses of
+ * the network (p_r <= lo_r, exact refines), audited exact refines, audited
+ * keep misses, audited exact keeps, 0.  work_dev:
+ * bssn_remesh_decide2_work_bytes(mesh) bytes. */
+size_t bssn_remesh_decide2_work_bytes(bssn_mesh mesh);
+int bssn_remesh_decide2_f64(bssn_mesh mesh, const double* const* unzip_dev,
+                            const void* wq_refine, const float* norm_refine,
+                            float lo_r, float hi_r, const void* wq_keep,
+                            const float* norm_keep, float lo_k, float hi_k,
+                            double audit_frac, uint64_t seed, double tol,
+                            double keep_fac, uint8_t* refine_dev,
+                            uint8_t* keep_dev, int* stats_dev, void* work_dev,
+                            size_t work_bytes, bssn_stream_t stream);
+
 /* ---------------------------------------------------------------------- */
 /* One whole RK4 step as a plan over a mesh (the reference's per-step
  * sequence rkBSSN.cpp:764-860: per stage unzip -> bssnRHS -> zip -> stage
@@ -528,6 +549,13 @@ int bssn_patches_maps(const BssnBlockDesc* blocks, int nblocks, int npatches, co
 int bssn_mesh_generate_levels(int nlevels, const int32_t M0[3], const BssnLevelBox* boxes,
                               double xmin, double h0, BssnBlockDesc* blocks, int* nblocks,
                               int64_t* n_nodes);
+/* The same tiling with blocks of at most max_w octants per axis (1, 2, 4 or
+ * 8: padded sides up to 13, 19, 31 or 55), the patches given as in
+ * bssn_mesh_generate_patches (a chain of one box per level is the patch list
+ * level l, parent l - 1). */
+int bssn_mesh_generate_patches_w(int npatches, const int32_t M0[3], const BssnPatch* patches,
+                                 double xmin, double h0, int max_w, BssnBlockDesc* blocks,
+                                 int* nblocks, int64_t* n_nodes);
 /* Mesh handle of a generated multi-level mesh.  bssn_unzip_f64 and
  * bssn_zip_f64 on it use the level maps; RK4 plans on it run the padded form
  * (ghost fill, right-hand side per block with its own spacing, owner gather,

@@ -870,6 +870,154 @@ int64_t orc_rk4_step(double** u, const OrcBlock* blks, int nblk,
                            nthreads, orc_bssnRHS, ws.data());
 }
 
+// The same RK4 step in about a third of the memory: the ghost fill and the
+// right-hand side run block by block in per-thread buffers (the padded block
+// is filled from the stage state exactly as orc_unzip fills it, the
+// right-hand side of the one block runs through `rhs` with a one-block list
+// at offset 0, and each node the block owns by orc_zip's rule takes its
+// value), so no unzipped arrays exist.  Caller arrays: acc, k, im (24 x N
+// each).  The arithmetic is orc_rk4_step's, in the same order: the final
+// state prev + C0 dt k0 + C1 dt k1 + ... is accumulated stage by stage into
+// acc, and each stage state is prev + U dt k; u holds prev until the end.
+int64_t orc_rk4_step_lowmem(double** u, const OrcBlock* blks, int nblk, const int32_t* G,
+                            double dt, const OrcParams* prm, double chi_floor, int enforce_stages,
+                            int nthreads, orc_rhs_fn rhs, double** acc, double** kbuf, double** im) {
+    static const double RK4_C[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+    static const double RK4_U[4] = {0.0, 1.0 / 2.0, 1.0 / 2.0, 1.0};
+    if (!rhs) rhs = orc_bssnRHS;
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+    const int64_t N = (int64_t)G[0] * G[1] * G[2];
+    const int M[3] = {(G[0] - 1) / 6, (G[1] - 1) / 6, (G[2] - 1) / 6};
+    std::vector<int> owner((size_t)M[0] * M[1] * M[2], -1);
+    int smax = 0;
+    for (int b = 0; b < nblk; b++) {
+        smax = std::max(smax, (int)blks[b].sz);
+        const int w = (blks[b].sz - 7) / 6;
+        const int o0[3] = {blks[b].g0[0] / 6, blks[b].g0[1] / 6, blks[b].g0[2] / 6};
+        for (int c = 0; c < w; c++)
+            for (int bb = 0; bb < w; bb++)
+                for (int a = 0; a < w; a++)
+                    owner[(o0[0] + a) + (size_t)M[0] * ((o0[1] + bb) + (size_t)M[1] * (o0[2] + c))] = b;
+    }
+#pragma omp parallel for num_threads(nthreads)
+    for (int64_t node = 0; node < N; node++)
+        for (int v = 0; v < NVARS; v++) acc[v][node] = u[v][node];
+    int64_t bad = 0;
+    const size_t cap = (size_t)smax * smax * smax;
+    for (int stage = 0; stage < 4; stage++) {
+        double** cur = stage == 0 ? u : im;
+#pragma omp parallel num_threads(nthreads)
+        {
+            std::vector<double> P(NVARS * cap), R(NVARS * cap, 0.0);
+            double *pp[NVARS], *rr[NVARS];
+            for (int v = 0; v < NVARS; v++) {
+                pp[v] = &P[v * cap];
+                rr[v] = &R[v * cap];
+            }
+#pragma omp for schedule(dynamic, 1)
+            for (int b = 0; b < nblk; b++) {
+                OrcBlock one = blks[b];
+                one.offset = 0;
+                orc_unzip(pp, (const double**)cur, &one, 1, G, NVARS);
+                rhs(rr, (const double**)pp, &one, 1, prm, 1);
+                const int s = one.sz, n = s - 6;
+                for (int k = 0; k < n; k++)
+                    for (int j = 0; j < n; j++)
+                        for (int i = 0; i < n; i++) {
+                            const int64_t g[3] = {one.g0[0] + i, one.g0[1] + j, one.g0[2] + k};
+                            int64_t o[3];
+                            for (int d = 0; d < 3; d++) o[d] = std::min<int64_t>(g[d] / 6, M[d] - 1);
+                            if (owner[o[0] + (size_t)M[0] * (o[1] + (size_t)M[1] * o[2])] != b) continue;
+                            const int64_t node = g[0] + (int64_t)G[0] * (g[1] + (int64_t)G[1] * g[2]);
+                            const int64_t p = (i + 3) + (int64_t)s * ((j + 3) + (int64_t)s * (k + 3));
+                            for (int v = 0; v < NVARS; v++) kbuf[v][node] = rr[v][p];
+                        }
+            }
+        }
+#pragma omp parallel for num_threads(nthreads) reduction(+ : bad)
+        for (int64_t node = 0; node < N; node++) {
+            for (int v = 0; v < NVARS; v++) acc[v][node] += (RK4_C[stage] * dt * kbuf[v][node]);
+            if (stage < 3) {
+                for (int v = 0; v < NVARS; v++) {
+                    im[v][node] = u[v][node];
+                    im[v][node] += (RK4_U[stage + 1] * dt * kbuf[v][node]);
+                }
+                if (enforce_stages) bad += enforce_node(im, node, chi_floor);
+            }
+        }
+    }
+#pragma omp parallel for num_threads(nthreads) reduction(+ : bad)
+    for (int64_t node = 0; node < N; node++) {
+        for (int v = 0; v < NVARS; v++) u[v][node] = acc[v][node];
+        bad += enforce_node(u, node, chi_floor);
+    }
+    return bad;
+}
+
+// Sums of squares of ham, mom0..2 and the node count over the nodes outside
+// both radii (grUtils.tcc:36-134's L2 norm before the square root), block by
+// block without unzipped arrays: each block is ghost-filled into a
+// per-thread buffer, its constraints computed (orc_physical_constraints) and
+// the nodes it owns by orc_zip's rule accumulated.  sums[0..3], sums[4] =
+// count; norm_c = sqrt(sums[c] / sums[4]).  Node coordinates xmin[d] + g h.
+void orc_constraint_sums_lowmem(const double** u, const OrcBlock* blks, int nblk, const int32_t* G,
+                                const double* xmin, double h, const double* bh,
+                                const double* radii, double* sums, int nthreads) {
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+    const int M[3] = {(G[0] - 1) / 6, (G[1] - 1) / 6, (G[2] - 1) / 6};
+    std::vector<int> owner((size_t)M[0] * M[1] * M[2], -1);
+    int smax = 0;
+    for (int b = 0; b < nblk; b++) {
+        smax = std::max(smax, (int)blks[b].sz);
+        const int w = (blks[b].sz - 7) / 6;
+        const int o0[3] = {blks[b].g0[0] / 6, blks[b].g0[1] / 6, blks[b].g0[2] / 6};
+        for (int c = 0; c < w; c++)
+            for (int bb = 0; bb < w; bb++)
+                for (int a = 0; a < w; a++)
+                    owner[(o0[0] + a) + (size_t)M[0] * ((o0[1] + bb) + (size_t)M[1] * (o0[2] + c))] = b;
+    }
+    const size_t cap = (size_t)smax * smax * smax;
+    std::vector<double> part((size_t)nblk * 5, 0.0);
+#pragma omp parallel num_threads(nthreads)
+    {
+        std::vector<double> P(NVARS * cap), Cn(4 * cap, 0.0), ws((size_t)WS_SLABS * cap);
+        double *pp[NVARS], *cc[NVARS];
+        for (int v = 0; v < NVARS; v++) pp[v] = &P[v * cap];
+        for (int c = 0; c < NVARS; c++) cc[c] = c < 4 ? &Cn[c * cap] : nullptr;
+#pragma omp for schedule(dynamic, 1)
+        for (int b = 0; b < nblk; b++) {
+            OrcBlock one = blks[b];
+            one.offset = 0;
+            orc_unzip(pp, u, &one, 1, G, NVARS);
+            const unsigned sz[3] = {(unsigned)one.sz, (unsigned)one.sz, (unsigned)one.sz};
+            orc_physical_constraints(cc, (const double**)pp, 0, one.ptmin, one.ptmax, sz, one.bflag, ws.data());
+            const int s = one.sz, n = s - 6;
+            double acc[5] = {0, 0, 0, 0, 0};
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++) {
+                        const int64_t g[3] = {one.g0[0] + i, one.g0[1] + j, one.g0[2] + k};
+                        int64_t o[3];
+                        for (int d = 0; d < 3; d++) o[d] = std::min<int64_t>(g[d] / 6, M[d] - 1);
+                        if (owner[o[0] + (size_t)M[0] * (o[1] + (size_t)M[1] * o[2])] != b) continue;
+                        const double x = xmin[0] + g[0] * h, y = xmin[1] + g[1] * h, z = xmin[2] + g[2] * h;
+                        const double d1 = std::sqrt((x - bh[0]) * (x - bh[0]) + (y - bh[1]) * (y - bh[1]) +
+                                                    (z - bh[2]) * (z - bh[2]));
+                        const double d2 = std::sqrt((x - bh[3]) * (x - bh[3]) + (y - bh[4]) * (y - bh[4]) +
+                                                    (z - bh[5]) * (z - bh[5]));
+                        if (d1 < radii[0] || d2 < radii[1]) continue;
+                        const int64_t p = (i + 3) + (int64_t)s * ((j + 3) + (int64_t)s * (k + 3));
+                        for (int c = 0; c < 4; c++) acc[c] += Cn[c * cap + p] * Cn[c * cap + p];
+                        acc[4] += 1.0;
+                    }
+            for (int c = 0; c < 5; c++) part[(size_t)b * 5 + c] = acc[c];
+        }
+    }
+    for (int c = 0; c < 5; c++) sums[c] = 0.0;
+    for (int b = 0; b < nblk; b++)
+        for (int c = 0; c < 5; c++) sums[c] += part[(size_t)b * 5 + c];
+}
+
 // ---------------------------------------------------------------------------
 // Synthetic single-level octree meshes (the workloads' block lists), restated
 // from the definition the product library's generator documents: mode 0 = a

@@ -116,6 +116,20 @@ int64_t orc_rk4_step_ws(double** u, const OrcBlock* blks, int nblk, const int32_
                         int64_t n_unzip, double dt, const OrcParams* prm, double chi_floor,
                         int enforce_stages, int nthreads, orc_rhs_fn rhs, double* ws);
 
+/* The same step without unzipped arrays (ghost fill and right-hand side per
+ * block in per-thread buffers; acc, kbuf, im: caller arrays of N per
+ * variable): identical arithmetic, for meshes whose unzipped copies do not
+ * fit in host memory. */
+int64_t orc_rk4_step_lowmem(double** u, const OrcBlock* blks, int nblk, const int32_t* G,
+                            double dt, const OrcParams* prm, double chi_floor, int enforce_stages,
+                            int nthreads, orc_rhs_fn rhs, double** acc, double** kbuf, double** im);
+
+/* Constraint L2 sums (ham, mom0..2, count) over nodes outside both radii,
+ * block by block without unzipped arrays; norm = sqrt(sums[c] / sums[4]). */
+void orc_constraint_sums_lowmem(const double** u, const OrcBlock* blks, int nblk, const int32_t* G,
+                                const double* xmin, double h, const double* bh,
+                                const double* radii, double* sums, int nthreads);
+
 /* --- the workloads' synthetic single-level octree meshes (block lists; see
  * bssn_oracle.cpp).  blks NULL: only *nblk, G and *h are set.  0 = ok. */
 int orc_mesh_generate(int mode, const int32_t* dims, const double* p, uint64_t seed,

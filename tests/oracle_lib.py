@@ -235,6 +235,18 @@ class MeshOracle:
                                         self.spec.n_unzip, dt, C.byref(prm), chi_floor,
                                         int(enforce_stages), nthreads, fn, P(ws))
 
+    def rk4_step_lowmem(self, Z, dt, prm, bufs, rhs_fn=None, chi_floor=1e-4, enforce_stages=True,
+                        nthreads=0):
+        """orc_rk4_step_lowmem: bufs = three (24, n_nodes) float64 arrays
+        (accumulator, stage right-hand side, stage state)."""
+        f = self.lib.orc_rk4_step_lowmem
+        f.restype = C.c_int64
+        f.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_void_p, C.c_double,
+                      C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        fn = C.cast(rhs_fn, C.c_void_p) if rhs_fn is not None else None
+        return f(rows(Z), self.spec.blocks, self.spec.nblocks, self.G, dt, C.byref(prm), chi_floor,
+                 int(enforce_stages), nthreads, fn, rows(bufs[0]), rows(bufs[1]), rows(bufs[2]))
+
     def rk4_step(self, Z, dt, prm, chi_floor=1e-4, enforce_stages=True, nthreads=0):
         self.lib.orc_rk4_step.restype = C.c_int64
         return self.lib.orc_rk4_step(rows(Z), self.spec.blocks, self.spec.nblocks, self.G,
@@ -288,6 +300,21 @@ def oracle_constraints(spec, Uz, lib=None, threads=1):
         with ThreadPoolExecutor(threads) as ex:
             list(ex.map(run, [range(t, spec.nblocks, threads) for t in range(threads)]))
     return MeshOracle(spec, O).zip(Cz, nvars=4)[:4]
+
+
+def constraint_norms_lowmem(spec, Z, lib=None, bh=(1.0, 0.0, 0.0, -1.0, 0.0, 0.0), radii=(0.5, 0.5),
+                            threads=0):
+    """The masked constraint L2 norms of a zipped state, block by block
+    (orc_constraint_sums_lowmem: no unzipped copies)."""
+    O = lib or oracle()
+    f = O.lib.orc_constraint_sums_lowmem
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
+                  C.c_void_p, C.c_void_p, C.c_int]
+    sums = np.zeros(5)
+    org = getattr(spec, "origin3", (spec.xmin,) * 3)
+    f(rows(Z), spec.blocks, spec.nblocks, (C.c_int32 * 3)(*spec.G), (C.c_double * 3)(*org), spec.h,
+      (C.c_double * 6)(*bh), (C.c_double * 2)(*radii), P(sums), threads)
+    return np.sqrt(sums[:4] / sums[4])
 
 
 def oracle_psi4(spec, Uz, lib=None):

@@ -1,5 +1,12 @@
 """GPU parity at the sizes of the benchmark configurations.
 
+Config 3 (the batched workload, mix20k: 20,909 blocks, 87.0 M zones): ten
+graph-replayed RK4 steps through the plan with the right-hand side tiles the
+autotuner picks, constraint L2 norms by the plan's in-graph diagnostics
+after every second step, against the norms the reference's own compiled
+right-hand side produced on the CPU (tests/golden/config3_norms.json,
+make_config3_golden.py), to 1e-10.
+
 Config 2 (the mixed-size octree at the plain-path size): 4,108 blocks of
 sides 13..55 with the configured size mix, ten graph-replayed RK4 steps
 (ghost fill, right-hand side, zip, stage algebra, enforcement) from the
@@ -80,3 +87,37 @@ def test_config2_ten_steps_vs_reference(rhs):
     assert (np.abs(sumsq - gold["sumsq"]) / gold["sumsq"]).max() <= 2 * TOL_STATE
     rel = np.abs(np.array(hist) - gold["norms"]) / np.abs(gold["norms"])
     assert rel.max() <= TOL_NORMS, rel.max(axis=1)
+
+
+def test_config3_norms_mix20k():
+    import json
+    import bssn_b200 as B
+    path = os.path.join(HERE, "golden", "config3_norms.json")
+    with open(path) as f:
+        gold = json.load(f)
+    spec = B.generate_mesh(1, (10, 10, 7), seed=20261203)
+    assert spec.nblocks == gold["nblocks"] and spec.zones() == gold["zones"]
+    mo = ol.MeshOracle(spec, ol.oracle())
+    U = torch.from_numpy(mo.initial_data(eps=1e-8)).cuda()
+    m = B.Mesh(spec)
+    plan = B.RK4Plan(m, B.default_params(), B.PLAN_ENFORCE_STAGES | B.PLAN_GRAPH)
+    plan.autotune(U, reps=1)
+    norms = torch.zeros(4, dtype=torch.float64, device="cuda")
+    dt = 0.25 * spec.h
+    got = {}
+    plan.diagnostics(U, norms)
+    torch.cuda.synchronize()
+    got[0] = norms.cpu().numpy().copy()
+    for step in range(1, 11):
+        plan.step(U, dt)
+        if step % 2 == 0:
+            plan.diagnostics(U, norms)
+            torch.cuda.synchronize()
+            got[step] = norms.cpu().numpy().copy()
+    assert plan.violations() == gold["enforce_violations"]
+    plan.close()
+    worst = 0.0
+    for h in gold["history"]:
+        ref = np.array([float.fromhex(x) for x in h["norms"]])
+        worst = max(worst, (np.abs(got[h["step"]] - ref) / np.abs(ref)).max())
+    assert worst <= TOL_NORMS, worst

@@ -177,3 +177,34 @@ def test_oracle_rk4_matches_reference_history_10_steps(O, REF):
     ref = np.array([float.fromhex(x) for x in gold["history"][1]["norms"]])
     assert gold["history"][1]["step"] == 10
     assert np.abs(got - ref).max() / np.abs(ref).min() <= 1e-10, (got, ref)
+
+
+def test_lowmem_rk4_step_bit_identical():
+    """The block-by-block RK4 step (no unzipped arrays; used for the
+    largest goldens) equals the oracle's RK4 step bit for bit, with the
+    oracle's and with the reference's compiled right-hand side."""
+    spec = ol.OracleMeshSpec(1, (2, 1, 1), seed=1, xmin=-8.25)
+    mo = ol.MeshOracle(spec, ol.oracle())
+    Z0 = mo.initial_data(eps=1e-8)
+    ref = ol.reference()
+    fns = [None] + ([ref.lib.ref_bssnRHS_blocks] if ref is not None else [])
+    for fn in fns:
+        A, Bz = Z0.copy(), Z0.copy()
+        ws = mo.rk4_workspace()
+        bufs = [np.zeros_like(Z0) for _ in range(3)]
+        for _ in range(2):
+            assert mo.rk4_step_ws(A, 0.25 * spec.h, ol.params(), ws, rhs_fn=fn) == 0
+            assert mo.rk4_step_lowmem(Bz, 0.25 * spec.h, ol.params(), bufs, rhs_fn=fn) == 0
+        assert np.array_equal(A.view(np.uint64), Bz.view(np.uint64))
+
+
+def test_lowmem_constraint_norms_match():
+    """Block-by-block constraint norms equal the unzipped computation to
+    rounding of the summation order."""
+    spec = ol.OracleMeshSpec(1, (2, 1, 1), seed=1, xmin=-8.25)
+    O = ol.oracle()
+    mo = ol.MeshOracle(spec, O)
+    Z = mo.initial_data(eps=1e-6)
+    ref = ol.l2_norms(spec, ol.oracle_constraints(spec, mo.unzip(Z), O))
+    got = ol.constraint_norms_lowmem(spec, Z, O)
+    assert np.allclose(got, ref, rtol=1e-13, atol=0), (got, ref)
