@@ -528,7 +528,9 @@ def main():
         torch.cuda.synchronize()
         pms = max_over_ranks(a0.elapsed_time(a1)) / k
         plain = {"value": zones * world / (pms * 1e-3), "ms_per_step": pms, "steps": k,
-                 "launches_per_step": 4 * (spec.nblocks + 2)}
+                 "launches_per_step": B.lib.bssn_rk4_plan_launches_per_step(pplan.h),
+                 "path": "the batched plan's own right-hand-side kernels and tiles, launched block by "
+                         "block in mesh order (the reference's bssnRHS loop, rhs.cpp:10-73), no graph"}
         pplan.close()
 
     # ---- end to end through the C ABI with host buffers
