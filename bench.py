@@ -12,8 +12,11 @@ as a CUDA graph.  Prints one JSON line (see the keys below).
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload mix20k|mix4k|uniform512|small|levels]
 
-Under torchrun each rank evolves its own replica of the workload (weak
-scaling); the time is the max over ranks.
+Under torchrun (N > 1) the mixed workloads run partitioned by default: the
+workload's super-cell box stretched N times along z (weak scaling), its
+blocks split along their Z-order over the ranks, each rank evolving its
+share with the halo exchange (NCCL) before every RK4 stage; --replicas
+runs N independent copies instead.  The time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -412,8 +415,11 @@ def main():
                     help="pin tiles instead of autotuning (profiling runs): one tile id for every "
                          "bucket, or side:tile pairs such as 13:6,19:6,31:8,55:6")
     ap.add_argument("--partition", action="store_true",
-                    help="multi-GPU form: one mesh N times larger, partitioned along the Z-order "
-                         "of its blocks, halo exchange before every RK4 stage (mixed workloads)")
+                    help="multi-GPU form (the default for N > 1 on mixed workloads): one mesh N times "
+                         "larger, partitioned along the Z-order of its blocks, halo exchange before "
+                         "every RK4 stage")
+    ap.add_argument("--replicas", action="store_true",
+                    help="N > 1: N independent replicas of the workload instead of the partitioned form")
     args = ap.parse_args()
     wl = args.workload
     if args.impl == "reference":
@@ -444,7 +450,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    if args.partition:
+    if args.partition or (world > 1 and WORKLOADS[wl][0] == 1 and not args.replicas):
         run_partitioned(args, wl, B, torch, dist, world, rank, local, barrier, max_over_ranks)
         if dist is not None:
             dist.destroy_process_group()

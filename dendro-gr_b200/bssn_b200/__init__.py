@@ -98,6 +98,7 @@ def _sig():
     lib.bssn_remesh_wavelet_f64.argtypes = [vp, vp, i, d, vp, vp, vp, vp]
     lib.bssn_remesh_features_f64.argtypes = [vp, vp, vp, vp]
     lib.bssn_remesh_mlp_fwd_bf16.argtypes = [vp, vp, vp, i, vp, vp]
+    lib.bssn_remesh_mlp_fwd_fp32_bf16.argtypes = [vp, vp, vp, i, vp, vp]
     lib.bssn_remesh_mlp_grad_scratch.argtypes = [i]
     lib.bssn_remesh_mlp_grad_scratch.restype = C.c_size_t
     lib.bssn_remesh_mlp_bwd_bf16.argtypes = [vp, vp, vp, vp, vp, i, vp, vp, vp, vp]
@@ -493,10 +494,19 @@ class RemeshMLP:
         self.norm = torch.cat([mu, 1.0 / sd]).float().contiguous()
 
     def logits(self, X, stream=None):
+        """Logits of the decisions' forward (tensor cores, BF16 operands)."""
         import torch
         out = torch.empty(X.shape[0], dtype=torch.float32, device="cuda")
         check(lib.bssn_remesh_mlp_fwd_bf16(_vp(self.wq), _vp(self.norm), _vp(X), X.shape[0], _vp(out),
                                            stream_ptr(stream)), "mlp_fwd")
+        return out
+
+    def logits_fp32(self, X, stream=None):
+        """Logits with FP32 activations (the training gradient's forward)."""
+        import torch
+        out = torch.empty(X.shape[0], dtype=torch.float32, device="cuda")
+        check(lib.bssn_remesh_mlp_fwd_fp32_bf16(_vp(self.wq), _vp(self.norm), _vp(X), X.shape[0], _vp(out),
+                                                stream_ptr(stream)), "mlp_fwd_fp32")
         return out
 
     def grad(self, X, Y, Cw=None, stream=None):

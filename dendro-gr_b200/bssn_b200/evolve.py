@@ -262,8 +262,11 @@ def main(argv=None):
     ap.add_argument("--amr-fac", type=float, default=0.1, help="keep threshold / tol (BSSN_DENDRO_AMR_FAC)")
     ap.add_argument("--audit", type=float, default=0.05)
     ap.add_argument("--train-steps", type=int, default=2000)
-    ap.add_argument("--margin", type=float, default=1.0,
+    ap.add_argument("--margin", type=float, default=0.5,
                     help="lower threshold margin in logit units (remesh_train.pick_thresholds)")
+    ap.add_argument("--fp-target", type=float, default=1e-2,
+                    help="fraction of validation negatives the upper threshold may let through "
+                         "(extra refinement or a delayed coarsening, never a missed refinement)")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     a.max_box = a.max_box or a.M0
@@ -280,13 +283,13 @@ def main(argv=None):
         net = RemeshMLP(seed=seed)
         train(net, X[tr], lab[tr], steps=a.train_steps, log=lambda s: None)
         pv = torch.sigmoid(net.logits(torch.tensor(X[va], device="cuda"))).cpu().numpy()
-        net.lo, net.hi = pick_thresholds(pv, lab[va], margin=a.margin)
+        net.lo, net.hi = pick_thresholds(pv, lab[va], fp_target=a.fp_target, margin=a.margin)
         nets.append(net)
     train_s = time.perf_counter() - t0
     le = run("learned", a, nets=nets)
     res = {"config": {k: getattr(a, k) for k in ("M0", "levels", "max_levels", "half", "max_box", "steps", "remesh_every",
                                                  "diag_every", "cfl", "tol", "amr_fac", "audit", "train_steps",
-                                                 "margin", "max_block_octants")},
+                                                 "margin", "fp_target", "max_block_octants")},
            "training": {"samples": int(len(tr)), "validation": int(nva), "refine_labels": int(Y.sum()),
                         "keep_labels": int(K.sum()), "thresholds": [[n.lo, n.hi] for n in nets],
                         "seconds": train_s},

@@ -456,6 +456,12 @@ int bssn_remesh_mlp_fwd_bf16(const void* wq_dev, const float* norm_dev, const fl
     return bssn::launch_mlp_fwd(wq_dev, norm_dev, x_dev, n, logits_dev, S(stream));
 }
 
+int bssn_remesh_mlp_fwd_fp32_bf16(const void* wq_dev, const float* norm_dev, const float* x_dev, int n,
+                                  float* logits_dev, bssn_stream_t stream) {
+    if (!wq_dev || !x_dev || !logits_dev || n < 0) return BSSN_EINVAL;
+    return bssn::launch_mlp_fwd_fp32(wq_dev, norm_dev, x_dev, n, logits_dev, S(stream));
+}
+
 size_t bssn_remesh_mlp_grad_scratch(int n) { return n > 0 ? bssn::mlp_grad_scratch_floats(n) : 0; }
 
 int bssn_remesh_mlp_bwd_bf16(const void* wq_dev, const float* norm_dev, const float* x_dev,

@@ -222,6 +222,104 @@ __global__ void __launch_bounds__(MLP_THREADS) mlp_fwd_kernel(const __nv_bfloat1
     logits[i] = out;
 }
 
+// Forward on the tensor cores: mma.sync m16n8k16 with BF16 operands and FP32
+// accumulation.  A warp evaluates 32 samples (two 16-row tiles): layer 1
+// (16 -> 64) is one k-step of 8 n-tiles, its accumulators go through bias +
+// GELU and, converted to BF16, are directly the A operands of layer 2
+// (64 -> 64; the m16n8 accumulator layout of two adjacent n-tiles is the
+// m16k16 A layout of one k-step), and the output layer (64 -> 1) is a dot
+// product summed over the four threads that share a row.  The inputs and
+// the hidden activations are rounded to BF16 as the operands require; every
+// sum accumulates in FP32.
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+__device__ __forceinline__ void mma_bf16_16816(float d[4], const uint32_t a[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__global__ void __launch_bounds__(MLP_THREADS) mlp_fwd_mma_kernel(const __nv_bfloat16* __restrict__ wq,
+                                                                  const float* __restrict__ norm,
+                                                                  const float* __restrict__ X, int n,
+                                                                  float* __restrict__ logits) {
+    // BF16 weights as loaded (W1 [64][16], W2 [64][64] row-major by output),
+    // FP32 biases and output weights
+    __shared__ __align__(16) __nv_bfloat16 w1[HID * IN], w2[HID * HID];
+    __shared__ float b1[HID], b2[HID], w3[HID], b3;
+    __shared__ float nm[2 * IN];
+    for (int q = threadIdx.x; q < HID * IN; q += blockDim.x) w1[q] = wq[OW1 + q];
+    for (int q = threadIdx.x; q < HID * HID; q += blockDim.x) w2[q] = wq[OW2 + q];
+    for (int q = threadIdx.x; q < HID; q += blockDim.x) {
+        b1[q] = __bfloat162float(wq[OB1 + q]);
+        b2[q] = __bfloat162float(wq[OB2 + q]);
+        w3[q] = __bfloat162float(wq[OW3 + q]);
+    }
+    if (threadIdx.x == 0) b3 = __bfloat162float(wq[OB3]);
+    if (threadIdx.x < 2 * IN) nm[threadIdx.x] = norm ? norm[threadIdx.x] : (threadIdx.x < IN ? 0.0f : 1.0f);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int base = (blockIdx.x * blockDim.x + (threadIdx.x & ~31));  // first sample of the warp
+    auto xin = [&](int row, int k) {
+        const int i = base + row;
+        return i < n ? (X[(int64_t)i * IN + k] - nm[k]) * nm[IN + k] : 0.0f;
+    };
+    auto wpair = [&](const __nv_bfloat16* w, int ld, int row, int col) {
+        return *reinterpret_cast<const uint32_t*>(w + row * ld + col);
+    };
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++) {
+        const int r0 = mt * 16 + g, r1 = r0 + 8;
+        // layer 1: A = normalised inputs (rows r0, r1; features 2t.., 2t+8..)
+        const uint32_t a1[4] = {pack_bf16(xin(r0, 2 * t), xin(r0, 2 * t + 1)),
+                                pack_bf16(xin(r1, 2 * t), xin(r1, 2 * t + 1)),
+                                pack_bf16(xin(r0, 2 * t + 8), xin(r0, 2 * t + 9)),
+                                pack_bf16(xin(r1, 2 * t + 8), xin(r1, 2 * t + 9))};
+        float h[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            h[nt][0] = h[nt][1] = h[nt][2] = h[nt][3] = 0.0f;
+            mma_bf16_16816(h[nt], a1, wpair(w1, IN, nt * 8 + g, 2 * t), wpair(w1, IN, nt * 8 + g, 2 * t + 8));
+            const int c = nt * 8 + 2 * t;
+            h[nt][0] = gelu(h[nt][0] + b1[c]);
+            h[nt][1] = gelu(h[nt][1] + b1[c + 1]);
+            h[nt][2] = gelu(h[nt][2] + b1[c]);
+            h[nt][3] = gelu(h[nt][3] + b1[c + 1]);
+        }
+        // layer 2: A k-step kt = the activations of layer-1 n-tiles 2kt, 2kt+1
+        float o0 = 0.0f, o1 = 0.0f;  // output-layer partial sums of rows r0, r1
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            float d[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int kt = 0; kt < 4; kt++) {
+                const uint32_t a2[4] = {pack_bf16(h[2 * kt][0], h[2 * kt][1]), pack_bf16(h[2 * kt][2], h[2 * kt][3]),
+                                        pack_bf16(h[2 * kt + 1][0], h[2 * kt + 1][1]),
+                                        pack_bf16(h[2 * kt + 1][2], h[2 * kt + 1][3])};
+                mma_bf16_16816(d, a2, wpair(w2, HID, nt * 8 + g, kt * 16 + 2 * t),
+                               wpair(w2, HID, nt * 8 + g, kt * 16 + 2 * t + 8));
+            }
+            const int c = nt * 8 + 2 * t;
+            o0 = fmaf(w3[c], gelu(d[0] + b2[c]), o0);
+            o0 = fmaf(w3[c + 1], gelu(d[1] + b2[c + 1]), o0);
+            o1 = fmaf(w3[c], gelu(d[2] + b2[c]), o1);
+            o1 = fmaf(w3[c + 1], gelu(d[3] + b2[c + 1]), o1);
+        }
+        o0 += __shfl_xor_sync(0xffffffffu, o0, 1);
+        o0 += __shfl_xor_sync(0xffffffffu, o0, 2);
+        o1 += __shfl_xor_sync(0xffffffffu, o1, 1);
+        o1 += __shfl_xor_sync(0xffffffffu, o1, 2);
+        if (t == 0) {
+            if (base + r0 < n) logits[base + r0] = o0 + b3;
+            if (base + r1 < n) logits[base + r1] = o1 + b3;
+        }
+    }
+}
+
 // Forward + backward of the weighted binary cross-entropy
 //   L = sum_i c_i * BCE(sigmoid(z_i), y_i) / n
 // for MLP_THREADS samples per CTA (one per thread).  Each CTA writes its
@@ -416,12 +514,16 @@ __global__ void __launch_bounds__(256) remesh_select2_kernel(const float* __rest
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nblk) return;
     const float pr = 1.0f / (1.0f + expf(-lr[b])), pk = 1.0f / (1.0f + expf(-lk[b]));
-    const bool ur = pr > lo_r && pr < hi_r, uk = pk > lo_k && pk < hi_k;
+    // refine implies keep (score > tol > keep_fac tol): a confident refine
+    // settles keep, a confident "no keep" settles refine
+    const bool refine_sure = pr >= hi_r, nokeep_sure = pk <= lo_k;
+    const bool ur = pr > lo_r && pr < hi_r && !nokeep_sure;
+    const bool uk = pk > lo_k && pk < hi_k && !refine_sure;
     const double u = (double)(hmix(seed + 0x9E3779B97F4A7C15ULL * (uint64_t)(b + 1)) >> 11) *
                      (1.0 / 9007199254740992.0);
     const bool audit = u < audit_frac;
     need[b] = (ur || uk || audit) ? 1 : 0;
-    decided[b] = (pr >= hi_r ? 1 : 0) | (pk >= hi_k ? 2 : 0);
+    decided[b] = (refine_sure && !nokeep_sure ? 1 : 0) | (pk >= hi_k || refine_sure ? 2 : 0);
     if (ur) atomicAdd(&stats[0], 1);
     if (uk) atomicAdd(&stats[1], 1);
     if (audit && !ur && !uk) atomicAdd(&stats[2], 1);
@@ -520,6 +622,14 @@ int launch_features(const MeshState* m, const double* const* U, float* feats, cu
 
 int launch_mlp_fwd(const void* wq, const float* norm, const float* X, int n, float* logits,
                    cudaStream_t s) {
+    if (n <= 0) return 0;
+    mlp_fwd_mma_kernel<<<(n + MLP_THREADS - 1) / MLP_THREADS, MLP_THREADS, 0, s>>>(
+        (const __nv_bfloat16*)wq, norm, X, n, logits);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_mlp_fwd_fp32(const void* wq, const float* norm, const float* X, int n, float* logits,
+                        cudaStream_t s) {
     if (n <= 0) return 0;
     mlp_fwd_kernel<<<(n + MLP_THREADS - 1) / MLP_THREADS, MLP_THREADS, 0, s>>>(
         (const __nv_bfloat16*)wq, norm, X, n, logits);

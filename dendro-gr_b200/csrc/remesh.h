@@ -23,8 +23,13 @@ int launch_wavelet_scores(MeshState* m, const double* const* U, int nvars, doubl
 int launch_block_flags(MeshState* m, const double* scores, int nvars, double tol, double* ratio,
                        uint8_t* flags, const uint8_t* need, cudaStream_t s);
 int launch_features(const MeshState* m, const double* const* U, float* feats, cudaStream_t s);
+// tensor-core forward (BF16 operands, FP32 accumulation); the decisions use it
 int launch_mlp_fwd(const void* wq, const float* norm, const float* X, int n, float* logits,
                    cudaStream_t s);
+// the same network with FP32 activations on the FP32 pipes (the training
+// kernel's forward)
+int launch_mlp_fwd_fp32(const void* wq, const float* norm, const float* X, int n, float* logits,
+                        cudaStream_t s);
 size_t mlp_grad_scratch_floats(int n);
 int launch_mlp_grad(const void* wq, const float* norm, const float* X, const float* Y,
                     const float* C, int n, float* grad, float* loss, float* scratch,

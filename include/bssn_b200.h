@@ -262,9 +262,17 @@ int bssn_remesh_features_f64(bssn_mesh mesh, const double* const* unzip_dev,
  * (optional): 16 means then 16 inverse standard deviations applied to the
  * inputs. */
 #define BSSN_MLP_NPARAM 5313
+/* Logits on the tensor cores (mma.sync, BF16 operands: the normalised
+ * inputs and hidden activations are rounded to BF16; FP32 accumulation).
+ * The learned decisions use this forward. */
 int bssn_remesh_mlp_fwd_bf16(const void* wq_dev, const float* norm_dev,
                              const float* x_dev, int n, float* logits_dev,
                              bssn_stream_t stream);
+/* The same network with FP32 activations (the forward of the training
+ * gradient, bssn_remesh_mlp_bwd_bf16). */
+int bssn_remesh_mlp_fwd_fp32_bf16(const void* wq_dev, const float* norm_dev,
+                                  const float* x_dev, int n, float* logits_dev,
+                                  bssn_stream_t stream);
 /* floats of scratch bssn_remesh_mlp_bwd_bf16 needs for n samples */
 size_t bssn_remesh_mlp_grad_scratch(int n);
 /* Gradient of L = sum_i c_i BCE(sigmoid(z_i), y_i) / n with respect to the
@@ -320,7 +328,10 @@ int bssn_remesh_decide_f64(bssn_mesh mesh, const double* const* unzip_dev,
  * BSSN_DENDRO_AMR_FAC) from wq_keep with lo_k / hi_k.  The features are
  * computed once; the exact wavelet test runs once, on the blocks either
  * network is unsure of plus one seeded audit sample (fraction audit_frac),
- * and gives both flags there.  stats_dev (8 ints): blocks uncertain for
+ * and gives both flags there.  Refine implies keep: a block the refine
+ * network is sure to refine (p_r >= hi_r) keeps its level without asking
+ * the keep network, and a block the keep network is sure to release
+ * (p_k <= lo_k) is not refined.  stats_dev (8 ints): blocks uncertain for
  * refine, uncertain for keep, extra audited blocks, audited refine misses of
  * the network (p_r <= lo_r, exact refines), audited exact refines, audited
  * keep misses, audited exact keeps, 0.  work_dev:

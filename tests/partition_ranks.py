@@ -178,6 +178,8 @@ def gpu_rank(rank, world, port, kind, steps, outdir):
         got = U.cpu().numpy()
         np.save(os.path.join(outdir, f"vals{rank}.npy"), got[:, pr.sub.owned])
         np.save(os.path.join(outdir, f"ids{rank}.npy"), pr.sub.owned_global)
+        # the global constraint norms, reduced over the ranks (every rank calls it)
+        np.save(os.path.join(outdir, f"norms{rank}.npy"), pr.constraint_norms(U))
         pr.close()
     finally:
         dist.destroy_process_group()

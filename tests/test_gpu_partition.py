@@ -27,13 +27,21 @@ def test_partitioned_gpu_step_matches_single_domain(kind):
     U = torch.from_numpy(Z0).cuda()
     for _ in range(steps):
         plan.step(U, 0.25 * spec.h)
+    norms = torch.zeros(4, dtype=torch.float64, device="cuda")
+    plan.diagnostics(U, norms)
     torch.cuda.synchronize()
     ref = U.cpu().numpy()
+    ref_norms = norms.cpu().numpy()
     plan.close()
     m.close()
     with tempfile.TemporaryDirectory() as d:
         run_ranks(pr.gpu_rank, world, kind, steps, d)
         ids, vals = gather(d, world)
+        got_norms = [np.load(f"{d}/norms{r}.npy") for r in range(world)]
     assert len(np.unique(np.concatenate(ids))) == spec.n_nodes
     for i, v in zip(ids, vals):
         assert np.array_equal(v, ref[:, i])
+    # norms from owned-node sums reduced over the ranks (different summation
+    # order than the single domain's reduction)
+    for n in got_norms:
+        assert np.allclose(n, ref_norms, rtol=1e-12, atol=0), (n, ref_norms)

@@ -110,7 +110,7 @@ def test_mlp_forward_backward_vs_numpy(B):
     Y = torch.tensor((rng.random(n) < 0.3).astype(np.float32), device="cuda")
     Cw = torch.tensor(rng.uniform(0.5, 2.0, n).astype(np.float32), device="cuda")
     net.set_norm(X)
-    z = net.logits(X)
+    z = net.logits_fp32(X)
     g, loss = net.grad(X, Y, Cw)
     torch.cuda.synchronize()
     p = net.wq.float().cpu().numpy().astype(np.float64)  # the BF16 values the kernels use
@@ -121,6 +121,39 @@ def test_mlp_forward_backward_vs_numpy(B):
     assert abs(loss.item() - lr) <= 1e-5 * abs(lr)
     gg = g.cpu().numpy()
     assert np.abs(gg - gr).max() <= 1e-3 * np.abs(gr).max(), np.abs(gg - gr).max() / np.abs(gr).max()
+
+
+def _bf16(a):
+    """Round float32 values to BF16 (nearest, ties to even), as float32."""
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return u.view(np.float32)
+
+
+def test_mlp_tensor_core_forward(B):
+    """The decisions' forward on the tensor cores (mma.sync m16n8k16, BF16
+    operands, FP32 accumulation) against a float64 restatement that rounds
+    the normalised inputs and the hidden activations to BF16 as the operands
+    do, and close to the FP32-activation forward; 1001 samples leave a
+    partial last warp."""
+    from scipy.special import erf
+    net = B.RemeshMLP(seed=7)
+    rng = np.random.default_rng(3)
+    n = 1001
+    X = torch.tensor(rng.standard_normal((n, 16)) * 2 + 1, dtype=torch.float32, device="cuda")
+    net.set_norm(X)
+    z = net.logits(X).cpu().numpy().astype(np.float64)
+    z32 = net.logits_fp32(X).cpu().numpy().astype(np.float64)
+    p = net.wq.float().cpu().numpy().astype(np.float64)
+    norm = net.norm.cpu().numpy()
+    W1, b1, W2, b2, W3, b3 = _split(p)
+    gelu = lambda a: 0.5 * a * (1.0 + erf(a / np.sqrt(2.0)))
+    x = _bf16((X.cpu().numpy() - norm[:16]) * norm[16:]).astype(np.float64)
+    h1 = _bf16(gelu(x @ W1.T + b1)).astype(np.float64)
+    zr = gelu(h1 @ W2.T + b2) @ W3 + b3
+    scale = np.abs(zr).max()
+    assert np.abs(z - zr).max() <= 5e-3 * scale, np.abs(z - zr).max() / scale
+    assert np.abs(z - z32).max() <= 3e-2 * np.abs(z32).max(), np.abs(z - z32).max() / np.abs(z32).max()
 
 
 def test_adam_step_vs_numpy(B):
