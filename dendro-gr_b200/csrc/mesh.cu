@@ -149,6 +149,11 @@ void mesh_destroy(MeshState* m) {
     cudaFree(m->d_partial);
     cudaFree(m->d_elems);
     cudaFree(m->d_elem_first);
+    cudaFree(m->d_fchunks);
+    cudaFree(m->d_need_off);
+    cudaFree(m->d_need_list);
+    cudaFree(m->d_fchunk_first);
+    cudaFree(m->d_fpart);
     for (auto& t : m->tasks) cudaFree(t.second.first);
     cudaFree(m->d_scratch);
     if (m->lv) {

@@ -49,6 +49,17 @@ struct MeshState {
     ElemRef* d_elems = nullptr;
     int64_t* d_elem_first = nullptr;
     int64_t n_elems = 0;
+    // element list of the blocks a decision sends to the exact test: offsets
+    // per block, the count (stored after the offsets) and the list
+    int64_t* d_need_off = nullptr;
+    int64_t* d_need_count = nullptr;
+    int32_t* d_need_list = nullptr;
+    // runs of sublattice points for the block features, the first run of each
+    // block and the runs' partial maxima (built on first use)
+    Chunk* d_fchunks = nullptr;
+    int64_t* d_fchunk_first = nullptr;
+    double* d_fpart = nullptr;
+    int n_fchunks = 0;
     // autotuned tile per padded side (0 = not tuned)
     std::map<int, int> tuned;
     // scratch of the split right-hand side (kSplitSlots doubles per zone)

@@ -17,6 +17,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -33,143 +34,299 @@ __constant__ double kWfine[3][6] = {
     {3.0 / 256, -25.0 / 256, 75.0 / 128, 75.0 / 128, -25.0 / 256, 3.0 / 256},
     {-3.0 / 256, 21.0 / 256, -35.0 / 128, 105.0 / 128, 105.0 / 256, -7.0 / 256}};
 
-__device__ double wavelet_interp(const double* __restrict__ p, int s, int a, int b, int c) {
-    const int loc[3] = {a, b, c};
-    int n[3], base[3], step[3], wrow[3];
-    for (int d = 0; d < 3; d++) {
-        if (loc[d] & 1) {
-            n[d] = 6;
-            base[d] = 1;
-            step[d] = 2;
-            wrow[d] = (loc[d] - 1) / 2;
-        } else {
-            n[d] = 1;
-            base[d] = loc[d] + 3;
-            step[d] = 0;
-            wrow[d] = -1;
-        }
-    }
-    double az = 0.0;
-    for (int k = 0; k < n[2]; k++) {
-        const int pz = base[2] + step[2] * k;
-        double ay = 0.0;
-        for (int j = 0; j < n[1]; j++) {
-            const int py = base[1] + step[1] * j;
-            double ax = 0.0;
-            const double* row = p + (int64_t)s * (py + (int64_t)s * pz);
-            for (int i = 0; i < n[0]; i++) {
-                const double wx = wrow[0] < 0 ? 1.0 : kWfine[wrow[0]][i];
-                ax = __dadd_rn(ax, __dmul_rn(wx, __ldg(row + base[0] + step[0] * i)));
-            }
-            const double wy = wrow[1] < 0 ? 1.0 : kWfine[wrow[1]][j];
-            ay = __dadd_rn(ay, __dmul_rn(wy, ax));
-        }
-        const double wz = wrow[2] < 0 ? 1.0 : kWfine[wrow[2]][k];
-        az = __dadd_rn(az, __dmul_rn(wz, ay));
-    }
-    return az;
-}
+// Separable form of the test, one warp per (element, variable).  The
+// interpolation at a node is a tensor product, evaluated inner x, then y,
+// then z; every partial sum of that product is shared by the nodes with the
+// same remaining coordinates, so the warp forms each once:
+//   X[k][j][a] = x-interpolation on coarse row (j, k) at element x-index a,
+//   Y[k][b][a] = y-interpolation of X over the coarse rows j,
+//   Z[c][b][a] = z-interpolation of Y over the coarse planes k,
+// where the coarse points are the patch positions 1,3,...,11 along each
+// axis (an even element index a sits on coarse point a/2 + 1 and is taken
+// with weight 1).  Each sum starts from 0 and adds the explicitly rounded
+// products in index order, so every value equals the per-node evaluation
+// bit for bit.  Squares of the residuals w = u - Z land in shared memory at
+// their node index q (z,y,x order over the 279 nodes with an odd
+// coordinate); lane l sums q = l, l+32, ... in order and lane 0 adds the 32
+// partials in lane order.
+constexpr int kWavWarps = 4;
+constexpr int kWavC = 216, kWavX = 252, kWavY = 294;  // 6^3, 36 x 7, 6 x 49
 
-// One warp per (element, variable): lane l sums the squares of the wavelet
-// nodes q = l, l+32, ... (q in z,y,x order), lane 0 adds the 32 partials.
-__global__ void __launch_bounds__(256) wavelet_kernel(ConstVars U, int nvars,
-                                                      const BssnBlockDesc* __restrict__ blocks,
-                                                      const ElemRef* __restrict__ elems,
-                                                      int64_t nelem, double* __restrict__ scores,
-                                                      const uint8_t* __restrict__ need) {
-    const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (wid >= nelem * nvars) return;
-    const int64_t e = wid / nvars;
-    const int v = (int)(wid % nvars);
-    const ElemRef er = elems[e];
-    if (need && !need[er.blk]) return;  // whole warp: same element
-    const BssnBlockDesc b = blocks[er.blk];
-    const int s = b.sz;
-    const double* p = U.p[v] + b.offset + 6 * er.o[0] + (int64_t)s * (6 * er.o[1] + (int64_t)s * 6 * er.o[2]);
+__device__ __forceinline__ double rn_one(double v) { return __dadd_rn(0.0, __dmul_rn(1.0, v)); }
+
+// One (element, variable) item for the calling warp: p points at patch
+// position (0,0,0) of the element, s is the block side, buf the warp's
+// kWavC + kWavX + kWavY doubles of shared memory.  Returns the sum of the
+// squared residuals (the same value in every lane).
+__device__ __forceinline__ double wavelet_item(const double* __restrict__ p, int64_t s,
+                                               const double* __restrict__ sW, double* buf, int lane) {
+    const int64_t s2 = s * s;
+    double* C = buf;
+    double* X = C + kWavC;
+    double* Y = X + kWavX;
+    double* SQ = C;  // reused once C and X are consumed
+    // the element's own nodes this lane needs in the last stage, fetched now
+    // so their latency hides behind the interpolation
+    double uv[11];
+#pragma unroll
+    for (int r = 0; r < 11; r++) {
+        const int t = lane + 32 * r;
+        const int a = t % 7, bb = (t / 7) % 7, c = t / 49;
+        uv[r] = (t < 343 && ((a | bb | c) & 1)) ? __ldg(p + (a + 3) + s * (bb + 3) + s2 * (c + 3)) : 0.0;
+    }
+    for (int t = lane; t < kWavC; t += 32) {
+        const int i = t % 6, j = (t / 6) % 6, k = t / 36;
+        C[t] = __ldg(p + (2 * i + 1) + s * (2 * j + 1) + s2 * (2 * k + 1));
+    }
+    __syncwarp();
+    // x: 36 coarse rows x 3 odd a (interpolated), x 4 even a (taken)
+    for (int t = lane; t < 108; t += 32) {
+        const int row = t / 3, ai = t % 3;
+        const double* c = C + row * 6;
+        const double* w = sW + ai * 6;
+        double acc = 0.0;
+#pragma unroll
+        for (int i = 0; i < 6; i++) acc = __dadd_rn(acc, __dmul_rn(w[i], c[i]));
+        X[row * 7 + 2 * ai + 1] = acc;
+    }
+    for (int t = lane; t < 144; t += 32) {
+        const int row = t / 4, ae = t % 4;
+        X[row * 7 + 2 * ae] = rn_one(C[row * 6 + ae + 1]);
+    }
+    __syncwarp();
+    // y: 6 coarse planes x 3 odd b x 7 a, and x 4 even b x 7 a
+    for (int t = lane; t < 126; t += 32) {
+        const int a = t % 7, bi = (t / 7) % 3, k = t / 21;
+        const double* w = sW + bi * 6;
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < 6; j++) acc = __dadd_rn(acc, __dmul_rn(w[j], X[(k * 6 + j) * 7 + a]));
+        Y[(k * 7 + 2 * bi + 1) * 7 + a] = acc;
+    }
+    for (int t = lane; t < 168; t += 32) {
+        const int a = t % 7, be = (t / 7) % 4, k = t / 28;
+        Y[(k * 7 + 2 * be) * 7 + a] = rn_one(X[(k * 6 + be + 1) * 7 + a]);
+    }
+    __syncwarp();
+    // z and the residuals at the nodes with an odd coordinate
+#pragma unroll
+    for (int r = 0; r < 11; r++) {
+        const int t = lane + 32 * r;
+        const int a = t % 7, bb = (t / 7) % 7, c = t / 49;
+        if (t >= 343 || !((a | bb | c) & 1)) continue;
+        // q = t minus the all-even nodes before t (even counts below a, b, c)
+        const int q = t - (((c + 1) >> 1) * 16 + ((c & 1) ? 0 : ((bb + 1) >> 1) * 4 + ((bb & 1) ? 0 : (a + 1) >> 1)));
+        double z;
+        if (c & 1) {
+            const double* w = sW + (c >> 1) * 6;
+            z = 0.0;
+#pragma unroll
+            for (int k = 0; k < 6; k++) z = __dadd_rn(z, __dmul_rn(w[k], Y[(k * 7 + bb) * 7 + a]));
+        } else {
+            z = rn_one(Y[((c / 2 + 1) * 7 + bb) * 7 + a]);
+        }
+        const double wv = __dsub_rn(uv[r], z);
+        SQ[q] = __dmul_rn(wv, wv);
+    }
+    __syncwarp();
     double part = 0.0;
-    // node q -> (a,b,c): enumerate the 343 element nodes in z,y,x order and
-    // keep those with an odd coordinate; lane l handles every 32nd kept node
-    int q = 0;
-    for (int c = 0; c < 7; c++)
-        for (int bb = 0; bb < 7; bb++)
-            for (int a = 0; a < 7; a++) {
-                if (!((a | bb | c) & 1)) continue;
-                if ((q & 31) == lane) {
-                    const double u = __ldg(p + (a + 3) + (int64_t)s * ((bb + 3) + (int64_t)s * (c + 3)));
-                    const double w = __dsub_rn(u, wavelet_interp(p, s, a, bb, c));
-                    part = __dadd_rn(part, __dmul_rn(w, w));
-                }
-                q++;
-            }
+    for (int q = lane; q < 279; q += 32) part = __dadd_rn(part, SQ[q]);
     double tot = 0.0;
     for (int l = 0; l < 32; l++) tot = __dadd_rn(tot, __shfl_sync(0xffffffffu, part, l));
-    if (lane == 0) scores[e * nvars + v] = __dsqrt_rn(__ddiv_rn(tot, 279.0));
+    return tot;
+}
+
+// Work items are (element, variable) pairs, variable fastest: every element
+// of the mesh (list == nullptr), or the elements listed in list[0, *count)
+// (the blocks a decision sends to the exact test).  Warps stride over the
+// items, so a list launch runs on a grid sized for the GPU.
+__global__ void __launch_bounds__(32 * kWavWarps) wavelet_kernel(ConstVars U, int nvars,
+                                                                 const BssnBlockDesc* __restrict__ blocks,
+                                                                 const ElemRef* __restrict__ elems,
+                                                                 int64_t nelem, const int32_t* __restrict__ list,
+                                                                 const int64_t* __restrict__ count,
+                                                                 double* __restrict__ scores) {
+    __shared__ double sW[18];
+    __shared__ double sbuf[kWavWarps][kWavC + kWavX + kWavY];
+    if (threadIdx.x < 18) sW[threadIdx.x] = kWfine[threadIdx.x / 6][threadIdx.x % 6];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t items = (list ? *count : nelem) * nvars;
+    for (int64_t wid = (int64_t)blockIdx.x * kWavWarps + warp; wid < items;
+         wid += (int64_t)gridDim.x * kWavWarps) {
+        const int64_t e = list ? (int64_t)list[wid / nvars] : wid / nvars;
+        const int v = (int)(wid % nvars);
+        const ElemRef er = elems[e];
+        const BssnBlockDesc b = blocks[er.blk];
+        const int64_t s = b.sz;
+        const double* p = U.p[v] + b.offset + 6 * er.o[0] + s * (6 * er.o[1]) + s * s * (6 * er.o[2]);
+        const double tot = wavelet_item(p, s, sW, sbuf[warp], lane);
+        if (lane == 0) scores[e * nvars + v] = __dsqrt_rn(__ddiv_rn(tot, 279.0));
+        __syncwarp();  // the next item overwrites this warp's buffers
+    }
+}
+
+// Element list of the blocks with need[b] set: one CTA scans the per-block
+// element counts into offsets (off[b]) and the total (*count) ...
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) need_scan_kernel(const uint8_t* __restrict__ need,
+                                                                 const int64_t* __restrict__ first, int nblk,
+                                                                 int64_t* __restrict__ off,
+                                                                 int64_t* __restrict__ count) {
+    __shared__ int64_t wsum[kScanThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int per = (nblk + kScanThreads - 1) / kScanThreads;
+    const int b0 = min(nblk, t * per), b1 = min(nblk, b0 + per);
+    int64_t mine = 0;
+    for (int b = b0; b < b1; b++) mine += need[b] ? first[b + 1] - first[b] : 0;
+    int64_t x = mine;  // inclusive scan over the warp
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int64_t z = wsum[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xffffffffu, z, o);
+            if (lane >= o) z += y;
+        }
+        wsum[lane] = z;
+    }
+    __syncthreads();
+    int64_t run = x - mine + (w > 0 ? wsum[w - 1] : 0);
+    for (int b = b0; b < b1; b++) {
+        off[b] = run;
+        run += need[b] ? first[b + 1] - first[b] : 0;
+    }
+    if (t == kScanThreads - 1) *count = run;
+}
+
+// ... and one warp per listed block writes its element numbers there.
+__global__ void __launch_bounds__(256) need_list_kernel(const uint8_t* __restrict__ need,
+                                                        const int64_t* __restrict__ first, int nblk,
+                                                        const int64_t* __restrict__ off,
+                                                        int32_t* __restrict__ list) {
+    const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (b >= nblk || !need[b]) return;
+    const int64_t n = first[b + 1] - first[b];
+    for (int64_t i = lane; i < n; i += 32) list[off[b] + i] = (int32_t)(first[b] + i);
 }
 
 // Per block: the largest score over its elements and variables divided by
-// the tolerance, and the refine flag (ratio > 1).
+// the tolerance, and the refine flag (ratio > 1).  One warp per block; the
+// maximum does not depend on the order its lanes take.
 __global__ void __launch_bounds__(256) block_flags_kernel(const double* __restrict__ scores, int nvars,
                                                           const int64_t* __restrict__ first,
                                                           int nblk, double tol, double* ratio,
                                                           uint8_t* flags, const uint8_t* need) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nblk || (need && !need[b])) return;
+    const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (b >= nblk || (need && !need[b])) return;  // whole warp
     double m = 0.0;
-    for (int64_t e = first[b]; e < first[b + 1]; e++)
-        for (int v = 0; v < nvars; v++) m = fmax(m, scores[e * nvars + v]);
-    const double r = m / tol;
-    if (ratio) ratio[b] = r;
-    if (flags) flags[b] = r > 1.0 ? 1 : 0;
+    const int64_t lo = first[b] * nvars, hi = first[b + 1] * nvars;
+    for (int64_t q = lo + lane; q < hi; q += 32) m = fmax(m, scores[q]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) {
+        const double r = m / tol;
+        if (ratio) ratio[b] = r;
+        if (flags) flags[b] = r > 1.0 ? 1 : 0;
+    }
 }
 
-// Block features (16 floats), one CTA per block.
-__global__ void __launch_bounds__(256) features_kernel(ConstVars U, const BssnBlockDesc* __restrict__ blocks,
-                                                       float* __restrict__ feats) {
-    const BssnBlockDesc b = blocks[blockIdx.x];
-    const int s = b.sz, N = s - 6;
-    const int64_t st[3] = {1, s, (int64_t)s * s};
+// Block features (16 floats) from chi, alpha, K and Gt^i on the even
+// sublattice of each block's interior (every second point along each axis),
+// with differences over two points: max |d chi| and |d alpha| per axis, max
+// |K|, max |Gt^i|, the largest second differences of chi and alpha, the
+// smallest chi; plus level, block side and spacing.  The sublattice touches
+// a quarter of the rows of six of the 24 variables, a small fraction of what
+// the exact test reads.  The maxima and the minimum are taken over runs of
+// kFeatChunk sublattice points, one warp per run (a 13^3 block is one run of
+// 64, a 55^3 block 62 runs), then per block over its runs; neither depends
+// on the order.
+constexpr int kFeatChunk = 256;
+
+__host__ __device__ inline int64_t feature_points(int sz) {
+    const int64_t n = (sz - 6 + 1) / 2;
+    return n * n * n;
+}
+
+__global__ void __launch_bounds__(256) features_partial_kernel(ConstVars U,
+                                                               const BssnBlockDesc* __restrict__ blocks,
+                                                               const Chunk* __restrict__ chunks, int nchunks,
+                                                               double* __restrict__ part) {
+    const int ci = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (ci >= nchunks) return;  // whole warp
+    const Chunk ch = chunks[ci];
+    const BssnBlockDesc b = blocks[ch.blk];
+    const int s = b.sz, n = (s - 6 + 1) / 2;
+    const int64_t st[3] = {2, 2 * s, 2 * (int64_t)s * s};
+    const double* chi = U.p[U_CHI];
+    const double* al = U.p[U_ALPHA];
     double mx[15];
     for (int f = 0; f < 15; f++) mx[f] = 0.0;
     double chimin = 1e300;
-    const int64_t n = (int64_t)N * N * N;
-    for (int64_t q = threadIdx.x; q < n; q += blockDim.x) {
-        const int i = 3 + (int)(q % N), j = 3 + (int)((q / N) % N), k = 3 + (int)(q / ((int64_t)N * N));
+    for (int64_t q = ch.start + lane; q < ch.start + ch.count; q += 32) {
+        const int i = 3 + 2 * (int)(q % n), j = 3 + 2 * (int)((q / n) % n), k = 3 + 2 * (int)(q / ((int64_t)n * n));
         const int64_t p = b.offset + i + s * (j + (int64_t)s * k);
-        const double* chi = U.p[U_CHI];
-        const double* al = U.p[U_ALPHA];
-        const double c0 = chi[p];
+        const double c0 = chi[p], a0 = al[p];
         for (int d = 0; d < 3; d++) {
             const double cp = chi[p + st[d]], cm = chi[p - st[d]];
-            mx[d] = fmax(mx[d], fabs(__dmul_rn(__dsub_rn(cp, cm), 0.5)));
-            mx[3 + d] = fmax(mx[3 + d], fabs(__dmul_rn(__dsub_rn(al[p + st[d]], al[p - st[d]]), 0.5)));
+            const double ap = al[p + st[d]], am = al[p - st[d]];
+            mx[d] = fmax(mx[d], fabs(__dmul_rn(__dsub_rn(cp, cm), 0.25)));
+            mx[3 + d] = fmax(mx[3 + d], fabs(__dmul_rn(__dsub_rn(ap, am), 0.25)));
             mx[7 + d] = fmax(mx[7 + d], fabs(U.p[U_GT0 + d][p]));
             mx[13] = fmax(mx[13], fabs(__dsub_rn(__dsub_rn(cp, c0), __dsub_rn(c0, cm))));
+            mx[14] = fmax(mx[14], fabs(__dsub_rn(__dsub_rn(ap, a0), __dsub_rn(a0, am))));
         }
         mx[6] = fmax(mx[6], fabs(U.p[U_K][p]));
-        for (int c = 0; c < 6; c++) mx[14] = fmax(mx[14], fabs(U.p[U_SYMAT0 + c][p]));
         chimin = fmin(chimin, c0);
     }
-    __shared__ double red[256][16];
-    for (int f = 0; f < 15; f++) red[threadIdx.x][f] = mx[f];
-    red[threadIdx.x][15] = chimin;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) {
-            for (int f = 0; f < 15; f++) red[threadIdx.x][f] = fmax(red[threadIdx.x][f], red[threadIdx.x + w][f]);
-            red[threadIdx.x][15] = fmin(red[threadIdx.x][15], red[threadIdx.x + w][15]);
-        }
-        __syncthreads();
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int f = 0; f < 15; f++) mx[f] = fmax(mx[f], __shfl_xor_sync(0xffffffffu, mx[f], o));
+        chimin = fmin(chimin, __shfl_xor_sync(0xffffffffu, chimin, o));
     }
-    if (threadIdx.x == 0) {
-        float* f = feats + (int64_t)blockIdx.x * 16;
-        for (int q = 0; q < 10; q++) f[q] = (float)log10(red[0][q] + 1e-30);
+    // lane f < 15 writes maximum f, lane 15 the minimum (static indices only)
+    double mine = chimin;
+#pragma unroll
+    for (int f = 0; f < 15; f++)
+        if (lane == f) mine = mx[f];
+    if (lane < 16) part[(int64_t)ci * 16 + lane] = mine;
+}
+
+// One warp per block: reduce the block's runs, then the 16 features.
+__global__ void __launch_bounds__(256) features_final_kernel(const BssnBlockDesc* __restrict__ blocks,
+                                                             const double* __restrict__ part,
+                                                             const int64_t* __restrict__ first, int nblk,
+                                                             float* __restrict__ feats) {
+    const int bi = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (bi >= nblk) return;
+    double r[16];
+    for (int f = 0; f < 15; f++) r[f] = 0.0;
+    r[15] = 1e300;
+    for (int64_t c = first[bi] + lane; c < first[bi + 1]; c += 32) {
+        for (int f = 0; f < 15; f++) r[f] = fmax(r[f], part[c * 16 + f]);
+        r[15] = fmin(r[15], part[c * 16 + 15]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int f = 0; f < 15; f++) r[f] = fmax(r[f], __shfl_xor_sync(0xffffffffu, r[f], o));
+        r[15] = fmin(r[15], __shfl_xor_sync(0xffffffffu, r[15], o));
+    }
+    if (lane == 0) {
+        const BssnBlockDesc b = blocks[bi];
+        const int s = b.sz;
+        float* f = feats + (int64_t)bi * 16;
+        for (int q = 0; q < 10; q++) f[q] = (float)log10(r[q] + 1e-30);
         const double h = (b.ptmax[0] - b.ptmin[0]) / (s - 1);
         f[10] = (float)b.level;
         f[11] = (float)(s / 55.0);
-        f[12] = (float)log10(red[0][15]);
-        f[13] = (float)log10(red[0][13] + 1e-30);
-        f[14] = (float)log10(red[0][14] + 1e-30);
+        f[12] = (float)log10(r[15]);
+        f[13] = (float)log10(r[13] + 1e-30);
+        f[14] = (float)log10(r[14] + 1e-30);
         f[15] = (float)log10(h);
     }
 }
@@ -586,6 +743,10 @@ int remesh_elements(MeshState* m) {
     }
     if (cudaMalloc((void**)&m->d_elems, e.size() * sizeof(ElemRef)) != cudaSuccess) return BSSN_ENOMEM;
     if (cudaMalloc((void**)&m->d_elem_first, first.size() * sizeof(int64_t)) != cudaSuccess) return BSSN_ENOMEM;
+    if (cudaMalloc((void**)&m->d_need_off, (first.size() + 1) * sizeof(int64_t)) != cudaSuccess) return BSSN_ENOMEM;
+    if (cudaMalloc((void**)&m->d_need_list, std::max<size_t>(e.size(), 1) * sizeof(int32_t)) != cudaSuccess)
+        return BSSN_ENOMEM;
+    m->d_need_count = m->d_need_off + first.size();
     cudaMemcpy(m->d_elems, e.data(), e.size() * sizeof(ElemRef), cudaMemcpyHostToDevice);
     cudaMemcpy(m->d_elem_first, first.data(), first.size() * sizeof(int64_t), cudaMemcpyHostToDevice);
     m->n_elems = (int64_t)e.size();
@@ -599,8 +760,23 @@ int launch_wavelet_scores(MeshState* m, const double* const* U, int nvars, doubl
     ConstVars u = {};
     for (int v = 0; v < nvars; v++) u.p[v] = U[v];
     const int64_t warps = m->n_elems * nvars;
-    const int64_t blocks = (warps * 32 + 255) / 256;
-    wavelet_kernel<<<(unsigned)blocks, 256, 0, s>>>(u, nvars, m->d_blocks, m->d_elems, m->n_elems, scores, need);
+    const int nb = (int)m->blocks.size();
+    if (warps == 0) return 0;
+    int64_t blocks = (warps + kWavWarps - 1) / kWavWarps;
+    if (!need) {
+        wavelet_kernel<<<(unsigned)blocks, 32 * kWavWarps, 0, s>>>(u, nvars, m->d_blocks, m->d_elems, m->n_elems,
+                                                                  nullptr, nullptr, scores);
+        return cuda_status(cudaGetLastError());
+    }
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    blocks = std::min<int64_t>(blocks, (int64_t)nsm * 8);
+    need_scan_kernel<<<1, kScanThreads, 0, s>>>(need, m->d_elem_first, nb, m->d_need_off, m->d_need_count);
+    need_list_kernel<<<(unsigned)(((int64_t)nb * 32 + 255) / 256), 256, 0, s>>>(need, m->d_elem_first, nb,
+                                                                              m->d_need_off, m->d_need_list);
+    wavelet_kernel<<<(unsigned)blocks, 32 * kWavWarps, 0, s>>>(u, nvars, m->d_blocks, m->d_elems, m->n_elems,
+                                                              m->d_need_list, m->d_need_count, scores);
     return cuda_status(cudaGetLastError());
 }
 
@@ -609,14 +785,42 @@ int launch_block_flags(MeshState* m, const double* scores, int nvars, double tol
     int st = remesh_elements(m);
     if (st) return st;
     const int nb = (int)m->blocks.size();
-    block_flags_kernel<<<(nb + 255) / 256, 256, 0, s>>>(scores, nvars, m->d_elem_first, nb, tol, ratio, flags, need);
+    block_flags_kernel<<<(unsigned)(((int64_t)nb * 32 + 255) / 256), 256, 0, s>>>(scores, nvars, m->d_elem_first, nb, tol,
+                                                                          ratio, flags, need);
     return cuda_status(cudaGetLastError());
 }
 
-int launch_features(const MeshState* m, const double* const* U, float* feats, cudaStream_t s) {
+int feature_chunks(MeshState* m) {
+    if (m->d_fchunks) return 0;
+    std::vector<Chunk> c;
+    std::vector<int64_t> first(m->blocks.size() + 1, 0);
+    for (size_t b = 0; b < m->blocks.size(); b++) {
+        const int64_t n = feature_points(m->blocks[b].sz);
+        for (int64_t q = 0; q < n; q += kFeatChunk)
+            c.push_back(Chunk{(int32_t)b, (int32_t)std::min<int64_t>(kFeatChunk, n - q), q});
+        first[b + 1] = (int64_t)c.size();
+    }
+    if (cudaMalloc((void**)&m->d_fchunks, c.size() * sizeof(Chunk)) != cudaSuccess) return BSSN_ENOMEM;
+    if (cudaMalloc((void**)&m->d_fchunk_first, first.size() * sizeof(int64_t)) != cudaSuccess)
+        return BSSN_ENOMEM;
+    if (cudaMalloc((void**)&m->d_fpart, c.size() * 16 * sizeof(double)) != cudaSuccess) return BSSN_ENOMEM;
+    cudaMemcpy(m->d_fchunks, c.data(), c.size() * sizeof(Chunk), cudaMemcpyHostToDevice);
+    cudaMemcpy(m->d_fchunk_first, first.data(), first.size() * sizeof(int64_t), cudaMemcpyHostToDevice);
+    m->n_fchunks = (int)c.size();
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_features(MeshState* m, const double* const* U, float* feats, cudaStream_t s) {
+    const int nb = (int)m->blocks.size();
+    if (nb == 0) return 0;
+    int st = feature_chunks(m);
+    if (st) return st;
     ConstVars u = {};
     for (int v = 0; v < NVARS; v++) u.p[v] = U[v];
-    features_kernel<<<(unsigned)m->blocks.size(), 256, 0, s>>>(u, m->d_blocks, feats);
+    features_partial_kernel<<<(unsigned)(((int64_t)m->n_fchunks * 32 + 255) / 256), 256, 0, s>>>(
+        u, m->d_blocks, m->d_fchunks, m->n_fchunks, m->d_fpart);
+    features_final_kernel<<<(unsigned)(((int64_t)nb * 32 + 255) / 256), 256, 0, s>>>(
+        m->d_blocks, m->d_fpart, m->d_fchunk_first, nb, feats);
     return cuda_status(cudaGetLastError());
 }
 

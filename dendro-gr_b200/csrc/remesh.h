@@ -22,7 +22,7 @@ int launch_wavelet_scores(MeshState* m, const double* const* U, int nvars, doubl
                           const uint8_t* need, cudaStream_t s);
 int launch_block_flags(MeshState* m, const double* scores, int nvars, double tol, double* ratio,
                        uint8_t* flags, const uint8_t* need, cudaStream_t s);
-int launch_features(const MeshState* m, const double* const* U, float* feats, cudaStream_t s);
+int launch_features(MeshState* m, const double* const* U, float* feats, cudaStream_t s);
 // tensor-core forward (BF16 operands, FP32 accumulation); the decisions use it
 int launch_mlp_fwd(const void* wq, const float* norm, const float* X, int n, float* logits,
                    cudaStream_t s);

@@ -250,10 +250,12 @@ int bssn_remesh_wavelet_f64(bssn_mesh mesh, const double* const* unzip_dev,
                             int nvars, double tol, double* scores_dev,
                             double* ratio_dev, uint8_t* flags_dev,
                             bssn_stream_t stream);
-/* 16 cheap features per block (floats): log10 of max |centred difference|
- * of chi (x,y,z), of alpha (x,y,z), max |K|, max |Gt^i| (3), level, side/55,
- * log10 min chi, log10 max |second difference of chi|, log10 max |At_ij|,
- * log10 h. */
+/* 16 cheap features per block (floats), taken on the even sublattice of the
+ * interior (every second point per axis, differences over two points, so
+ * a quarter of the rows of chi, alpha, K and Gt^i are read): log10 of max
+ * |centred difference| of chi (x,y,z), of alpha (x,y,z), max |K|, max |Gt^i|
+ * (3), level, side/55, log10 min chi, log10 max |second difference| of chi
+ * and of alpha, log10 h. */
 int bssn_remesh_features_f64(bssn_mesh mesh, const double* const* unzip_dev,
                              float* feats_dev, bssn_stream_t stream);
 /* The indicator network: 16 -> 64 -> 64 -> 1 with GELU, parameters

@@ -1389,26 +1389,30 @@ extern "C" void orc_block_features(const double** unzip, const OrcBlock* blks, i
                                    float* feats) {
 #pragma omp parallel for schedule(dynamic, 1)
     for (int b = 0; b < nblk; b++) {
+        // even sublattice of the interior, differences over two points
         const int s = blks[b].sz;
-        const int64_t st[3] = {1, s, (int64_t)s * s};
+        const int64_t st[3] = {2, 2 * s, 2 * (int64_t)s * s};
+        const double* chi = unzip[U_CHI];
+        const double* al = unzip[U_ALPHA];
         double mx[16];
         for (int f = 0; f < 16; f++) mx[f] = 0.0;
         double chimin = 1e300;
-        for (int k = 3; k < s - 3; k++)
-            for (int j = 3; j < s - 3; j++)
-                for (int i = 3; i < s - 3; i++) {
+        for (int k = 3; k < s - 3; k += 2)
+            for (int j = 3; j < s - 3; j += 2)
+                for (int i = 3; i < s - 3; i += 2) {
                     const int64_t p = blks[b].offset + i + s * (j + (int64_t)s * k);
-                    const double* chi = unzip[U_CHI];
-                    const double* al = unzip[U_ALPHA];
+                    const double c0 = chi[p], a0 = al[p];
                     for (int d = 0; d < 3; d++) {
-                        mx[d] = std::max(mx[d], fabs((chi[p + st[d]] - chi[p - st[d]]) * 0.5));
-                        mx[3 + d] = std::max(mx[3 + d], fabs((al[p + st[d]] - al[p - st[d]]) * 0.5));
+                        const double cp = chi[p + st[d]], cm = chi[p - st[d]];
+                        const double ap = al[p + st[d]], am = al[p - st[d]];
+                        mx[d] = std::max(mx[d], fabs((cp - cm) * 0.25));
+                        mx[3 + d] = std::max(mx[3 + d], fabs((ap - am) * 0.25));
                         mx[7 + d] = std::max(mx[7 + d], fabs(unzip[U_GT0 + d][p]));
-                        mx[13] = std::max(mx[13], fabs((chi[p + st[d]] - chi[p]) - (chi[p] - chi[p - st[d]])));
+                        mx[13] = std::max(mx[13], fabs((cp - c0) - (c0 - cm)));
+                        mx[14] = std::max(mx[14], fabs((ap - a0) - (a0 - am)));
                     }
                     mx[6] = std::max(mx[6], fabs(unzip[U_K][p]));
-                    for (int c = 0; c < 6; c++) mx[14] = std::max(mx[14], fabs(unzip[U_SYMAT0 + c][p]));
-                    chimin = std::min(chimin, chi[p]);
+                    chimin = std::min(chimin, c0);
                 }
         const double h = (blks[b].ptmax[0] - blks[b].ptmin[0]) / (s - 1);
         float* f = feats + (int64_t)b * 16;

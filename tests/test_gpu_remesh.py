@@ -202,6 +202,33 @@ def test_decide2_matches_exact_where_it_defers(B, state):
     assert st[4] == int(exact.sum()) and st[6] == int((ratio > 0.1).sum())
 
 
+def test_decide2_partial_list_matches_exact(B, state):
+    """The exact test on part of the mesh (the compacted element list of the
+    deferred blocks): refine network unsure of every block, keep network
+    sure (lo = hi = 0.5), so only the blocks the keep network would keep
+    (p > 0.5) are deferred for refine; there the refine flag equals the
+    exact test's, and elsewhere it is 0 or (audited blocks) the exact flag."""
+    spec, m, Pz = state
+    nr, nk = B.RemeshMLP(seed=5), B.RemeshMLP(seed=8)
+    nr.lo, nr.hi, nk.lo, nk.hi = 0.0, 1.0, 0.5, 0.5
+    f = B.block_features(m, Pz)
+    nk.set_norm(f)
+    # output bias at minus the median logit: about half the blocks deferred
+    nk.master[B.MLP_NPARAM - 1] -= float(nk.logits(f).median())
+    nk.wq = nk.master.to(torch.bfloat16)
+    lk = nk.logits(f).cpu().numpy()
+    refine, keep, stats = B.remesh_decide2(m, Pz, nr, nk, tol=1e-6, keep_fac=0.1, audit_frac=0.05)
+    _, ratio, exact = B.wavelet_scores(m, Pz, tol=1e-6)
+    torch.cuda.synchronize()
+    r, e = refine.cpu().numpy(), exact.cpu().numpy()
+    deferred = lk > 1e-3
+    sure_no = lk < -1e-3
+    assert 0 < deferred.sum() < spec.nblocks
+    assert np.array_equal(r[deferred], e[deferred])
+    assert np.all(r[sure_no] <= e[sure_no])
+    assert stats.cpu().tolist()[0] == int((lk > 0).sum())
+
+
 def test_trained_indicator_meets_the_contract(B):
     """Train on labels from small mixed-mesh runs; set the thresholds on a
     validation split with a margin of one logit unit; evaluate on blocks of
