@@ -130,8 +130,7 @@ TileEntry make_onchip_tile(int shape) {
 // (13x5x5 and 9x9x5 fit the 25-zone interiors of 31^3 blocks with few idle
 // threads); 10..13: on chip (128-zone bricks, every extent >= 3 for every
 // block side, as the one-sided closures need; 10, 11 at two CTAs per SM,
-// 12, 13 the same shapes at three); 14, 15: tiles 8, 9 with the
-// derivative pass's stencils interleaved tap by tap
+// 12, 13 the same shapes at three)
 // (rhs_split.cu's shape order).  `fused` is the tile a single-block launch
 // of the shape runs (the nearest fused shape for split-only ones).
 const TileEntry* tile_table(int* count) {
@@ -150,8 +149,6 @@ const TileEntry* tile_table(int* count) {
         make_onchip_tile<7, 4, 4>(1),
         make_onchip_tile<5, 5, 5>(2),
         make_onchip_tile<7, 4, 4>(3),
-        make_split_tile<13, 5, 5>(7, 1),
-        make_split_tile<9, 9, 5>(8, 1),
     };
     *count = (int)(sizeof(table) / sizeof(table[0]));
     return table;

@@ -86,10 +86,7 @@ __device__ __forceinline__ bool owns_node(const BssnBlockDesc& blk, const int o[
 }
 
 // ZIP: stage from the zipped node grid (g) instead of the padded blocks.
-// IL: the interior stencils advanced one tap at a time across the nine
-// chains (zone_dirs_il) instead of chain by chain; the results are the same
-// bit for bit, only the instruction order differs.
-template <int BX, int BY, int BZ, bool ZIP, bool IL>
+template <int BX, int BY, int BZ, bool ZIP>
 __global__ void __launch_bounds__(Brick<BX, BY, BZ>::THREADS,
                                    deriv_min_ctas(Brick<BX, BY, BZ>::THREADS))
 deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
@@ -136,10 +133,7 @@ deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
             cp_async_commit();
         if (stage_second(step)) {
             Dir3 r[3];
-            if (IL)
-                zone_dirs_il<true, Bk>(bz.zc, cur, r);
-            else
-                zone_dirs<true, Bk>(bz.zc, cur, r);
+            zone_dirs<true, Bk>(bz.zc, cur, r);
             // the brick part of the mixed scratch from the zones' own gradient
             if (th.active) {
                 mx[bz.mxj_off] = r[0].d1;  // the offsets include the halo
@@ -171,10 +165,7 @@ deriv_kernel(ConstVars u, const BssnBlockDesc* __restrict__ blocks,
             }
         } else {
             Dir3 r[3];
-            if (IL)
-                zone_dirs_il<false, Bk>(bz.zc, cur, r);
-            else
-                zone_dirs<false, Bk>(bz.zc, cur, r);
+            zone_dirs<false, Bk>(bz.zc, cur, r);
             if (keep) {
                 const double v[kSlotsFirst] = {r[0].d1, r[1].d1, r[2].d1,
                                                r[0].ko + r[1].ko + r[2].ko};
@@ -289,17 +280,16 @@ struct SplitEntry {
     void (*eq)(RhsArgs, const BssnBlockDesc*, const BrickTask*, const double*, int64_t, ZipGrid, int);
 };
 
-template <int BX, int BY, int BZ, bool IL = false>
+template <int BX, int BY, int BZ>
 SplitEntry make_split() {
     using Bk = Brick<BX, BY, BZ>;
     return SplitEntry{Bk::NZ, Bk::THREADS, deriv_smem_bytes<Bk>(),
-                      deriv_kernel<BX, BY, BZ, false, IL>, deriv_kernel<BX, BY, BZ, true, IL>,
+                      deriv_kernel<BX, BY, BZ, false>, deriv_kernel<BX, BY, BZ, true>,
                       eq_kernel<BX, BY, BZ>};
 }
 
 // the fused tiles' shapes in their order, then split-only shapes (bricks too
-// large for the fused kernel's 255 registers per zone), then the two
-// split-only shapes with the tap-interleaved stencils
+// large for the fused kernel's 255 registers per zone)
 const SplitEntry* split_table(int* count) {
     static const SplitEntry table[] = {
         make_split<8, 8, 4>(),
@@ -309,8 +299,6 @@ const SplitEntry* split_table(int* count) {
         make_split<8, 8, 8>(),
         make_split<13, 5, 5>(),
         make_split<9, 9, 5>(),
-        make_split<13, 5, 5, true>(),
-        make_split<9, 9, 5, true>(),
     };
     *count = (int)(sizeof(table) / sizeof(table[0]));
     return table;
