@@ -54,25 +54,55 @@ constexpr int kWavC = 216, kWavX = 252, kWavY = 294;  // 6^3, 36 x 7, 6 x 49
 
 __device__ __forceinline__ double rn_one(double v) { return __dadd_rn(0.0, __dmul_rn(1.0, v)); }
 
+// Lane roles: a lane l < 30 always evaluates with the weight row l % 3 (its
+// six weights stay in registers for the whole kernel) on the items
+// g = l / 3, g + 10, ...; every lane shares the trivial copies (even index).
+// The mapping only moves work between lanes: each value is still formed by
+// the same rounded products and sums in the same order.
+struct WavLane {
+    double w[6];
+    int rho, g;
+    bool interp;
+};
+
+// node index q of (a, b, c) among the 279 nodes with an odd coordinate (z,y,x
+// order): t = a + 7b + 49c minus the all-even nodes before it
+__device__ __forceinline__ int wav_q(int a, int b, int c) {
+    const int t = a + 7 * b + 49 * c;
+    return t - (((c + 1) >> 1) * 16 + ((c & 1) ? 0 : ((b + 1) >> 1) * 4 + ((b & 1) ? 0 : (a + 1) >> 1)));
+}
+
 // One (element, variable) item for the calling warp: p points at patch
 // position (0,0,0) of the element, s is the block side, buf the warp's
-// kWavC + kWavX + kWavY doubles of shared memory.  Returns the sum of the
+// kWavC + kWavX + kWavY doubles of shared memory, pairs the 33 (b, a) pairs
+// with an odd coordinate (b * 7 + a, b-major).  Returns the sum of the
 // squared residuals (the same value in every lane).
-__device__ __forceinline__ double wavelet_item(const double* __restrict__ p, int64_t s,
-                                               const double* __restrict__ sW, double* buf, int lane) {
+__device__ __forceinline__ double wavelet_item(const double* __restrict__ p, int64_t s, const WavLane& L,
+                                               const uint8_t* __restrict__ pairs, double* buf, int lane) {
     const int64_t s2 = s * s;
     double* C = buf;
     double* X = C + kWavC;
     double* Y = X + kWavX;
     double* SQ = C;  // reused once C and X are consumed
     // the element's own nodes this lane needs in the last stage, fetched now
-    // so their latency hides behind the interpolation
-    double uv[11];
+    // so their latency hides behind the interpolation: odd c (its role's
+    // c = 2 rho + 1, pairs g + 10 j) and even c (nodes lane + 32 r)
+    double uo[5], ue[5];
 #pragma unroll
-    for (int r = 0; r < 11; r++) {
+    for (int j = 0; j < 5; j++) {
+        const int pr = L.g + 10 * j;
+        uo[j] = (L.interp && pr < 49)
+                    ? __ldg(p + (pr % 7 + 3) + s * (pr / 7 + 3) + s2 * (2 * L.rho + 4)) : 0.0;
+    }
+#pragma unroll
+    for (int r = 0; r < 5; r++) {
         const int t = lane + 32 * r;
-        const int a = t % 7, bb = (t / 7) % 7, c = t / 49;
-        uv[r] = (t < 343 && ((a | bb | c) & 1)) ? __ldg(p + (a + 3) + s * (bb + 3) + s2 * (c + 3)) : 0.0;
+        if (t < 132) {
+            const int ba = pairs[t % 33], ce = t / 33;
+            ue[r] = __ldg(p + (ba % 7 + 3) + s * (ba / 7 + 3) + s2 * (2 * ce + 3));
+        } else {
+            ue[r] = 0.0;
+        }
     }
     for (int t = lane; t < kWavC; t += 32) {
         const int i = t % 6, j = (t / 6) % 6, k = t / 36;
@@ -80,53 +110,65 @@ __device__ __forceinline__ double wavelet_item(const double* __restrict__ p, int
     }
     __syncwarp();
     // x: 36 coarse rows x 3 odd a (interpolated), x 4 even a (taken)
-    for (int t = lane; t < 108; t += 32) {
-        const int row = t / 3, ai = t % 3;
-        const double* c = C + row * 6;
-        const double* w = sW + ai * 6;
-        double acc = 0.0;
+    if (L.interp) {
 #pragma unroll
-        for (int i = 0; i < 6; i++) acc = __dadd_rn(acc, __dmul_rn(w[i], c[i]));
-        X[row * 7 + 2 * ai + 1] = acc;
+        for (int k = 0; k < 4; k++) {
+            const int m = L.g + 10 * k;
+            if (m < 36) {
+                const double* c = C + m * 6;
+                double acc = 0.0;
+#pragma unroll
+                for (int i = 0; i < 6; i++) acc = __dadd_rn(acc, __dmul_rn(L.w[i], c[i]));
+                X[m * 7 + 2 * L.rho + 1] = acc;
+            }
+        }
     }
-    for (int t = lane; t < 144; t += 32) {
-        const int row = t / 4, ae = t % 4;
-        X[row * 7 + 2 * ae] = rn_one(C[row * 6 + ae + 1]);
-    }
+    for (int t = lane; t < 144; t += 32) X[(t >> 2) * 7 + 2 * (t & 3)] = rn_one(C[(t >> 2) * 6 + (t & 3) + 1]);
     __syncwarp();
     // y: 6 coarse planes x 3 odd b x 7 a, and x 4 even b x 7 a
-    for (int t = lane; t < 126; t += 32) {
-        const int a = t % 7, bi = (t / 7) % 3, k = t / 21;
-        const double* w = sW + bi * 6;
-        double acc = 0.0;
+    if (L.interp) {
 #pragma unroll
-        for (int j = 0; j < 6; j++) acc = __dadd_rn(acc, __dmul_rn(w[j], X[(k * 6 + j) * 7 + a]));
-        Y[(k * 7 + 2 * bi + 1) * 7 + a] = acc;
+        for (int j = 0; j < 5; j++) {
+            const int pr = L.g + 10 * j;
+            if (pr < 42) {
+                const int k = pr / 7, a = pr % 7;
+                double acc = 0.0;
+#pragma unroll
+                for (int jj = 0; jj < 6; jj++) acc = __dadd_rn(acc, __dmul_rn(L.w[jj], X[(k * 6 + jj) * 7 + a]));
+                Y[(k * 7 + 2 * L.rho + 1) * 7 + a] = acc;
+            }
+        }
     }
     for (int t = lane; t < 168; t += 32) {
         const int a = t % 7, be = (t / 7) % 4, k = t / 28;
         Y[(k * 7 + 2 * be) * 7 + a] = rn_one(X[(k * 6 + be + 1) * 7 + a]);
     }
     __syncwarp();
-    // z and the residuals at the nodes with an odd coordinate
+    // z and the residuals: odd c by role, then even c with an odd a or b
+    if (L.interp) {
+        const int c = 2 * L.rho + 1;
 #pragma unroll
-    for (int r = 0; r < 11; r++) {
-        const int t = lane + 32 * r;
-        const int a = t % 7, bb = (t / 7) % 7, c = t / 49;
-        if (t >= 343 || !((a | bb | c) & 1)) continue;
-        // q = t minus the all-even nodes before t (even counts below a, b, c)
-        const int q = t - (((c + 1) >> 1) * 16 + ((c & 1) ? 0 : ((bb + 1) >> 1) * 4 + ((bb & 1) ? 0 : (a + 1) >> 1)));
-        double z;
-        if (c & 1) {
-            const double* w = sW + (c >> 1) * 6;
-            z = 0.0;
+        for (int j = 0; j < 5; j++) {
+            const int pr = L.g + 10 * j;
+            if (pr < 49) {
+                const int bb = pr / 7, a = pr % 7;
+                double z = 0.0;
 #pragma unroll
-            for (int k = 0; k < 6; k++) z = __dadd_rn(z, __dmul_rn(w[k], Y[(k * 7 + bb) * 7 + a]));
-        } else {
-            z = rn_one(Y[((c / 2 + 1) * 7 + bb) * 7 + a]);
+                for (int k = 0; k < 6; k++) z = __dadd_rn(z, __dmul_rn(L.w[k], Y[(k * 7 + bb) * 7 + a]));
+                const double wv = __dsub_rn(uo[j], z);
+                SQ[wav_q(a, bb, c)] = __dmul_rn(wv, wv);
+            }
         }
-        const double wv = __dsub_rn(uv[r], z);
-        SQ[q] = __dmul_rn(wv, wv);
+    }
+#pragma unroll
+    for (int r = 0; r < 5; r++) {
+        const int t = lane + 32 * r;
+        if (t < 132) {
+            const int ba = pairs[t % 33], ce = t / 33;
+            const int bb = ba / 7, a = ba % 7;
+            const double wv = __dsub_rn(ue[r], rn_one(Y[((ce + 1) * 7 + bb) * 7 + a]));
+            SQ[wav_q(a, bb, 2 * ce)] = __dmul_rn(wv, wv);
+        }
     }
     __syncwarp();
     double part = 0.0;
@@ -146,11 +188,25 @@ __global__ void __launch_bounds__(32 * kWavWarps) wavelet_kernel(ConstVars U, in
                                                                  int64_t nelem, const int32_t* __restrict__ list,
                                                                  const int64_t* __restrict__ count,
                                                                  double* __restrict__ scores) {
-    __shared__ double sW[18];
     __shared__ double sbuf[kWavWarps][kWavC + kWavX + kWavY];
-    if (threadIdx.x < 18) sW[threadIdx.x] = kWfine[threadIdx.x / 6][threadIdx.x % 6];
+    __shared__ uint8_t spairs[33];
+    if (threadIdx.x < 49) {
+        // b-major list of the (b, a) pairs with an odd coordinate
+        const int b = threadIdx.x / 7, a = threadIdx.x % 7;
+        if ((a | b) & 1) {
+            int k = 0;
+            for (int x = 0; x < (int)threadIdx.x; x++) k += ((x % 7) | (x / 7)) & 1;
+            spairs[k] = (uint8_t)threadIdx.x;
+        }
+    }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WavLane L;
+    L.interp = lane < 30;
+    L.rho = lane % 3;
+    L.g = lane / 3;
+#pragma unroll
+    for (int i = 0; i < 6; i++) L.w[i] = kWfine[L.rho][i];
     const int64_t items = (list ? *count : nelem) * nvars;
     for (int64_t wid = (int64_t)blockIdx.x * kWavWarps + warp; wid < items;
          wid += (int64_t)gridDim.x * kWavWarps) {
@@ -160,7 +216,7 @@ __global__ void __launch_bounds__(32 * kWavWarps) wavelet_kernel(ConstVars U, in
         const BssnBlockDesc b = blocks[er.blk];
         const int64_t s = b.sz;
         const double* p = U.p[v] + b.offset + 6 * er.o[0] + s * (6 * er.o[1]) + s * s * (6 * er.o[2]);
-        const double tot = wavelet_item(p, s, sW, sbuf[warp], lane);
+        const double tot = wavelet_item(p, s, L, spairs, sbuf[warp], lane);
         if (lane == 0) scores[e * nvars + v] = __dsqrt_rn(__ddiv_rn(tot, 279.0));
         __syncwarp();  // the next item overwrites this warp's buffers
     }

@@ -229,6 +229,29 @@ def test_decide2_partial_list_matches_exact(B, state):
     assert stats.cpu().tolist()[0] == int((lk > 0).sum())
 
 
+def test_decide2_nothing_deferred(B, state):
+    """Both networks sure of every block (lo = hi = 0.5) and no audit: the
+    exact test's element list is empty, and the flags are the networks'
+    decisions with the refine-implies-keep rule."""
+    spec, m, Pz = state
+    nr, nk = B.RemeshMLP(seed=5), B.RemeshMLP(seed=8)
+    f = B.block_features(m, Pz)
+    nr.set_norm(f)
+    nk.set_norm(f)
+    nr.lo = nr.hi = nk.lo = nk.hi = 0.5
+    refine, keep, stats = B.remesh_decide2(m, Pz, nr, nk, tol=1e-6, keep_fac=0.1, audit_frac=0.0)
+    pr = torch.sigmoid(nr.logits(f)).cpu().numpy()
+    pk = torch.sigmoid(nk.logits(f)).cpu().numpy()
+    torch.cuda.synchronize()
+    assert stats.cpu().tolist() == [0] * 8
+    # away from the threshold, where host and device sigmoids cannot disagree
+    sure = (np.abs(pr - 0.5) > 1e-4) & (np.abs(pk - 0.5) > 1e-4)
+    want_r = (pr >= 0.5) & (pk > 0.5)
+    want_k = (pk >= 0.5) | (pr >= 0.5)
+    assert np.array_equal(refine.cpu().numpy()[sure], want_r[sure].astype(np.uint8))
+    assert np.array_equal(keep.cpu().numpy()[sure], want_k[sure].astype(np.uint8))
+
+
 def test_trained_indicator_meets_the_contract(B):
     """Train on labels from small mixed-mesh runs; set the thresholds on a
     validation split with a margin of one logit unit; evaluate on blocks of
