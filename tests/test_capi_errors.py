@@ -96,6 +96,28 @@ def test_remesh_arguments():
     assert f(FAKE, FAKE, FAKE, FAKE, FAKE, 16385, FAKE, FAKE, None) == ELIMIT
     assert f(FAKE, FAKE, FAKE, FAKE, FAKE, 0, FAKE, FAKE, None) == EINVAL
     assert f(None, FAKE, FAKE, FAKE, FAKE, 16, FAKE, FAKE, None) == EINVAL
+    # exact test: variable count outside 1..24, tolerance not positive, no mesh
+    w = lib.bssn_remesh_wavelet_f64
+    assert w(FAKE, PTRS, 25, 1e-6, FAKE, None, None, None) == EINVAL
+    assert w(FAKE, PTRS, 0, 1e-6, FAKE, None, None, None) == EINVAL
+    assert w(FAKE, PTRS, 24, 0.0, FAKE, None, None, None) == EINVAL
+    assert w(None, PTRS, 24, 1e-6, FAKE, None, None, None) == EINVAL
+    assert lib.bssn_remesh_features_f64(None, PTRS, FAKE, None) == EINVAL
+    # two-flag decision: thresholds out of order, audit fraction or keep factor
+    # outside [0, 1], tolerance not positive, missing outputs
+    d = lib.bssn_remesh_decide2_f64
+
+    def dec(lo_r=0.1, hi_r=0.9, lo_k=0.1, hi_k=0.9, audit=0.05, tol=1e-6, kf=0.1, out=FAKE):
+        return d(FAKE, PTRS, FAKE, FAKE, lo_r, hi_r, FAKE, FAKE, lo_k, hi_k, audit, 7, tol, kf,
+                 out, FAKE, FAKE, FAKE, 1 << 30, None)
+    assert dec(lo_r=0.9, hi_r=0.1) == EINVAL
+    assert dec(lo_k=0.9, hi_k=0.1) == EINVAL
+    assert dec(audit=1.5) == EINVAL
+    assert dec(audit=-0.1) == EINVAL
+    assert dec(kf=1.5) == EINVAL
+    assert dec(kf=0.0) == EINVAL
+    assert dec(tol=0.0) == EINVAL
+    assert dec(out=None) == EINVAL
 
 
 def test_tile_queries():
