@@ -542,6 +542,49 @@ def remesh_decide(mesh: Mesh, unz, net: RemeshMLP, tol=1e-6, audit_frac=0.05, se
     return flags, stats
 
 
+lib.bssn_remesh_decide2_elem_work_bytes.argtypes = [C.c_void_p]
+lib.bssn_remesh_decide2_elem_work_bytes.restype = C.c_size_t
+lib.bssn_remesh_decide2_elem_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float,
+                                             C.c_float, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
+                                             C.c_double, C.c_uint64, C.c_double, C.c_double, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
+lib.bssn_remesh_element_features_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+
+
+def element_features(mesh: Mesh, unz, stream=None):
+    """16 features per element (num_elements x 16 float32, CUDA)."""
+    import torch
+    ne = lib.bssn_mesh_num_elements(mesh.h)
+    f = torch.empty((ne, 16), dtype=torch.float32, device="cuda")
+    check(lib.bssn_remesh_element_features_f64(mesh.h, ptrs(unz), _vp(f), stream_ptr(stream)),
+          "remesh_element_features")
+    return f
+
+
+def remesh_decide2_elem(mesh: Mesh, unz, net_refine: RemeshMLP, net_keep: RemeshMLP, tol=1e-6, keep_fac=0.1,
+                        audit_frac=0.05, seed=7, work=None, stream=None):
+    """Block refine and keep flags from per-element decisions (networks
+    trained on element features and labels): the exact test runs only on the
+    elements either network is unsure of and on a seeded audit sample of the
+    elements; a block takes a flag when any of its elements does.  Returns
+    (refine uint8[nblocks], keep uint8[nblocks], stats int32[8] counted per
+    element)."""
+    import torch
+    nb = mesh.spec.nblocks
+    wb = lib.bssn_remesh_decide2_elem_work_bytes(mesh.h)
+    if work is None or work.numel() < wb:
+        work = torch.empty(wb, dtype=torch.uint8, device="cuda")
+    refine = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    keep = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    stats = torch.zeros(8, dtype=torch.int32, device="cuda")
+    check(lib.bssn_remesh_decide2_elem_f64(mesh.h, ptrs(unz), _vp(net_refine.wq), _vp(net_refine.norm),
+                                           net_refine.lo, net_refine.hi, _vp(net_keep.wq), _vp(net_keep.norm),
+                                           net_keep.lo, net_keep.hi, audit_frac, seed, tol, keep_fac, _vp(refine),
+                                           _vp(keep), _vp(stats), _vp(work), wb, stream_ptr(stream)),
+          "remesh_decide2_elem")
+    return refine, keep, stats
+
+
 lib.bssn_remesh_decide2_work_bytes.argtypes = [C.c_void_p]
 lib.bssn_remesh_decide2_work_bytes.restype = C.c_size_t
 lib.bssn_remesh_decide2_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float,

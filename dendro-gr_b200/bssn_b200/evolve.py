@@ -20,14 +20,17 @@ a refined region scores below tol on its finer grid, coarsens at the next
 test and refines again at the one after.
 
 The learned run uses two networks of the same shape, one per threshold,
-trained on the labels the exact test gave during the exact run (features of
-every block at every remesh test).  Their decision thresholds are set on the
-samples of the exact run's last fifth of remesh tests, which the networks
-never saw in training (snapshots later in the evolution, on the meshes of
-that time), and lowered by a margin in logit units.  One decision pass
-serves both flags (bssn_remesh_decide2_f64): the features once, both
-networks, and one exact-test pass on the blocks either network is unsure of
-plus a seeded audit sample.  In the learned run the exact test is also
+trained on the labels the exact test gave during the exact run: features of
+every element (the default) or every block at every remesh test.  Their
+decision thresholds are set on the samples of the exact run's last fifth of
+remesh tests, which the networks never saw in training (snapshots later in
+the evolution, on the meshes of that time), and lowered by a margin in logit
+units.  One decision pass serves both flags (bssn_remesh_decide2_elem_f64,
+or bssn_remesh_decide2_f64 per block): the features once, both networks, and
+one exact-test pass on the elements (blocks) either network is unsure of plus
+a seeded audit sample; per element, a block takes a flag when any of its
+elements does, so an uncertain corner of a large block no longer sends the
+whole block to the exact test.  In the learned run the exact test is also
 evaluated at every remesh test, outside the timed decision, to count the
 refine and keep flags the decision missed.
 
@@ -42,7 +45,8 @@ import time
 import numpy as np
 
 from . import (Mesh, NVARS, PLAN_ENFORCE_STAGES, PLAN_GRAPH, RemeshMLP, RK4Plan, block_features,
-               constraints, default_params, remesh_decide2, wavelet_scores)
+               constraints, default_params, element_features, remesh_decide2, remesh_decide2_elem,
+               wavelet_scores)
 from . import levels as LV
 from .remesh_train import pick_thresholds, train
 
@@ -163,11 +167,12 @@ def run(indicator, a, nets=None, collect=False, log=print):
             st.mesh.unzip(st.P, st.U)
             e0.record()
             if indicator == "exact":
-                _, ratio, flags = wavelet_scores(st.mesh, st.P, tol=a.tol)
+                scores, ratio, flags = wavelet_scores(st.mesh, st.P, tol=a.tol)
                 keep = (ratio > a.amr_fac).to(torch.uint8)
             else:
-                flags, keep, stats = remesh_decide2(st.mesh, st.P, nets[0], nets[1], tol=a.tol,
-                                                    keep_fac=a.amr_fac, audit_frac=a.audit, seed=step)
+                decide = remesh_decide2_elem if a.granularity == "element" else remesh_decide2
+                flags, keep, stats = decide(st.mesh, st.P, nets[0], nets[1], tol=a.tol,
+                                            keep_fac=a.amr_fac, audit_frac=a.audit, seed=step)
             e1.record()
             e1.synchronize()
             rec["decide_ms"] += e0.elapsed_time(e1)
@@ -183,7 +188,14 @@ def run(indicator, a, nets=None, collect=False, log=print):
             else:
                 rec["exact_refinements"] += int(flags.sum())
                 rec["exact_keeps"] += int(keep.sum())
-            if collect:
+            if collect and a.granularity == "element":
+                # per element: its largest score over the variables against
+                # tol and amr_fac * tol (the block test's ratio, per element)
+                r = scores.amax(dim=1) / a.tol
+                X.append(element_features(st.mesh, st.P).cpu().numpy())
+                Y.append((r > 1.0).float().cpu().numpy())
+                K.append((r > a.amr_fac).float().cpu().numpy())
+            elif collect:
                 X.append(block_features(st.mesh, st.P).cpu().numpy())
                 Y.append(flags.float().cpu().numpy())
                 K.append(keep.float().cpu().numpy())
@@ -267,6 +279,9 @@ def main(argv=None):
     ap.add_argument("--fp-target", type=float, default=1e-2,
                     help="fraction of validation negatives the upper threshold may let through "
                          "(extra refinement or a delayed coarsening, never a missed refinement)")
+    ap.add_argument("--granularity", default="element", choices=("element", "block"),
+                    help="what the networks decide: each element (the exact test then runs on the "
+                         "uncertain elements only) or each block")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     a.max_box = a.max_box or a.M0
@@ -289,7 +304,7 @@ def main(argv=None):
     le = run("learned", a, nets=nets)
     res = {"config": {k: getattr(a, k) for k in ("M0", "levels", "max_levels", "half", "max_box", "steps", "remesh_every",
                                                  "diag_every", "cfl", "tol", "amr_fac", "audit", "train_steps",
-                                                 "margin", "fp_target", "max_block_octants")},
+                                                 "margin", "fp_target", "max_block_octants", "granularity")},
            "training": {"samples": int(len(tr)), "validation": int(nva), "refine_labels": int(Y.sum()),
                         "keep_labels": int(K.sum()), "thresholds": [[n.lo, n.hi] for n in nets],
                         "seconds": train_s},

@@ -578,6 +578,71 @@ int bssn_remesh_decide2_f64(bssn_mesh mesh, const double* const* unzip_dev, cons
     return st;
 }
 
+int bssn_remesh_element_features_f64(bssn_mesh mesh, const double* const* unzip_dev, float* feats_dev,
+                                     bssn_stream_t stream) {
+    if (!mesh || !unzip_dev || !feats_dev) return BSSN_EINVAL;
+    return bssn::launch_element_features(mesh->st, unzip_dev, feats_dev, S(stream));
+}
+
+size_t bssn_remesh_decide2_elem_work_bytes(bssn_mesh mesh) {
+    if (!mesh) return 0;
+    const size_t ne = (size_t)bssn_mesh_num_elements(mesh);
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    return al(ne * 16 * sizeof(float)) + 2 * al(ne * sizeof(float)) + 2 * al(ne) +
+           al((ne + 2) * sizeof(int64_t)) + al(ne * sizeof(int32_t)) + al(ne * bssn::NVARS * sizeof(double));
+}
+
+int bssn_remesh_decide2_elem_f64(bssn_mesh mesh, const double* const* unzip_dev, const void* wq_refine,
+                                 const float* norm_refine, float lo_r, float hi_r, const void* wq_keep,
+                                 const float* norm_keep, float lo_k, float hi_k, double audit_frac,
+                                 uint64_t seed, double tol, double keep_fac, uint8_t* refine_dev,
+                                 uint8_t* keep_dev, int* stats_dev, void* work_dev, size_t work_bytes,
+                                 bssn_stream_t stream) {
+    if (!mesh || !unzip_dev || !wq_refine || !wq_keep || !refine_dev || !keep_dev || !stats_dev ||
+        !work_dev)
+        return BSSN_EINVAL;
+    if (!(lo_r <= hi_r) || !(lo_k <= hi_k) || audit_frac < 0 || audit_frac > 1 || !(tol > 0) ||
+        !(keep_fac > 0) || keep_fac > 1)
+        return BSSN_EINVAL;
+    if (work_bytes < bssn_remesh_decide2_elem_work_bytes(mesh)) return BSSN_EINVAL;
+    bssn::MeshState* m = mesh->st;
+    int st = bssn::remesh_elements(m);
+    if (st) return st;
+    const int64_t ne = m->n_elems;
+    if (ne > 0x7fffffff) return BSSN_ELIMIT;
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    char* w = (char*)work_dev;
+    float* feats = (float*)w;
+    w += al((size_t)ne * 16 * sizeof(float));
+    float* lr = (float*)w;
+    w += al((size_t)ne * sizeof(float));
+    float* lk = (float*)w;
+    w += al((size_t)ne * sizeof(float));
+    uint8_t* need = (uint8_t*)w;
+    w += al(ne);
+    uint8_t* decided = (uint8_t*)w;
+    w += al(ne);
+    int64_t* off = (int64_t*)w;  // ne offsets, then the count
+    w += al((size_t)(ne + 2) * sizeof(int64_t));
+    int32_t* list = (int32_t*)w;
+    w += al((size_t)ne * sizeof(int32_t));
+    double* scores = (double*)w;
+    cudaStream_t s = S(stream);
+    st = cudaMemsetAsync(stats_dev, 0, 8 * sizeof(int), s) == cudaSuccess ? 0 : BSSN_EINVAL;
+    if (!st) st = bssn::launch_element_features(m, unzip_dev, feats, s);
+    if (!st) st = bssn::launch_mlp_fwd(wq_refine, norm_refine, feats, (int)ne, lr, s);
+    if (!st) st = bssn::launch_mlp_fwd(wq_keep, norm_keep, feats, (int)ne, lk, s);
+    if (!st)
+        st = bssn::launch_remesh_select_elem(m, lr, lk, lo_r, hi_r, lo_k, hi_k, audit_frac, seed, need, decided,
+                                             stats_dev, s);
+    if (!st)
+        st = bssn::launch_wavelet_elements(m, unzip_dev, bssn::NVARS, scores, need, off, off + ne + 1, list, s);
+    if (!st)
+        st = bssn::launch_remesh_merge_elem(m, need, decided, scores, bssn::NVARS, tol, keep_fac, lr, lk, lo_r,
+                                            lo_k, stats_dev, refine_dev, keep_dev, s);
+    return st;
+}
+
 int bssn_mesh_partition(const BssnBlockDesc* blocks, int nblocks, int nparts, int32_t* part) {
     return bssn::mesh_partition(blocks, nblocks, nparts, part);
 }

@@ -223,7 +223,9 @@ __global__ void __launch_bounds__(32 * kWavWarps) wavelet_kernel(ConstVars U, in
 }
 
 // Element list of the blocks with need[b] set: one CTA scans the per-block
-// element counts into offsets (off[b]) and the total (*count) ...
+// element counts into offsets (off[b]) and the total (*count) ...  With
+// first == nullptr every entry counts one (need[] is per element, and the
+// list is of the entries themselves).
 constexpr int kScanThreads = 1024;
 __global__ void __launch_bounds__(kScanThreads) need_scan_kernel(const uint8_t* __restrict__ need,
                                                                  const int64_t* __restrict__ first, int nblk,
@@ -234,7 +236,7 @@ __global__ void __launch_bounds__(kScanThreads) need_scan_kernel(const uint8_t* 
     const int per = (nblk + kScanThreads - 1) / kScanThreads;
     const int b0 = min(nblk, t * per), b1 = min(nblk, b0 + per);
     int64_t mine = 0;
-    for (int b = b0; b < b1; b++) mine += need[b] ? first[b + 1] - first[b] : 0;
+    for (int b = b0; b < b1; b++) mine += need[b] ? (first ? first[b + 1] - first[b] : 1) : 0;
     int64_t x = mine;  // inclusive scan over the warp
     for (int o = 1; o < 32; o <<= 1) {
         const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -254,7 +256,7 @@ __global__ void __launch_bounds__(kScanThreads) need_scan_kernel(const uint8_t* 
     int64_t run = x - mine + (w > 0 ? wsum[w - 1] : 0);
     for (int b = b0; b < b1; b++) {
         off[b] = run;
-        run += need[b] ? first[b + 1] - first[b] : 0;
+        run += need[b] ? (first ? first[b + 1] - first[b] : 1) : 0;
     }
     if (t == kScanThreads - 1) *count = run;
 }
@@ -267,6 +269,10 @@ __global__ void __launch_bounds__(256) need_list_kernel(const uint8_t* __restric
     const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (b >= nblk || !need[b]) return;
+    if (!first) {
+        if (lane == 0) list[off[b]] = b;
+        return;
+    }
     const int64_t n = first[b + 1] - first[b];
     for (int64_t i = lane; i < n; i += 32) list[off[b] + i] = (int32_t)(first[b] + i);
 }
@@ -384,6 +390,104 @@ __global__ void __launch_bounds__(256) features_final_kernel(const BssnBlockDesc
         f[13] = (float)log10(r[13] + 1e-30);
         f[14] = (float)log10(r[14] + 1e-30);
         f[15] = (float)log10(h);
+    }
+}
+
+// Element features (16 floats per element): the block features' definitions
+// taken over one element's own sublattice, the nodes with even local index
+// (0, 2, 4, 6 along each axis: 64 points, padded coordinates 3 + 6 o + 2 m);
+// level, side and spacing are its block's.  One warp per element.
+__global__ void __launch_bounds__(256) element_features_kernel(ConstVars U,
+                                                               const BssnBlockDesc* __restrict__ blocks,
+                                                               const ElemRef* __restrict__ elems, int64_t nelem,
+                                                               float* __restrict__ feats) {
+    const int64_t e = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (e >= nelem) return;  // whole warp
+    const ElemRef er = elems[e];
+    const BssnBlockDesc b = blocks[er.blk];
+    const int s = b.sz;
+    const int64_t st[3] = {2, 2 * s, 2 * (int64_t)s * s};
+    const double* chi = U.p[U_CHI];
+    const double* al = U.p[U_ALPHA];
+    double mx[15];
+    for (int f = 0; f < 15; f++) mx[f] = 0.0;
+    double chimin = 1e300;
+    for (int q = lane; q < 64; q += 32) {
+        const int i = 3 + 6 * er.o[0] + 2 * (q & 3), j = 3 + 6 * er.o[1] + 2 * ((q >> 2) & 3),
+                  k = 3 + 6 * er.o[2] + 2 * (q >> 4);
+        const int64_t p = b.offset + i + s * (j + (int64_t)s * k);
+        const double c0 = chi[p], a0 = al[p];
+        for (int d = 0; d < 3; d++) {
+            const double cp = chi[p + st[d]], cm = chi[p - st[d]];
+            const double ap = al[p + st[d]], am = al[p - st[d]];
+            mx[d] = fmax(mx[d], fabs(__dmul_rn(__dsub_rn(cp, cm), 0.25)));
+            mx[3 + d] = fmax(mx[3 + d], fabs(__dmul_rn(__dsub_rn(ap, am), 0.25)));
+            mx[7 + d] = fmax(mx[7 + d], fabs(U.p[U_GT0 + d][p]));
+            mx[13] = fmax(mx[13], fabs(__dsub_rn(__dsub_rn(cp, c0), __dsub_rn(c0, cm))));
+            mx[14] = fmax(mx[14], fabs(__dsub_rn(__dsub_rn(ap, a0), __dsub_rn(a0, am))));
+        }
+        mx[6] = fmax(mx[6], fabs(U.p[U_K][p]));
+        chimin = fmin(chimin, c0);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int f = 0; f < 15; f++) mx[f] = fmax(mx[f], __shfl_xor_sync(0xffffffffu, mx[f], o));
+        chimin = fmin(chimin, __shfl_xor_sync(0xffffffffu, chimin, o));
+    }
+    if (lane == 0) {
+        float* f = feats + e * 16;
+        for (int q = 0; q < 10; q++) f[q] = (float)log10(mx[q] + 1e-30);
+        const double h = (b.ptmax[0] - b.ptmin[0]) / (s - 1);
+        f[10] = (float)b.level;
+        f[11] = (float)(s / 55.0);
+        f[12] = (float)log10(chimin);
+        f[13] = (float)log10(mx[13] + 1e-30);
+        f[14] = (float)log10(mx[14] + 1e-30);
+        f[15] = (float)log10(h);
+    }
+}
+
+// Block flags from element decisions, one warp per block: an element the
+// exact test ran on (need) takes its flags from its largest score over the
+// variables (ratio = max / tol: refine above 1, keep above keep_fac), the
+// others the networks' decisions; a block refines (keeps) when any of its
+// elements does.  stats as remesh_merge2_kernel's, counted per element.
+__global__ void __launch_bounds__(256) remesh_merge_elem_kernel(int nblk, const int64_t* __restrict__ first,
+                                                                const uint8_t* __restrict__ need,
+                                                                const uint8_t* __restrict__ decided,
+                                                                const double* __restrict__ scores, int nvars,
+                                                                double tol, double keep_fac,
+                                                                const float* __restrict__ lr,
+                                                                const float* __restrict__ lk, float lo_r,
+                                                                float lo_k, int* stats, uint8_t* flags_r,
+                                                                uint8_t* flags_k) {
+    const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (b >= nblk) return;  // whole warp
+    unsigned fr = 0, fk = 0;
+    for (int64_t e = first[b] + lane; e < first[b + 1]; e += 32) {
+        if (need[e]) {
+            double m = 0.0;
+            for (int v = 0; v < nvars; v++) m = fmax(m, scores[e * nvars + v]);
+            const double r = m / tol;
+            const unsigned er = r > 1.0 ? 1u : 0u, ek = r > keep_fac ? 1u : 0u;
+            fr |= er;
+            fk |= ek;
+            const float pr = 1.0f / (1.0f + expf(-lr[e])), pk = 1.0f / (1.0f + expf(-lk[e]));
+            if (pr <= lo_r && er) atomicAdd(&stats[3], 1);
+            if (er) atomicAdd(&stats[4], 1);
+            if (pk <= lo_k && ek) atomicAdd(&stats[5], 1);
+            if (ek) atomicAdd(&stats[6], 1);
+        } else {
+            fr |= decided[e] & 1u;
+            fk |= (decided[e] >> 1) & 1u;
+        }
+    }
+    fr = __any_sync(0xffffffffu, fr) ? 1u : 0u;
+    fk = __any_sync(0xffffffffu, fk) ? 1u : 0u;
+    if (lane == 0) {
+        flags_r[b] = (uint8_t)fr;
+        flags_k[b] = (uint8_t)fk;
     }
 }
 
@@ -742,6 +846,61 @@ __global__ void __launch_bounds__(256) remesh_select2_kernel(const float* __rest
     if (audit && !ur && !uk) atomicAdd(&stats[2], 1);
 }
 
+// Per element, as remesh_select2_kernel, but keeping the reasons apart for
+// remesh_settle_elem_kernel: need bit 0 = unsure for refine, bit 1 = unsure
+// for keep, bit 2 = audited.
+__global__ void __launch_bounds__(256) remesh_select_elem_kernel(const float* __restrict__ lr,
+                                                                 const float* __restrict__ lk, int n,
+                                                                 float lo_r, float hi_r, float lo_k,
+                                                                 float hi_k, double audit_frac,
+                                                                 uint64_t seed, uint8_t* need,
+                                                                 uint8_t* decided) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const float pr = 1.0f / (1.0f + expf(-lr[e])), pk = 1.0f / (1.0f + expf(-lk[e]));
+    const bool refine_sure = pr >= hi_r, nokeep_sure = pk <= lo_k;
+    const bool ur = pr > lo_r && pr < hi_r && !nokeep_sure;
+    const bool uk = pk > lo_k && pk < hi_k && !refine_sure;
+    const double u = (double)(hmix(seed + 0x9E3779B97F4A7C15ULL * (uint64_t)(e + 1)) >> 11) *
+                     (1.0 / 9007199254740992.0);
+    need[e] = (ur ? 1 : 0) | (uk ? 2 : 0) | (u < audit_frac ? 4 : 0);
+    decided[e] = (refine_sure && !nokeep_sure ? 1 : 0) | (pk >= hi_k || refine_sure ? 2 : 0);
+}
+
+// One warp per block.  A block takes a flag when any of its elements does, so
+// once the networks refine (keep) one of its elements, its other elements
+// are tested only for a flag still open: need becomes 1 for an element unsure
+// of an open flag or audited, else 0.  stats[0..2] += elements sent for
+// refine, for keep, audited only.
+__global__ void __launch_bounds__(256) remesh_settle_elem_kernel(int nblk, const int64_t* __restrict__ first,
+                                                                 uint8_t* need,
+                                                                 const uint8_t* __restrict__ decided,
+                                                                 int* stats) {
+    const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (b >= nblk) return;  // whole warp
+    unsigned any = 0;
+    for (int64_t e = first[b] + lane; e < first[b + 1]; e += 32) any |= decided[e] & 3u;
+    for (int o = 16; o > 0; o >>= 1) any |= __shfl_xor_sync(0xffffffffu, any, o);
+    const bool rs = any & 1u, ks = any & 2u;
+    int cr = 0, ck = 0, ca = 0;
+    for (int64_t e0 = first[b]; e0 < first[b + 1]; e0 += 32) {
+        const int64_t e = e0 + lane;
+        const bool in = e < first[b + 1];
+        const unsigned nb = in ? need[e] : 0u;
+        const bool ur = (nb & 1u) && !rs, uk = (nb & 2u) && !rs && !ks, au = nb & 4u;
+        if (in) need[e] = (ur || uk || au) ? 1 : 0;
+        cr += __popc(__ballot_sync(0xffffffffu, ur));
+        ck += __popc(__ballot_sync(0xffffffffu, uk));
+        ca += __popc(__ballot_sync(0xffffffffu, au && !ur && !uk));
+    }
+    if (lane == 0) {
+        if (cr) atomicAdd(&stats[0], cr);
+        if (ck) atomicAdd(&stats[1], ck);
+        if (ca) atomicAdd(&stats[2], ca);
+    }
+}
+
 // Final flags: from the exact ratio (block max score / tol) where the exact
 // test ran, the networks' decisions elsewhere.
 __global__ void __launch_bounds__(256) remesh_merge2_kernel(int nblk, const uint8_t* need,
@@ -774,6 +933,21 @@ int launch_remesh_select2(const float* lr, const float* lk, int nblk, float lo_r
                           uint8_t* decided, int* stats, cudaStream_t s) {
     remesh_select2_kernel<<<(nblk + 255) / 256, 256, 0, s>>>(lr, lk, nblk, lo_r, hi_r, lo_k, hi_k,
                                                              audit_frac, seed, need, decided, stats);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_remesh_select_elem(MeshState* m, const float* lr, const float* lk, float lo_r, float hi_r,
+                              float lo_k, float hi_k, double audit_frac, uint64_t seed, uint8_t* need_e,
+                              uint8_t* decided_e, int* stats, cudaStream_t s) {
+    int st = remesh_elements(m);
+    if (st) return st;
+    const int64_t ne = m->n_elems;
+    const int nb = (int)m->blocks.size();
+    if (ne == 0) return 0;
+    remesh_select_elem_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(lr, lk, (int)ne, lo_r, hi_r, lo_k, hi_k,
+                                                                           audit_frac, seed, need_e, decided_e);
+    remesh_settle_elem_kernel<<<(unsigned)(((int64_t)nb * 32 + 255) / 256), 256, 0, s>>>(nb, m->d_elem_first,
+                                                                                       need_e, decided_e, stats);
     return cuda_status(cudaGetLastError());
 }
 
@@ -843,6 +1017,50 @@ int launch_block_flags(MeshState* m, const double* scores, int nvars, double tol
     const int nb = (int)m->blocks.size();
     block_flags_kernel<<<(unsigned)(((int64_t)nb * 32 + 255) / 256), 256, 0, s>>>(scores, nvars, m->d_elem_first, nb, tol,
                                                                           ratio, flags, need);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_element_features(MeshState* m, const double* const* U, float* feats, cudaStream_t s) {
+    int st = remesh_elements(m);
+    if (st) return st;
+    if (m->n_elems == 0) return 0;
+    ConstVars u = {};
+    for (int v = 0; v < NVARS; v++) u.p[v] = U[v];
+    element_features_kernel<<<(unsigned)((m->n_elems * 32 + 255) / 256), 256, 0, s>>>(u, m->d_blocks, m->d_elems,
+                                                                                   m->n_elems, feats);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_wavelet_elements(MeshState* m, const double* const* U, int nvars, double* scores,
+                            const uint8_t* need_e, int64_t* off, int64_t* count, int32_t* list,
+                            cudaStream_t s) {
+    int st = remesh_elements(m);
+    if (st) return st;
+    const int64_t ne = m->n_elems;
+    if (ne == 0) return 0;
+    ConstVars u = {};
+    for (int v = 0; v < nvars; v++) u.p[v] = U[v];
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t blocks = std::min<int64_t>((ne * nvars + kWavWarps - 1) / kWavWarps, (int64_t)nsm * 8);
+    need_scan_kernel<<<1, kScanThreads, 0, s>>>(need_e, nullptr, (int)ne, off, count);
+    need_list_kernel<<<(unsigned)((ne * 32 + 255) / 256), 256, 0, s>>>(need_e, nullptr, (int)ne, off, list);
+    wavelet_kernel<<<(unsigned)blocks, 32 * kWavWarps, 0, s>>>(u, nvars, m->d_blocks, m->d_elems, ne, list, count,
+                                                              scores);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_remesh_merge_elem(MeshState* m, const uint8_t* need_e, const uint8_t* decided_e,
+                             const double* scores, int nvars, double tol, double keep_fac, const float* lr,
+                             const float* lk, float lo_r, float lo_k, int* stats, uint8_t* flags_r,
+                             uint8_t* flags_k, cudaStream_t s) {
+    int st = remesh_elements(m);
+    if (st) return st;
+    const int nb = (int)m->blocks.size();
+    remesh_merge_elem_kernel<<<(unsigned)(((int64_t)nb * 32 + 255) / 256), 256, 0, s>>>(
+        nb, m->d_elem_first, need_e, decided_e, scores, nvars, tol, keep_fac, lr, lk, lo_r, lo_k, stats, flags_r,
+        flags_k);
     return cuda_status(cudaGetLastError());
 }
 

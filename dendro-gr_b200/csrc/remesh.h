@@ -23,6 +23,21 @@ int launch_wavelet_scores(MeshState* m, const double* const* U, int nvars, doubl
 int launch_block_flags(MeshState* m, const double* scores, int nvars, double tol, double* ratio,
                        uint8_t* flags, const uint8_t* need, cudaStream_t s);
 int launch_features(MeshState* m, const double* const* U, float* feats, cudaStream_t s);
+// per-element features (n_elems x 16)
+int launch_element_features(MeshState* m, const double* const* U, float* feats, cudaStream_t s);
+// exact test on the elements with need_e set (off: n_elems + 1, list: n_elems
+// scratch entries, count: one)
+int launch_wavelet_elements(MeshState* m, const double* const* U, int nvars, double* scores,
+                            const uint8_t* need_e, int64_t* off, int64_t* count, int32_t* list,
+                            cudaStream_t s);
+// per-element decision with block settling (remesh_settle_elem_kernel)
+int launch_remesh_select_elem(MeshState* m, const float* lr, const float* lk, float lo_r, float hi_r,
+                              float lo_k, float hi_k, double audit_frac, uint64_t seed, uint8_t* need_e,
+                              uint8_t* decided_e, int* stats, cudaStream_t s);
+int launch_remesh_merge_elem(MeshState* m, const uint8_t* need_e, const uint8_t* decided_e,
+                             const double* scores, int nvars, double tol, double keep_fac, const float* lr,
+                             const float* lk, float lo_r, float lo_k, int* stats, uint8_t* flags_r,
+                             uint8_t* flags_k, cudaStream_t s);
 // tensor-core forward (BF16 operands, FP32 accumulation); the decisions use it
 int launch_mlp_fwd(const void* wq, const float* norm, const float* X, int n, float* logits,
                    cudaStream_t s);

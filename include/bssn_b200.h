@@ -348,6 +348,34 @@ int bssn_remesh_decide2_f64(bssn_mesh mesh, const double* const* unzip_dev,
                             uint8_t* keep_dev, int* stats_dev, void* work_dev,
                             size_t work_bytes, bssn_stream_t stream);
 
+/* The two-flag decision per element instead of per block (the learned
+ * decision has no counterpart in the reference; the exact test it stands in
+ * for, isReMeshWAMR, BSSN_GR/src/dataUtils.cpp:511-624, also scores each
+ * element): 16 features per element
+ * (bssn_remesh_element_features_f64), both networks per element, the exact
+ * test only on the elements either network is unsure of plus the seeded audit
+ * sample (a fraction of the elements); a block refines (keeps its level)
+ * when any of its elements does, so once the networks refine (keep) one
+ * element of a block, its other elements go to the exact test only for a
+ * flag still open.  Same parameters and stats as
+ * bssn_remesh_decide2_f64, with every count per element; work_dev:
+ * bssn_remesh_decide2_elem_work_bytes(mesh) bytes.  A deferred large block no
+ * longer sends all of its elements to the exact test. */
+size_t bssn_remesh_decide2_elem_work_bytes(bssn_mesh mesh);
+int bssn_remesh_decide2_elem_f64(bssn_mesh mesh, const double* const* unzip_dev,
+                                 const void* wq_refine, const float* norm_refine, float lo_r,
+                                 float hi_r, const void* wq_keep, const float* norm_keep,
+                                 float lo_k, float hi_k, double audit_frac, uint64_t seed,
+                                 double tol, double keep_fac, uint8_t* refine_dev,
+                                 uint8_t* keep_dev, int* stats_dev, void* work_dev,
+                                 size_t work_bytes, bssn_stream_t stream);
+/* 16 features per element (num_elements x 16 floats): the block features'
+ * definitions over the element's own sublattice (local node indices 0, 2,
+ * 4, 6 along each axis: 64 points); level, side and spacing are the
+ * block's. */
+int bssn_remesh_element_features_f64(bssn_mesh mesh, const double* const* unzip_dev,
+                                     float* feats_dev, bssn_stream_t stream);
+
 /* ---------------------------------------------------------------------- */
 /* One whole RK4 step as a plan over a mesh (the reference's per-step
  * sequence rkBSSN.cpp:764-860: per stage unzip -> bssnRHS -> zip -> stage

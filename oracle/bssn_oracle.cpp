@@ -1385,6 +1385,54 @@ extern "C" void orc_wavelet_scores(const double** unzip, const OrcBlock* blks, i
     }
 }
 
+// Per-element features: the block features' definitions over each element's
+// even local nodes (4 x 4 x 4 points), elements block by block, octant x
+// fastest (the library's element order).
+extern "C" void orc_element_features(const double** unzip, const OrcBlock* blks, int nblk,
+                                     float* feats) {
+    int64_t e0 = 0;
+    for (int b = 0; b < nblk; b++) {
+        const int s = blks[b].sz, w = (s - 7) / 6;
+        const int64_t st[3] = {2, 2 * s, 2 * (int64_t)s * s};
+        const double* chi = unzip[U_CHI];
+        const double* al = unzip[U_ALPHA];
+        const double h = (blks[b].ptmax[0] - blks[b].ptmin[0]) / (s - 1);
+        for (int oz = 0; oz < w; oz++)
+            for (int oy = 0; oy < w; oy++)
+                for (int ox = 0; ox < w; ox++, e0++) {
+                    double mx[16];
+                    for (int f = 0; f < 16; f++) mx[f] = 0.0;
+                    double chimin = 1e300;
+                    for (int mz = 0; mz < 4; mz++)
+                        for (int my = 0; my < 4; my++)
+                            for (int mxi = 0; mxi < 4; mxi++) {
+                                const int i = 3 + 6 * ox + 2 * mxi, j = 3 + 6 * oy + 2 * my, k = 3 + 6 * oz + 2 * mz;
+                                const int64_t p = blks[b].offset + i + s * (j + (int64_t)s * k);
+                                const double c0 = chi[p], a0 = al[p];
+                                for (int d = 0; d < 3; d++) {
+                                    const double cp = chi[p + st[d]], cm = chi[p - st[d]];
+                                    const double ap = al[p + st[d]], am = al[p - st[d]];
+                                    mx[d] = std::max(mx[d], fabs((cp - cm) * 0.25));
+                                    mx[3 + d] = std::max(mx[3 + d], fabs((ap - am) * 0.25));
+                                    mx[7 + d] = std::max(mx[7 + d], fabs(unzip[U_GT0 + d][p]));
+                                    mx[13] = std::max(mx[13], fabs((cp - c0) - (c0 - cm)));
+                                    mx[14] = std::max(mx[14], fabs((ap - a0) - (a0 - am)));
+                                }
+                                mx[6] = std::max(mx[6], fabs(unzip[U_K][p]));
+                                chimin = std::min(chimin, c0);
+                            }
+                    float* f = feats + e0 * 16;
+                    for (int q = 0; q < 10; q++) f[q] = (float)log10(mx[q] + 1e-30);
+                    f[10] = (float)blks[b].level;
+                    f[11] = (float)(s / 55.0);
+                    f[12] = (float)log10(chimin);
+                    f[13] = (float)log10(mx[13] + 1e-30);
+                    f[14] = (float)log10(mx[14] + 1e-30);
+                    f[15] = (float)log10(h);
+                }
+    }
+}
+
 extern "C" void orc_block_features(const double** unzip, const OrcBlock* blks, int nblk,
                                    float* feats) {
 #pragma omp parallel for schedule(dynamic, 1)

@@ -161,6 +161,8 @@ void orc_psi4(double* re, double* im, const double** u, unsigned offset, const d
  * variable, elements numbered block by block, octant x fastest. */
 void orc_wavelet_scores(const double** unzip, const OrcBlock* blks, int nblk,
                         int nvars, double* scores);
+/* Per-element remesh features (16 floats per element, see bssn_b200.h). */
+void orc_element_features(const double** unzip, const OrcBlock* blks, int nblk, float* feats);
 /* Per-block remesh features (16 floats per block, see bssn_b200.h). */
 void orc_block_features(const double** unzip, const OrcBlock* blks, int nblk,
                         float* feats);

@@ -252,6 +252,86 @@ def test_decide2_nothing_deferred(B, state):
     assert np.array_equal(keep.cpu().numpy()[sure], want_k[sure].astype(np.uint8))
 
 
+def test_element_features_vs_oracle(B, state):
+    spec, m, Pz = state
+    f = B.element_features(m, Pz).cpu().numpy()
+    U = Pz.cpu().numpy()
+    ne = B.lib.bssn_mesh_num_elements(m.h)
+    ref = np.zeros((ne, 16), dtype=np.float32)
+    ol.oracle().lib.orc_element_features(ol.rows(U), spec.blocks, spec.nblocks, ref.ctypes.data_as(C.c_void_p))
+    assert np.allclose(f, ref, rtol=1e-6, atol=1e-6)
+
+
+def test_decide2_elem_defer_all_matches_exact(B, state):
+    """Per-element decision with both networks unsure of every element: the
+    exact test runs on every element and the block flags equal the exact
+    test's block flags."""
+    spec, m, Pz = state
+    nr, nk = B.RemeshMLP(seed=5), B.RemeshMLP(seed=6)
+    nr.lo, nr.hi, nk.lo, nk.hi = 0.0, 1.0, 0.0, 1.0
+    refine, keep, stats = B.remesh_decide2_elem(m, Pz, nr, nk, tol=1e-6, keep_fac=0.1, audit_frac=0.05)
+    _, ratio, exact = B.wavelet_scores(m, Pz, tol=1e-6)
+    torch.cuda.synchronize()
+    ne = B.lib.bssn_mesh_num_elements(m.h)
+    assert torch.equal(refine, exact)
+    assert torch.equal(keep, (ratio > 0.1).to(torch.uint8))
+    st = stats.cpu().tolist()
+    assert st[0] == ne and st[1] == ne and st[2] == 0
+
+
+def test_decide2_elem_nothing_deferred(B, state):
+    """Per-element decision with both networks sure everywhere and no audit:
+    no element reaches the exact test, and a block takes a flag when any of
+    its elements' network decisions does."""
+    spec, m, Pz = state
+    fe = B.element_features(m, Pz)
+    nr, nk = B.RemeshMLP(seed=5), B.RemeshMLP(seed=8)
+    nr.set_norm(fe)
+    nk.set_norm(fe)
+    nr.lo = nr.hi = nk.lo = nk.hi = 0.5
+    refine, keep, stats = B.remesh_decide2_elem(m, Pz, nr, nk, tol=1e-6, keep_fac=0.1, audit_frac=0.0)
+    pr = torch.sigmoid(nr.logits(fe)).cpu().numpy()
+    pk = torch.sigmoid(nk.logits(fe)).cpu().numpy()
+    torch.cuda.synchronize()
+    assert stats.cpu().tolist() == [0] * 8
+    er = (pr >= 0.5) & (pk > 0.5)
+    ek = (pk >= 0.5) | (pr >= 0.5)
+    sure = (np.abs(pr - 0.5) > 1e-4) & (np.abs(pk - 0.5) > 1e-4)
+    first = np.cumsum([0] + [((int(s) - 7) // 6) ** 3 for s in spec.sides])
+    r, k = refine.cpu().numpy(), keep.cpu().numpy()
+    checked = 0
+    for b in range(spec.nblocks):
+        sl = slice(first[b], first[b + 1])
+        if sure[sl].all():
+            assert r[b] == int(er[sl].any()) and k[b] == int(ek[sl].any()), b
+            checked += 1
+    assert checked > spec.nblocks // 2
+
+
+def test_decide2_elem_settled_blocks(B, state):
+    """A block takes a flag when any of its elements does.  Keep network sure
+    of every element (keep), refine network unsure: only the refine flag is
+    open, every element goes to the exact test for it and the block refine
+    flags equal the exact test's.  Refine network sure of every element:
+    every block refines and keeps, and no element is deferred."""
+    spec, m, Pz = state
+    ne = B.lib.bssn_mesh_num_elements(m.h)
+    nr, nk = B.RemeshMLP(seed=5), B.RemeshMLP(seed=8)
+    _, _, exact = B.wavelet_scores(m, Pz, tol=1e-6)
+    nr.lo, nr.hi, nk.lo, nk.hi = 0.0, 1.0, 0.0, 0.0
+    refine, keep, stats = B.remesh_decide2_elem(m, Pz, nr, nk, tol=1e-6, keep_fac=0.1, audit_frac=0.05)
+    torch.cuda.synchronize()
+    assert torch.equal(refine, exact)
+    assert bool((keep == 1).all())
+    st = stats.cpu().tolist()
+    assert st[0] == ne and st[1] == 0 and st[2] == 0
+    nr.lo, nr.hi, nk.lo, nk.hi = 0.0, 0.0, 0.0, 1.0
+    refine, keep, stats = B.remesh_decide2_elem(m, Pz, nr, nk, tol=1e-6, keep_fac=0.1, audit_frac=0.0)
+    torch.cuda.synchronize()
+    assert bool((refine == 1).all()) and bool((keep == 1).all())
+    assert stats.cpu().tolist()[:3] == [0, 0, 0]
+
+
 def test_trained_indicator_meets_the_contract(B):
     """Train on labels from small mixed-mesh runs; set the thresholds on a
     validation split with a margin of one logit unit; evaluate on blocks of
