@@ -279,6 +279,12 @@ def main(argv=None):
     ap.add_argument("--fp-target", type=float, default=1e-2,
                     help="fraction of validation negatives the upper threshold may let through "
                          "(extra refinement or a delayed coarsening, never a missed refinement)")
+    ap.add_argument("--fn-target", type=float, default=1e-3,
+                    help="missed-refinement budget of the refine network's lower threshold (half of it, "
+                         "before the margin, on the validation samples)")
+    ap.add_argument("--fn-keep", type=float, default=1e-2,
+                    help="the same budget for the keep network (a missed keep lets a block coarsen one "
+                         "test early; it never drops a refinement)")
     ap.add_argument("--granularity", default="element", choices=("element", "block"),
                     help="what the networks decide: each element (the exact test then runs on the "
                          "uncertain elements only) or each block")
@@ -298,13 +304,15 @@ def main(argv=None):
         net = RemeshMLP(seed=seed)
         train(net, X[tr], lab[tr], steps=a.train_steps, log=lambda s: None)
         pv = torch.sigmoid(net.logits(torch.tensor(X[va], device="cuda"))).cpu().numpy()
-        net.lo, net.hi = pick_thresholds(pv, lab[va], fp_target=a.fp_target, margin=a.margin)
+        fn = a.fn_target if seed == 0 else a.fn_keep
+        net.lo, net.hi = pick_thresholds(pv, lab[va], fn_target=fn, fp_target=a.fp_target, margin=a.margin)
         nets.append(net)
     train_s = time.perf_counter() - t0
     le = run("learned", a, nets=nets)
     res = {"config": {k: getattr(a, k) for k in ("M0", "levels", "max_levels", "half", "max_box", "steps", "remesh_every",
                                                  "diag_every", "cfl", "tol", "amr_fac", "audit", "train_steps",
-                                                 "margin", "fp_target", "max_block_octants", "granularity")},
+                                                 "margin", "fp_target", "fn_target", "fn_keep", "max_block_octants",
+                                                 "granularity")},
            "training": {"samples": int(len(tr)), "validation": int(nva), "refine_labels": int(Y.sum()),
                         "keep_labels": int(K.sum()), "thresholds": [[n.lo, n.hi] for n in nets],
                         "seconds": train_s},
