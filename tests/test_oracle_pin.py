@@ -208,3 +208,34 @@ def test_lowmem_constraint_norms_match():
     ref = ol.l2_norms(spec, ol.oracle_constraints(spec, mo.unzip(Z), O))
     got = ol.constraint_norms_lowmem(spec, Z, O)
     assert np.allclose(got, ref, rtol=1e-13, atol=0), (got, ref)
+
+
+def test_element_features_consistent_with_block_features():
+    """The per-element features partition the block features' sublattice: a
+    block's maxima are the largest of its elements' maxima, its smallest chi
+    the smallest of theirs, and a one-element block (13^3) has the same 16
+    features as its element (oracle against itself, on a mixed mesh with
+    every side and a perturbed state)."""
+    import ctypes as C
+    spec = ol.OracleMeshSpec(1, (2, 1, 1), seed=1, xmin=-8.25)
+    mo = ol.MeshOracle(spec, ol.oracle())
+    rng = np.random.default_rng(3)
+    Z = mo.initial_data(eps=1e-8, bh=(0.6, -4.1, -4.2, -0.6, -4.1, -4.2))
+    Z += rng.standard_normal(Z.shape) * 1e-6
+    U = mo.unzip(Z)
+    sides = np.array([spec.blocks[b].sz for b in range(spec.nblocks)])
+    assert set(sides.tolist()) == {13, 19, 31, 55}
+    first = np.cumsum([0] + [((int(s) - 7) // 6) ** 3 for s in sides])
+    fb = np.zeros((spec.nblocks, 16), dtype=np.float32)
+    fe = np.zeros((first[-1], 16), dtype=np.float32)
+    lib = mo.lib
+    lib.orc_block_features(ol.rows(U), spec.blocks, spec.nblocks, fb.ctypes.data_as(C.c_void_p))
+    lib.orc_element_features(ol.rows(U), spec.blocks, spec.nblocks, fe.ctypes.data_as(C.c_void_p))
+    maxima = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 13, 14]
+    for b in range(spec.nblocks):
+        e = fe[first[b]:first[b + 1]]
+        assert np.array_equal(fb[b, maxima], e[:, maxima].max(axis=0)), b
+        assert fb[b, 12] == e[:, 12].min(), b
+        assert np.all(e[:, [10, 11, 15]] == fb[b, [10, 11, 15]]), b
+        if sides[b] == 13:
+            assert np.array_equal(fb[b], e[0]), b
