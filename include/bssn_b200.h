@@ -359,8 +359,9 @@ int bssn_remesh_decide2_f64(bssn_mesh mesh, const double* const* unzip_dev,
  * element of a block, its other elements go to the exact test only for a
  * flag still open.  Same parameters and stats as
  * bssn_remesh_decide2_f64, with every count per element; work_dev:
- * bssn_remesh_decide2_elem_work_bytes(mesh) bytes.  A deferred large block no
- * longer sends all of its elements to the exact test. */
+ * bssn_remesh_decide2_elem_work_bytes(mesh) bytes; BSSN_ELIMIT for meshes of
+ * 2^31 elements or more.  A deferred large block no longer sends all of its
+ * elements to the exact test. */
 size_t bssn_remesh_decide2_elem_work_bytes(bssn_mesh mesh);
 int bssn_remesh_decide2_elem_f64(bssn_mesh mesh, const double* const* unzip_dev,
                                  const void* wq_refine, const float* norm_refine, float lo_r,
