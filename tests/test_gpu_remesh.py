@@ -337,7 +337,7 @@ def test_trained_indicator_meets_the_contract(B):
     validation split with a margin of one logit unit; evaluate on blocks of
     runs with other seeds: the learned decision misses at most 0.1 % of the
     blocks the exact test refines there, and on a fresh config-2-sized
-    snapshot (about 3,300 blocks) it is at least 5 times faster than the
+    snapshot (3,948 blocks) it is at least 5 times faster than the
     exact test on every block."""
     from bssn_b200 import remesh_train as rt
     X, Y = rt.collect(16000, dims=(4, 3, 3), log=lambda *a: None)
